@@ -1,0 +1,170 @@
+/*
+ * acgpu — C ABI of the B200 solve phase for Laplacians.jl's approxchol_lap.
+ *
+ * The reference (Laplacians.jl v1.4.1) builds, in Julia,
+ *     f = approxchol_lap(a; tol, maxits, maxtime, verbose, pcgIts, params)
+ * (src/approxChol.jl:1522-1545) whose closure (src/approxChol.jl:1624) runs
+ *     pcg(lap(a), b .- mean(b), b -> LDLsolver(ldli, b); stag_test = 5)
+ * (src/pcg.jl:256-445, src/approxChol.jl:1347-1408).  This library replaces
+ * that closure body: the host hands over the adjacency matrix and the LDLinv
+ * factor once (acg_create), and every solve runs on the GPU (acg_solve).
+ *
+ * Conventions
+ *   - Plain C types only.  Index arrays are int64 as Julia stores them; the
+ *     `index_base` argument says whether they are 1-based (Julia) or 0-based.
+ *   - Every function returns an int status: 0 = ACG_OK, > 0 = a convergence
+ *     outcome of a finished solve (mirrors the reference's PCG stop reasons),
+ *     < 0 = an error; acg_last_error() then holds a message (thread-local).
+ *   - No exception crosses the ABI.  The caller keeps ownership of every
+ *     array it passes; the library copies what it needs.
+ *   - A solver handle is used by one host thread at a time.
+ */
+#ifndef ACGPU_H
+#define ACGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define ACG_OK 0
+/* convergence outcomes (>0): the solve finished and x holds the best iterate */
+#define ACG_STOP_MAXITS 1      /* itcnt reached maxits            (src/pcg.jl:288)     */
+#define ACG_STOP_STAG_X 2      /* al*|p|_1 < eps*|x|_1            (src/pcg.jl:308-317) */
+#define ACG_STOP_STAG_R 3      /* al*|q|_1 < eps*|r|_1            (src/pcg.jl:330-338) */
+#define ACG_STOP_STAG_RHO 4    /* rho stagnation test             (src/pcg.jl:370-383) */
+#define ACG_STOP_INF 5         /* rho or beta infinite            (src/pcg.jl:385-400) */
+#define ACG_STOP_STAG_P 6      /* beta*|p|_1 < eps*|z|_1          (src/pcg.jl:406-414) */
+#define ACG_STOP_MAXTIME 7     /* wall time above maxtime         (src/pcg.jl:425-430) */
+/* errors (<0) */
+#define ACG_ERR_INVALID -1     /* bad argument or malformed input  */
+#define ACG_ERR_NOMEM -2       /* host or device allocation failed */
+#define ACG_ERR_CUDA -3        /* a CUDA runtime call failed       */
+#define ACG_ERR_TIMEOUT -4     /* a bounded device wait gave up    */
+#define ACG_ERR_NODEVICE -5    /* no usable sm_100 device          */
+#define ACG_ERR_BUSY -6        /* admission refused (memory budget)*/
+
+/* Last error message of the calling thread ("" if none). */
+const char* acg_last_error(void);
+
+/* ---- host: Julia-compatible random stream ------------------------------ */
+/* Random.seed!(seed) of Julia 1.8 (stdlib Random, Xoshiro256++ seeded through
+ * SHA-256 of the seed's 32-bit limbs).  Writes the 4-word state. */
+int acg_rng_seed(uint64_t seed, uint64_t state[4]);
+/* `count` draws of Julia's rand()::Float64 from `state` (advanced in place). */
+int acg_rng_rand(uint64_t state[4], double* out, int64_t count);
+/* SHA-256 digest, exposed for the known-answer test of the seeding path. */
+int acg_sha256(const uint8_t* data, int64_t len, uint8_t out[32]);
+
+/* ---- host: approximate Cholesky elimination ---------------------------- */
+typedef struct acg_factor acg_factor;
+/* approxChol(LLmatp(a)) with the default :deg order (src/approxChol.jl:864-977,
+ * 102-136, 2085-2239).  `a` is the adjacency matrix in CSC form: n columns,
+ * colptr[n+1] (0- or 1-based, detected from colptr[0]), sorted rowval, weights
+ * nzval >= 0, structurally symmetric, zero diagonal, every vertex with an
+ * edge.  Draws from `rng_state` exactly where the reference calls rand(), and
+ * advances it.  On success *out owns the factor (free with acg_factor_free). */
+int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval,
+                   const double* nzval, uint64_t rng_state[4], acg_factor** out);
+/* n and F = length(ldli.fval). */
+int acg_factor_dims(const acg_factor* f, int64_t* n, int64_t* nnz);
+/* Copy out the LDLinv arrays in the reference layout (src/approxCholTypes.jl:73-79),
+ * 1-based: col[n-1], colptr[n], rowval[F], fval[F], d[n]. */
+int acg_factor_export(const acg_factor* f, int64_t* col, int64_t* colptr, int64_t* rowval,
+                      double* fval, double* d);
+void acg_factor_free(acg_factor* f);
+
+/* ---- device solver ------------------------------------------------------ */
+typedef struct acg_solver acg_solver;
+
+/* Optional tuning knobs of acg_create (0 = automatic). */
+typedef struct {
+  int sweep_lanes;     /* lanes per vertex in the LDLinv sweeps: 2, 4, 8 or 16      */
+  int spmv_lanes;      /* lanes per row in the Laplacian mat-vec: 2, 4, 8 or 16     */
+  int wide_level_min;  /* levels at least this wide get a grid launch; thinner runs
+                          of levels run in one CTA with block barriers            */
+  int reserved[5];
+} acg_options;
+
+/* Shape of an uploaded solver. */
+typedef struct {
+  int64_t n;           /* vertices                                   */
+  int64_t nnz_lap;     /* stored entries of lap(a) = nnz(a) + n       */
+  int64_t nnz_factor;  /* F = length(ldli.fval)                       */
+  int64_t levels;      /* depth of the LDLinv dependency DAG          */
+  int64_t wide_levels; /* levels swept with one grid launch each      */
+  int64_t thin_runs;   /* runs of thin levels swept by one CTA        */
+  int sweep_lanes, spmv_lanes;
+} acg_stats;
+
+/* Outcome of one solve (one right-hand side). */
+typedef struct {
+  int64_t iterations;  /* PCG iterations = pcgIts[1] (mixed: inner iterations summed) */
+  int64_t refinements; /* FP64 refinement steps (mixed precision), 0 for FP64        */
+  double relres;       /* |r|/|b| of the recursive residual when PCG stopped         */
+  double best_relres;  /* smallest recursive |r|/|b| (that of the returned bestx)    */
+  double true_relres;  /* |(b - mean b) - L x| / |b - mean b| of the returned x, FP64 */
+  double solve_ms;     /* device time of the solve graph (CUDA events)               */
+  int status;          /* 0 converged, else the ACG_STOP_* code                      */
+  int levels;          /* depth of the LDLinv dependency DAG                         */
+} acg_solve_info;
+
+/* Device time of the solve's kernels (milliseconds per call). */
+typedef struct {
+  double spmv_ms;           /* q = L p (one launch)                          */
+  double forward_ms;        /* forward LDLinv sweep (all its launches)       */
+  double backward_ms;       /* backward LDLinv sweep                         */
+  double iteration_ms;      /* the kernels of one PCG iteration              */
+  int launches_per_iteration;
+  int forward_launches;
+} acg_kernel_times;
+
+/* 0 if the current CUDA device is usable (sm_100), else an error code. */
+int acg_device_check(void);
+
+/* Upload lap(a) and an LDLinv factor to the current device.
+ * Replaces the captures `la = lap(a)` and `F(b) = LDLsolver(ldli, b)` of the
+ * closure built at src/approxChol.jl:1597-1624.
+ *   a_*: adjacency CSC (n columns, colptr[n+1], sorted rowval, nzval >= 0).
+ *   ldli_*: the LDLinv arrays (src/approxCholTypes.jl:73-79) with F = ldli_nnz
+ *           entries; index_base 1 for Julia arrays, 0 for 0-based ones.
+ * Builds the level schedule of the factor's dependency DAG, renumbers vertices
+ * by level, folds the running products of forward!/backward! into per-entry
+ * coefficients, and keeps FP64 and FP32 copies on the device. */
+int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, const double* a_nzval,
+               const int64_t* ldli_col, const int64_t* ldli_colptr, const int64_t* ldli_rowval,
+               const double* ldli_fval, const double* ldli_d, int64_t ldli_nnz, int index_base,
+               const acg_options* opts, acg_solver** out);
+void acg_destroy(acg_solver* h);
+int acg_solver_stats(const acg_solver* h, acg_stats* out);
+
+/* x = f(b): the closure body of src/approxChol.jl:1624, i.e.
+ * pcg(la, b .- mean(b), LDLsolver; tol, maxits, maxtime, stag_test) with the
+ * stop rules of src/pcg.jl:256-445, returning bestx.  Host arrays; nrhs
+ * right-hand sides stored column-major with leading dimension ldb (>= n when
+ * nrhs > 1), info[nrhs] optional.
+ *   precision 0: FP64 PCG (the reference algorithm).
+ *   precision 1: FP32 PCG (SpMV, LDLinv sweeps, vectors) inside FP64 iterative
+ *                refinement on the true residual; tol is then on
+ *                |b - L x| / |b| and maxits bounds the inner iterations.
+ * Returns 0 (all converged), the largest ACG_STOP_* code, or an error (<0). */
+int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol, int64_t maxits,
+              double maxtime, int stag_test, int precision, acg_solve_info* info);
+/* As acg_solve for one right-hand side already in device memory. */
+int acg_solve_device(acg_solver* h, const double* b_dev, double* x_dev, double tol, int64_t maxits, double maxtime,
+                     int stag_test, int precision, acg_solve_info* info);
+/* y = LDLsolver(ldli, r) (src/approxChol.jl:1347-1366) on the device; host arrays. */
+int acg_ldlsolve(acg_solver* h, const double* r, double* y, int precision);
+/* y = lap(a) * x on the device (FP64 or FP32 values); host arrays. */
+int acg_lap_mul(acg_solver* h, const double* x, double* y, int precision);
+/* Time the solve's kernels: each captured `reps` times into a CUDA graph and
+ * timed with CUDA events on the solver's stream (no reference counterpart). */
+int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ACGPU_H */

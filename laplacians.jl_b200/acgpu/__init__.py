@@ -1,0 +1,16 @@
+"""acgpu — the solve phase of Laplacians.jl's approxchol_lap on B200.
+
+Public interface (mirrors the reference's names and keyword semantics):
+    approxchol_lap, ApproxCholParams, lap, seed (Random.seed!), approx_chol,
+    DeviceLapSolver, components, generators.
+The solves run in libacgpu.so (CUDA, sm_100a); see include/acgpu.h.
+"""
+from . import generators
+from .solvers import (ApproxCholParams, DeviceLapSolver, LDLinv, approx_chol, approxchol_lap, approxchol_lap1,
+                      components, lap, null_solver, rng_state, seed, set_rng_state, vec_to_comps)
+from .solvers import _init as _solvers_init
+
+_solvers_init()
+
+__all__ = ["approxchol_lap", "approxchol_lap1", "ApproxCholParams", "LDLinv", "DeviceLapSolver", "approx_chol",
+           "lap", "seed", "rng_state", "set_rng_state", "components", "vec_to_comps", "null_solver", "generators"]

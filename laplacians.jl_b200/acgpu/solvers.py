@@ -1,0 +1,375 @@
+"""Host-side mirror of Laplacians.jl's `approxchol_lap` solver interface.
+
+    f = approxchol_lap(a; tol=1e-6, maxits=1000, maxtime=Inf, verbose=false,
+                       pcgIts=Int[], params=ApproxCholParams())
+    x = f(b; tol, maxits, maxtime, verbose, pcgIts)
+
+(src/approxChol.jl:1522-1545, 1581-1626; kwarg semantics in
+docs/src/usingSolvers.md:102-113.)  Here ``a`` is a symmetric
+``scipy.sparse`` adjacency matrix and ``f`` is a callable whose solves run on
+the GPU through libacgpu.so.  Every keyword keeps its meaning: ``pcgIts`` is a
+list whose first entry receives the iteration count, keywords given to ``f``
+override the ones given at construction, and a disconnected graph is solved
+per component as `lapWrapComponents` does (src/solverInterface.jl:212-275).
+
+Extra keyword (not in the reference): ``precision`` = "fp64" (default; the
+reference algorithm in FP64 on the GPU) or "mixed" (FP32 PCG inside FP64
+iterative refinement on the true residual).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from ._lib import AcgOptions, AcgSolveInfo, AcgStats, check, lib
+
+__all__ = [
+    "ApproxCholParams", "LDLinv", "approxchol_lap", "approxchol_lap1", "lap", "seed", "rng_state",
+    "set_rng_state", "approx_chol", "components", "vec_to_comps", "DeviceLapSolver", "null_solver",
+]
+
+_PRECISIONS = {"fp64": 0, "mixed": 1}
+
+# ---- the global random stream (Julia's default RNG) -------------------------
+
+_RNG = np.zeros(4, dtype=np.uint64)
+
+
+def seed(s: int) -> None:
+    """`Random.seed!(s)`: reseed the stream the elimination draws from."""
+    check(lib().acg_rng_seed(int(s), _RNG))
+
+
+def rng_state() -> np.ndarray:
+    return _RNG.copy()
+
+
+def set_rng_state(state) -> None:
+    _RNG[:] = np.asarray(state, dtype=np.uint64)
+
+
+def _seed_from_entropy():
+    # Julia seeds its default generator from system entropy at start-up.
+    seed(int.from_bytes(os.urandom(8), "little"))
+
+
+# ---- parameters and factor ----------------------------------------------------
+
+@dataclass
+class ApproxCholParams:
+    """`ApproxCholParams(order, stag_test, split, merge)`, default (:deg, 5, 0, 0)
+    (src/approxChol.jl:80-90)."""
+    order: str = "deg"
+    stag_test: int = 5
+    split: int = 0
+    merge: int = 0
+
+
+@dataclass
+class LDLinv:
+    """The factor in the reference layout (src/approxCholTypes.jl:73-79), 1-based."""
+    col: np.ndarray
+    colptr: np.ndarray
+    rowval: np.ndarray
+    fval: np.ndarray
+    d: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return int(self.d.shape[0])
+
+    @property
+    def nnz(self) -> int:
+        return int(self.fval.shape[0])
+
+
+def _csc(a) -> sp.csc_matrix:
+    a = sp.csc_matrix(a, dtype=np.float64)
+    a.sum_duplicates()
+    a.sort_indices()
+    return a
+
+
+def lap(a) -> sp.csc_matrix:
+    """`lap(a) = sparse(Diagonal(a*ones(n))) - a` (src/graphOps.jl:25)."""
+    a = _csc(a)
+    return _csc(sp.diags(np.asarray(a.sum(axis=1)).ravel()) - a)
+
+
+def approx_chol(a) -> LDLinv:
+    """`approxChol(LLmatp(a))` with the :deg order, drawing from the global
+    stream (src/approxChol.jl:864-977).  Runs on the host."""
+    a = _csc(a)
+    n = a.shape[0]
+    L = lib()
+    h = ctypes.c_void_p()
+    cp = a.indptr.astype(np.int64) + 1
+    rv = a.indices.astype(np.int64) + 1
+    check(L.acg_approxchol(n, cp, rv, np.ascontiguousarray(a.data), _RNG, ctypes.byref(h)))
+    try:
+        nn = ctypes.c_int64()
+        F = ctypes.c_int64()
+        check(L.acg_factor_dims(h, ctypes.byref(nn), ctypes.byref(F)))
+        col = np.empty(n - 1, np.int64)
+        colptr = np.empty(n, np.int64)
+        rowval = np.empty(F.value, np.int64)
+        fval = np.empty(F.value, np.float64)
+        d = np.empty(n, np.float64)
+        check(L.acg_factor_export(h, col, colptr, rowval, fval, d))
+    finally:
+        L.acg_factor_free(h)
+    return LDLinv(col, colptr, rowval, fval, d)
+
+
+# ---- components (src/graphAlgs.jl:64-108, 135-155) ---------------------------
+
+def components(a) -> np.ndarray:
+    """Component label (1-based) of every vertex, numbered in order of each
+    component's smallest vertex, as `components` does."""
+    from scipy.sparse.csgraph import connected_components
+    a = _csc(a)
+    _, lab = connected_components(a, directed=False)
+    first = np.full(lab.max() + 1, a.shape[0], dtype=np.int64)
+    np.minimum.at(first, lab, np.arange(a.shape[0]))
+    order = np.argsort(first, kind="stable")
+    relabel = np.empty_like(order)
+    relabel[order] = np.arange(order.shape[0])
+    return relabel[lab] + 1
+
+
+def vec_to_comps(co: np.ndarray) -> list:
+    order = np.argsort(co, kind="stable")
+    bounds = np.cumsum(np.bincount(co)[1:])
+    return np.split(order, bounds[:-1])
+
+
+# ---- the device solver ----------------------------------------------------------
+
+def _maxits_int(maxits) -> int:
+    if maxits is None or (isinstance(maxits, float) and math.isinf(maxits)):
+        return 1 << 62
+    return int(maxits)
+
+
+class DeviceLapSolver:
+    """The closure `f` of approxchol_lapGreedy (src/approxChol.jl:1624) with the
+    solve on the GPU.  Holds the uploaded lap(a) and LDLinv until closed."""
+
+    def __init__(self, a, ldli: LDLinv, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False, pcgIts=None,
+                 params: ApproxCholParams | None = None, precision="fp64", options: dict | None = None):
+        a = _csc(a)
+        self.n = a.shape[0]
+        self.ldli = ldli
+        self.params = params or ApproxCholParams()
+        self.defaults = dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts,
+                             precision=precision)
+        opts = AcgOptions()
+        for k, v in (options or {}).items():
+            setattr(opts, k, int(v))
+        h = ctypes.c_void_p()
+        check(lib().acg_create(self.n, a.indptr.astype(np.int64), a.indices.astype(np.int64),
+                               np.ascontiguousarray(a.data), ldli.col, ldli.colptr, ldli.rowval, ldli.fval, ldli.d,
+                               ldli.nnz, 1, ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+        self.last_info: list[AcgSolveInfo] = []
+
+    def stats(self) -> dict:
+        s = AcgStats()
+        check(lib().acg_solver_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in AcgStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().acg_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __call__(self, b, tol=None, maxits=None, maxtime=None, verbose=None, pcgIts=None, precision=None):
+        d = self.defaults
+        tol = d["tol"] if tol is None else tol
+        maxits = d["maxits"] if maxits is None else maxits
+        maxtime = d["maxtime"] if maxtime is None else maxtime
+        verbose = d["verbose"] if verbose is None else verbose
+        pcgIts = d["pcgIts"] if pcgIts is None else pcgIts
+        precision = d["precision"] if precision is None else precision
+        b = np.asarray(b, dtype=np.float64)
+        if b.shape[0] != self.n:
+            raise ValueError(f"rhs has {b.shape[0]} rows, solver has {self.n}")
+        cols = b.reshape(self.n, -1)
+        k = cols.shape[1]
+        B = np.ascontiguousarray(cols.T)  # each right-hand side contiguous
+        X = np.empty_like(B)
+        infos = (AcgSolveInfo * k)()
+        rc = check(lib().acg_solve(self._h, B, X, k, self.n, float(tol), _maxits_int(maxits), float(maxtime),
+                                   int(self.params.stag_test), _PRECISIONS[precision], infos))
+        self.last_info = list(infos)
+        its = max(int(i.iterations) for i in infos) if k else 0
+        if pcgIts is not None and len(pcgIts) > 0:
+            pcgIts[0] = its
+        if verbose:
+            for i in infos:
+                print(f"PCG stopped after: {i.solve_ms / 1e3:.3f} seconds and {i.iterations} iterations with relative "
+                      f"error {i.relres} ({_lib.STOP_NAMES.get(i.status, i.status)}).")
+        x = X.T.reshape(b.shape)
+        return x
+
+    # one-shot device operations used by the parity tests
+    def ldlsolve(self, r, precision="fp64"):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        y = np.empty_like(r)
+        check(lib().acg_ldlsolve(self._h, r, y, _PRECISIONS[precision]))
+        return y
+
+    def time_kernels(self, precision="fp64", reps=20) -> dict:
+        t = _lib.AcgKernelTimes()
+        check(lib().acg_time_kernels(self._h, _PRECISIONS[precision], int(reps), ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in _lib.AcgKernelTimes._fields_}
+
+    def lap_mul(self, x, precision="fp64"):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        check(lib().acg_lap_mul(self._h, x, y, _PRECISIONS[precision]))
+        return y
+
+
+def null_solver(b, **kw):
+    """`nullSolver` (src/solverInterface.jl:69-72): zeros."""
+    return np.zeros_like(np.asarray(b, dtype=np.float64))
+
+
+class _DenseGroundedSolver:
+    """`lapWrapConnected(chol_sddm, a)` (src/solverInterface.jl:113-142) for a
+    component with fewer than 50 vertices, as the reference does: drop the
+    vertex of largest degree, Cholesky-solve the rest, centre the result."""
+
+    def __init__(self, a):
+        la = lap(a).toarray()
+        self.N = la.shape[0]
+        ind = int(np.argmax(np.diag(la)))
+        self.leave = np.array([i for i in range(self.N) if i != ind], dtype=np.int64)
+        sub = la[np.ix_(self.leave, self.leave)]
+        self.chol = np.linalg.cholesky(sub)
+
+    def __call__(self, b, **kw):
+        b = np.asarray(b, dtype=np.float64)
+        bs = b[self.leave] - b.mean()
+        y = np.linalg.solve(self.chol, bs)
+        xs = np.linalg.solve(self.chol.T, y)
+        x = np.zeros(self.N)
+        x[self.leave] = xs
+        return x - x.mean()
+
+
+class _BlockSolver:
+    """`blockSolver` (src/solverInterface.jl:152-188): one solver per component."""
+
+    def __init__(self, comps, solvers, defaults):
+        self.comps = comps
+        self.solvers = solvers
+        self.defaults = defaults
+
+    def __call__(self, b, tol=None, maxits=None, maxtime=None, verbose=None, pcgIts=None, precision=None):
+        d = self.defaults
+        kw = dict(tol=d["tol"] if tol is None else tol, maxits=d["maxits"] if maxits is None else maxits,
+                  maxtime=d["maxtime"] if maxtime is None else maxtime,
+                  verbose=d["verbose"] if verbose is None else verbose)
+        if precision is not None:
+            kw["precision"] = precision
+        pcgIts = d["pcgIts"] if pcgIts is None else pcgIts
+        if pcgIts is not None and len(pcgIts) > 0:
+            pcgIts[0] = 0
+            tmp = [0]
+        else:
+            tmp = []
+        b = np.asarray(b, dtype=np.float64)
+        x = np.zeros(b.shape)
+        for ind, s in zip(self.comps, self.solvers):
+            if isinstance(s, DeviceLapSolver):
+                x[ind] = s(b[ind], pcgIts=tmp, **kw)
+            else:
+                x[ind] = s(b[ind])
+            if pcgIts is not None and len(pcgIts) > 0:
+                pcgIts[0] = max(pcgIts[0], tmp[0] if tmp else 0)
+        return x
+
+
+def approxchol_lap1(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False, pcgIts=None,
+                    params: ApproxCholParams | None = None, precision="fp64", options=None):
+    """Dispatch on params.order (src/approxChol.jl:1791-1851); the :deg order is
+    approxchol_lapGreedy (src/approxChol.jl:1581-1626)."""
+    params = params or ApproxCholParams()
+    if params.order != "deg":
+        raise NotImplementedError(f"order {params.order!r}: only the default :deg elimination is built")
+    if params.split >= 1:
+        raise NotImplementedError("split/merge elimination (approxchol_lap2) is not built")
+    t1 = time.time()
+    ldli = approx_chol(a)
+    s = DeviceLapSolver(a, ldli, tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts,
+                        params=params, precision=precision, options=options)
+    if verbose:
+        a = _csc(a)
+        dg = np.asarray(a.sum(axis=0)).ravel()
+        print("Using greedy degree ordering. Factorization time: ", time.time() - t1)
+        print(f"Factorization size: {2 * ldli.nnz}")
+        print("Ratio of operator edges to original edges: ", 2 * ldli.nnz / a.nnz)
+        print("ratio of max to min diagonal of laplacian : ", dg.max() / dg.min())
+    return s
+
+
+def approxchol_lap(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False, pcgIts=None,
+                   params: ApproxCholParams | None = None, precision="fp64", options=None):
+    """`approxchol_lap` (src/approxChol.jl:1522-1545) through `lapWrapComponents`
+    (src/solverInterface.jl:212-275)."""
+    a = _csc(a)
+    if a.nnz and a.data.min() < 0:
+        raise ValueError("Adjacency matrix can not have negative edge weights")
+    if a.diagonal().any():
+        import warnings
+        warnings.warn("The matrix should not have any nonzero diagonal entries.")
+        a = _csc(a - sp.diags(a.diagonal()))
+        a.eliminate_zeros()
+    kw = dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts, params=params,
+              precision=precision, options=options)
+    co = components(a)
+    if co.max() == 1:
+        return approxchol_lap1(a, **kw)
+    comps = vec_to_comps(co)
+    solvers = []
+    sizes = np.array([len(c) for c in comps])
+    null_idx = np.where(sizes == 1)[0]
+    if null_idx.size:
+        flat = np.concatenate([comps[i] for i in null_idx])
+        comps = [flat] + [c for i, c in enumerate(comps) if sizes[i] != 1]
+        solvers.append(null_solver)
+        rest = comps[1:]
+    else:
+        rest = comps
+    for ind in rest:
+        asub = a[ind][:, ind]
+        if len(ind) < 50:
+            solvers.append(_DenseGroundedSolver(asub))
+        else:
+            solvers.append(approxchol_lap1(asub, **kw))
+    return _BlockSolver(comps, solvers, dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose,
+                                             pcgIts=pcgIts))
+
+
+_seed_from_entropy_done = False
+
+
+def _init():
+    global _seed_from_entropy_done
+    if not _seed_from_entropy_done:
+        try:
+            _seed_from_entropy()
+        except ImportError:
+            pass
+        _seed_from_entropy_done = True

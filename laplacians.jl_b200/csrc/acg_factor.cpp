@@ -1,0 +1,370 @@
+// Host-side randomized approximate Cholesky elimination (the `:deg` order).
+//
+// This produces the LDLinv factor that the GPU solve applies.  It restates
+// the reference's elimination step by step so that, from the same seeded
+// random stream, it makes the same choices:
+//   LLmatp(a)              src/approxChol.jl:102-136   (linked columns)
+//   flipIndex(a)           src/graphUtils.jl:49-55     (reverse edge index)
+//   get_ll_col             src/approxChol.jl:354-385
+//   compressCol!           src/approxChol.jl:415-449
+//   approxChol(::LLmatp)   src/approxChol.jl:864-977
+//   ApproxCholPQ & ops     src/approxChol.jl:2085-2239
+// The two sorts inside compressCol! are Julia 1.8's `QuickSort` (Base.Sort:
+// median-of-three pivot, insertion sort at <= 20 elements); equal keys are
+// ordered by that algorithm, so it is restated here rather than replaced by
+// std::sort.  `searchsortedfirst` (src/approxChol.jl:918) is a plain lower
+// bound on a strictly increasing cumulative sum.
+//
+// Memory: edge records are struct-of-arrays indexed by CSC position, so the
+// working set is 32 bytes per stored adjacency entry plus O(n).
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "acg_internal.h"
+#include "acg_rng.h"
+
+namespace acg {
+
+namespace {
+
+// Edge records of the linked-column matrix (LLp in src/approxCholTypes.jl:14-23).
+struct LinkedCols {
+  int64_t n = 0;
+  std::vector<int64_t> row;   // 1-based vertex id of the row
+  std::vector<double> val;    // weight; 0 marks a removed edge
+  std::vector<int64_t> next;  // next record in the column; self terminates
+  std::vector<int64_t> rev;   // record of the same edge in the other column
+  std::vector<int64_t> head;  // head[v] (v 1-based) = first record of column v
+  std::vector<int64_t> degs;  // initial degrees (1-based)
+};
+
+// Approximate priority queue on degrees (ApproxCholPQ, split = 1).
+struct DegreeQueue {
+  int64_t n = 0;
+  int64_t minlist = 1;
+  int64_t nitems = 0;
+  std::vector<int64_t> prev, next, key;  // indexed by 1-based vertex id; 0 = none
+  std::vector<int64_t> lists;            // indexed 1..2n+1
+
+  int64_t key_map(int64_t x) const {
+    const int64_t k = n, upper = 2 * n + 1;
+    if (x <= k) return x;
+    int64_t m = k + x / k;
+    return m < upper ? m : upper;
+  }
+
+  void init(const std::vector<int64_t>& degs, int64_t nv) {
+    n = nv;
+    prev.assign(n + 1, 0);
+    next.assign(n + 1, 0);
+    key.assign(n + 1, 0);
+    lists.assign(2 * n + 2, 0);
+    minlist = 1;
+    nitems = n;
+    for (int64_t i = 1; i <= n; ++i) {
+      int64_t k = degs[i];
+      if (k < 1 || k > 2 * n + 1) throw std::runtime_error("vertex degree out of queue range");
+      int64_t h = lists[k];
+      if (h > 0) {
+        prev[i] = 0; next[i] = h; key[i] = k;
+        prev[h] = i;  // next[h], key[h] unchanged
+      } else {
+        prev[i] = 0; next[i] = 0; key[i] = k;
+      }
+      lists[k] = i;
+    }
+  }
+
+  int64_t pop() {
+    if (nitems == 0) throw std::runtime_error("ApproxPQ is empty");
+    while (lists[minlist] == 0) ++minlist;
+    int64_t i = lists[minlist];
+    int64_t nx = next[i];
+    lists[minlist] = nx;
+    if (nx > 0) prev[nx] = 0;
+    --nitems;
+    return i;
+  }
+
+  void move(int64_t i, int64_t newkey, int64_t oldlist, int64_t newlist) {
+    int64_t pv = prev[i], nx = next[i];
+    if (nx > 0) prev[nx] = pv;
+    if (pv > 0) next[pv] = nx; else lists[oldlist] = nx;
+    int64_t h = lists[newlist];
+    if (h > 0) prev[h] = i;
+    lists[newlist] = i;
+    prev[i] = 0; next[i] = h; key[i] = newkey;
+  }
+
+  void dec(int64_t i) {
+    int64_t oldlist = key_map(key[i]);
+    int64_t newlist = key_map(key[i] - 1);
+    if (newlist < 1) throw std::runtime_error("degree queue key underflow");
+    if (newlist != oldlist) {
+      move(i, key[i] - 1, oldlist, newlist);
+      if (newlist < minlist) minlist = newlist;
+    } else {
+      key[i] -= 1;
+    }
+  }
+
+  void inc(int64_t i) {
+    int64_t oldlist = key_map(key[i]);
+    int64_t newlist = key_map(key[i] + 1);
+    if (newlist > 2 * n + 1) throw std::runtime_error("degree queue key overflow");
+    if (newlist != oldlist) {
+      move(i, key[i] + 1, oldlist, newlist);
+    } else {
+      key[i] += 1;
+    }
+  }
+};
+
+// Julia 1.8 Base.Sort QuickSort on v[lo..hi] (inclusive, 0-based) with a
+// strict-weak "less" on the element handles.
+template <class Less>
+void julia_insertion_sort(int64_t* v, int64_t lo, int64_t hi, const Less& lt) {
+  for (int64_t i = lo + 1; i <= hi; ++i) {
+    int64_t j = i;
+    int64_t x = v[i];
+    while (j > lo) {
+      if (lt(x, v[j - 1])) {
+        v[j] = v[j - 1];
+        --j;
+        continue;
+      }
+      break;
+    }
+    v[j] = x;
+  }
+}
+
+template <class Less>
+int64_t julia_partition(int64_t* v, int64_t lo, int64_t hi, const Less& lt) {
+  // selectpivot!: order v[mi] <= v[lo] <= v[hi]; the pivot ends in v[lo].
+  int64_t mi = lo + ((hi - lo) >> 1);
+  if (lt(v[lo], v[mi])) std::swap(v[mi], v[lo]);
+  if (lt(v[hi], v[lo])) {
+    if (lt(v[hi], v[mi])) {
+      int64_t a = v[lo], b = v[mi], c = v[hi];
+      v[hi] = a; v[lo] = b; v[mi] = c;
+    } else {
+      std::swap(v[hi], v[lo]);
+    }
+  }
+  int64_t pivot = v[lo];
+  int64_t i = lo, j = hi;
+  while (true) {
+    ++i; --j;
+    while (lt(v[i], pivot)) ++i;
+    while (lt(pivot, v[j])) --j;
+    if (i >= j) break;
+    std::swap(v[i], v[j]);
+  }
+  v[lo] = v[j];
+  v[j] = pivot;
+  return j;
+}
+
+template <class Less>
+void julia_quicksort(int64_t* v, int64_t lo, int64_t hi, const Less& lt) {
+  while (lo < hi) {
+    if (hi - lo <= 20) {
+      julia_insertion_sort(v, lo, hi, lt);
+      return;
+    }
+    int64_t j = julia_partition(v, lo, hi, lt);
+    if (j - lo < hi - j) {
+      if (lo < j - 1) julia_quicksort(v, lo, j - 1, lt);
+      lo = j + 1;
+    } else {
+      if (j + 1 < hi) julia_quicksort(v, j + 1, hi, lt);
+      hi = j - 1;
+    }
+  }
+}
+
+void build_linked_cols(int64_t n, const int64_t* colptr, const int64_t* rowval,
+                       const double* nzval, LinkedCols& ll) {
+  const int64_t m = colptr[n] - colptr[0];
+  ll.n = n;
+  ll.row.resize(m);
+  ll.val.resize(m);
+  ll.next.resize(m);
+  ll.rev.resize(m);
+  ll.head.assign(n + 1, -1);
+  ll.degs.assign(n + 1, 0);
+  const int64_t base = colptr[0];
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t p0 = colptr[i] - base, p1 = colptr[i + 1] - base;
+    ll.degs[i + 1] = p1 - p0;
+    if (p1 <= p0) throw std::runtime_error("vertex " + std::to_string(i + 1) + " has no edges");
+    ll.row[p0] = rowval[p0];
+    ll.val[p0] = nzval[p0];
+    ll.next[p0] = p0;
+    int64_t prevrec = p0;
+    for (int64_t p = p0 + 1; p < p1; ++p) {
+      ll.row[p] = rowval[p];
+      ll.val[p] = nzval[p];
+      ll.next[p] = prevrec;
+      prevrec = p;
+    }
+    ll.head[i + 1] = prevrec;
+  }
+  // flipIndex: with rows sorted in every column and a symmetric pattern, the
+  // records (row c, col r) are met in increasing c while scanning columns c.
+  std::vector<int64_t> cursor(n, 0);
+  for (int64_t c = 0; c < n; ++c) {
+    for (int64_t p = colptr[c] - base; p < colptr[c + 1] - base; ++p) {
+      int64_t r = rowval[p] - 1;
+      int64_t q = colptr[r] - base + cursor[r]++;
+      if (q >= colptr[r + 1] - base || rowval[q] != c + 1)
+        throw std::runtime_error("adjacency matrix is not structurally symmetric with sorted rows");
+      ll.rev[p] = q;
+    }
+  }
+}
+
+}  // namespace
+
+void approx_chol_deg(int64_t n, const int64_t* colptr, const int64_t* rowval,
+                     const double* nzval, JuliaRng* rng, HostFactor& out) {
+  if (n < 2) throw std::runtime_error("approxChol needs at least 2 vertices");
+  LinkedCols a;
+  build_linked_cols(n, colptr, rowval, nzval, a);
+
+  out.n = n;
+  out.col.assign(n - 1, 0);
+  out.colptr.assign(n, 0);
+  out.rowval.clear();
+  out.fval.clear();
+  out.rowval.reserve((size_t)(a.row.size() * 0.6) + 16);
+  out.fval.reserve((size_t)(a.row.size() * 0.6) + 16);
+  out.d.assign(n, 0.0);
+
+  DegreeQueue pq;
+  pq.init(a.degs, n);
+
+  std::vector<int64_t> colspace(n);
+  std::vector<double> cumspace(n), vals(n);
+
+  int64_t it = 1;  // 1-based elimination step, as in the reference
+  int64_t ldli_row_ptr = 1;
+
+  auto by_row = [&](int64_t x, int64_t y) { return a.row[x] < a.row[y]; };
+  auto by_val = [&](int64_t x, int64_t y) { return a.val[x] < a.val[y]; };
+
+  while (it < n) {
+    int64_t i = pq.pop();
+    out.col[it - 1] = i;
+    out.colptr[it - 1] = ldli_row_ptr;
+    ++it;
+
+    // get_ll_col: walk the column, keep live records.
+    int64_t len = 0;
+    int64_t rec = a.head[i];
+    while (true) {
+      if (a.val[rec] > 0.0) {
+        if (len >= (int64_t)colspace.size()) colspace.resize(2 * colspace.size() + 1);
+        colspace[len++] = rec;
+      }
+      if (a.next[rec] == rec) break;
+      rec = a.next[rec];
+    }
+    if (len == 0) throw std::runtime_error("eliminated vertex has no live edges (graph disconnected?)");
+
+    // compressCol!: merge parallel edges, then order by weight.
+    julia_quicksort(colspace.data(), 0, len - 1, by_row);
+    int64_t ptr = -1;
+    int64_t currow = 0;
+    for (int64_t k = 0; k < len; ++k) {
+      int64_t ck = colspace[k];
+      if (a.row[ck] != currow) {
+        currow = a.row[ck];
+        ++ptr;
+        colspace[ptr] = ck;
+      } else {
+        int64_t cp = colspace[ptr];
+        a.val[cp] = a.val[cp] + a.val[ck];
+        a.val[a.rev[ck]] = 0.0;
+        pq.dec(currow);
+      }
+    }
+    len = ptr + 1;
+    julia_quicksort(colspace.data(), 0, len - 1, by_val);
+
+    if ((int64_t)cumspace.size() < len) {
+      cumspace.resize(len);
+      vals.resize(len);
+    }
+    double csum = 0.0;
+    for (int64_t k = 0; k < len; ++k) {
+      vals[k] = a.val[colspace[k]];
+      csum = csum + a.val[colspace[k]];
+      cumspace[k] = csum;
+    }
+    double wdeg = csum;
+    double colScale = 1.0;
+
+    for (int64_t jo = 0; jo < len - 1; ++jo) {
+      int64_t llr = colspace[jo];
+      double w = vals[jo] * colScale;
+      int64_t j = a.row[llr];
+      int64_t revj = a.rev[llr];
+      double f = w / wdeg;
+      vals[jo] = 0.0;
+
+      double r = julia_rand(rng) * (csum - cumspace[jo]) + cumspace[jo];
+      // searchsortedfirst(cumspace, r, jo.., len): first index with cumspace >= r
+      int64_t lo = -1, hi = len;  // over the full 1..len range like the reference
+      while (lo < hi - 1) {
+        int64_t mid = lo + ((hi - lo) >> 1);
+        if (cumspace[mid] < r) lo = mid; else hi = mid;
+      }
+      int64_t koff = hi < len ? hi : len - 1;  // r can only exceed csum by rounding
+      int64_t k = a.row[colspace[koff]];
+
+      pq.inc(k);
+
+      double newEdgeVal = f * (1.0 - f) * wdeg;
+
+      // fix row k in col j
+      a.row[revj] = k;
+      a.val[revj] = newEdgeVal;
+      a.rev[revj] = llr;
+
+      // fix row j in col k
+      int64_t khead = a.head[k];
+      a.head[k] = llr;
+      a.next[llr] = khead;
+      a.rev[llr] = revj;
+      a.val[llr] = newEdgeVal;
+      a.row[llr] = j;
+
+      colScale = colScale * (1.0 - f);
+      double omf = 1.0 - f;
+      wdeg = wdeg * (omf * omf);
+
+      out.rowval.push_back(j);
+      out.fval.push_back(f);
+      ++ldli_row_ptr;
+    }
+
+    int64_t llr = colspace[len - 1];
+    double w = vals[len - 1] * colScale;
+    int64_t j = a.row[llr];
+    int64_t revj = a.rev[llr];
+    if (it < n) pq.dec(j);
+    a.val[revj] = 0.0;
+    out.rowval.push_back(j);
+    out.fval.push_back(1.0);
+    ++ldli_row_ptr;
+    out.d[i - 1] = w;
+  }
+  out.colptr[it - 1] = ldli_row_ptr;
+}
+
+}  // namespace acg

@@ -1,0 +1,140 @@
+// C-ABI entry points that run on the host only: the Julia-compatible random
+// stream and the approximate Cholesky elimination.  See include/acgpu.h.
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "../../include/acgpu.h"
+#include "acg_internal.h"
+
+struct acg_factor {
+  acg::HostFactor f;
+};
+
+namespace acg {
+namespace {
+thread_local std::string g_last_error;
+}
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace acg
+
+extern "C" {
+
+const char* acg_last_error(void) { return acg::g_last_error.c_str(); }
+
+int acg_rng_seed(uint64_t seed, uint64_t state[4]) {
+  if (!state) {
+    acg::set_last_error("acg_rng_seed: null state");
+    return ACG_ERR_INVALID;
+  }
+  acg::JuliaRng r;
+  acg::julia_seed(&r, seed);
+  std::memcpy(state, r.s, sizeof(r.s));
+  return ACG_OK;
+}
+
+int acg_rng_rand(uint64_t state[4], double* out, int64_t count) {
+  if (!state || (!out && count > 0) || count < 0) {
+    acg::set_last_error("acg_rng_rand: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  acg::JuliaRng r;
+  std::memcpy(r.s, state, sizeof(r.s));
+  for (int64_t k = 0; k < count; ++k) out[k] = acg::julia_rand(&r);
+  std::memcpy(state, r.s, sizeof(r.s));
+  return ACG_OK;
+}
+
+int acg_sha256(const uint8_t* data, int64_t len, uint8_t out[32]) {
+  if ((!data && len > 0) || len < 0 || !out) {
+    acg::set_last_error("acg_sha256: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  acg::sha256(data, (size_t)len, out);
+  return ACG_OK;
+}
+
+int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                   uint64_t rng_state[4], acg_factor** out) {
+  if (!out || !colptr || !rowval || !nzval || !rng_state || n < 2) {
+    acg::set_last_error("acg_approxchol: bad arguments (need n >= 2 and non-null arrays)");
+    return ACG_ERR_INVALID;
+  }
+  *out = nullptr;
+  const int64_t base = colptr[0];
+  if (base != 0 && base != 1) {
+    acg::set_last_error("acg_approxchol: colptr[0] must be 0 or 1");
+    return ACG_ERR_INVALID;
+  }
+  try {
+    const int64_t m = colptr[n] - base;
+    for (int64_t p = 0; p < m; ++p) {
+      if (!(nzval[p] >= 0.0)) {
+        acg::set_last_error("Adjacency matrix can not have negative edge weights");
+        return ACG_ERR_INVALID;
+      }
+    }
+    // The elimination works on 1-based rows like the reference; shift 0-based input.
+    const int64_t* rv = rowval;
+    std::vector<int64_t> shifted;
+    if (base == 0) {
+      shifted.resize(m);
+      for (int64_t p = 0; p < m; ++p) shifted[p] = rowval[p] + 1;
+      rv = shifted.data();
+    }
+    for (int64_t p = 0; p < m; ++p) {
+      if (rv[p] < 1 || rv[p] > n) {
+        acg::set_last_error("acg_approxchol: row index out of range");
+        return ACG_ERR_INVALID;
+      }
+    }
+    acg::JuliaRng r;
+    std::memcpy(r.s, rng_state, sizeof(r.s));
+    auto* fac = new acg_factor();
+    try {
+      acg::approx_chol_deg(n, colptr, rv, nzval, &r, fac->f);
+    } catch (...) {
+      delete fac;
+      throw;
+    }
+    std::memcpy(rng_state, r.s, sizeof(r.s));
+    *out = fac;
+    return ACG_OK;
+  } catch (const std::bad_alloc&) {
+    acg::set_last_error("acg_approxchol: host out of memory");
+    return ACG_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    acg::set_last_error(std::string("acg_approxchol: ") + e.what());
+    return ACG_ERR_INVALID;
+  }
+}
+
+int acg_factor_dims(const acg_factor* f, int64_t* n, int64_t* nnz) {
+  if (!f || !n || !nnz) {
+    acg::set_last_error("acg_factor_dims: null argument");
+    return ACG_ERR_INVALID;
+  }
+  *n = f->f.n;
+  *nnz = (int64_t)f->f.fval.size();
+  return ACG_OK;
+}
+
+int acg_factor_export(const acg_factor* f, int64_t* col, int64_t* colptr, int64_t* rowval,
+                      double* fval, double* d) {
+  if (!f || !col || !colptr || !rowval || !fval || !d) {
+    acg::set_last_error("acg_factor_export: null argument");
+    return ACG_ERR_INVALID;
+  }
+  const acg::HostFactor& h = f->f;
+  std::memcpy(col, h.col.data(), sizeof(int64_t) * h.col.size());
+  std::memcpy(colptr, h.colptr.data(), sizeof(int64_t) * h.colptr.size());
+  std::memcpy(rowval, h.rowval.data(), sizeof(int64_t) * h.rowval.size());
+  std::memcpy(fval, h.fval.data(), sizeof(double) * h.fval.size());
+  std::memcpy(d, h.d.data(), sizeof(double) * h.d.size());
+  return ACG_OK;
+}
+
+void acg_factor_free(acg_factor* f) { delete f; }
+
+}  // extern "C"

@@ -1,0 +1,26 @@
+// Internal host-side types shared by the C-ABI translation units.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "acg_rng.h"
+
+namespace acg {
+
+// The LDLinv factor as the reference stores it (src/approxCholTypes.jl:73-79):
+// 1-based vertex ids, col[ii] = vertex eliminated at step ii (n-1 of them),
+// colptr (n entries, colptr[n-1] = F+1), rowval/fval (F), d (n, by vertex).
+struct HostFactor {
+  int64_t n = 0;
+  std::vector<int64_t> col, colptr, rowval;
+  std::vector<double> fval, d;
+};
+
+void approx_chol_deg(int64_t n, const int64_t* colptr, const int64_t* rowval,
+                     const double* nzval, JuliaRng* rng, HostFactor& out);
+
+// Thread-local error text returned by acg_last_error().
+void set_last_error(const std::string& msg);
+
+}  // namespace acg

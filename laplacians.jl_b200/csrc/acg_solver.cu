@@ -1,0 +1,919 @@
+// Device-resident solver: upload of a graph + LDLinv factor, and the solve
+// (FP64 PCG, or FP32 PCG inside FP64 iterative refinement) as one CUDA graph
+// whose PCG loop is a conditional WHILE node, so a whole solve is one graph
+// launch with no host round trip per iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/acgpu.h"
+#include "acg_internal.h"
+#include "acg_pcg.cuh"
+
+namespace acg {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct InputError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct DeviceNoMem : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define ACG_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::acg::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + \
+                             __FILE__ + ":" + std::to_string(__LINE__));                    \
+  } while (0)
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    free();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      p = nullptr;
+      throw DeviceNoMem("device allocation of " + std::to_string(count * sizeof(T)) + " bytes failed");
+    }
+    ACG_CUDA(e);
+    n = count;
+  }
+  void upload(const std::vector<T>& h, cudaStream_t s) {
+    alloc(h.size());
+    if (!h.empty()) ACG_CUDA(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// One step of a sweep plan: a single wide level (grid launch) or a run of
+// thin levels executed by one CTA.
+struct SweepStep {
+  int thin;
+  int l0, l1;  // levels [l0, l1)
+  int v0, v1;  // vertex range of the levels
+};
+
+struct SolverImpl {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int n = 0;
+  int64_t nnz_l = 0, nnz_f = 0;
+  int nlev = 0;
+  int vl_sweep = 8, vl_spmv = 8;
+  int wide_min = 2048;
+  std::vector<int> lvl_off;  // host copy
+  std::vector<SweepStep> plan;
+
+  DevBuf<int> perm, lvl_off_d;
+  DevBuf<int> l_ptr, l_idx, f_ptr, f_idx, b_ptr, b_idx;
+  DevBuf<double> l_v64, f_c64, b_c64, g64;
+  DevBuf<float> l_v32, f_c32, b_c32, g32;
+
+  // work vectors
+  DevBuf<double> b_ext, x_ext, bm, r64, y64, p64, q64, x3_64, xf;
+  DevBuf<float> r32, y32, p32, q32, x3_32;
+  DevBuf<double> partials;
+  PcgState* st = nullptr;    // device
+  PcgState* h_st = nullptr;  // pinned host mirror
+
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  std::mutex mu;
+
+  ~SolverImpl() {
+    for (auto& e : exec)
+      if (e) cudaGraphExecDestroy(e);
+    if (st) cudaFree(st);
+    if (h_st) cudaFreeHost(h_st);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int choose_vl(double avg) {
+  if (avg <= 2.5) return 2;
+  if (avg <= 5.0) return 4;
+  if (avg <= 12.0) return 8;
+  return 16;
+}
+
+// ---- kernel launch helpers (runtime VL -> template) -----------------------
+
+template <typename T>
+struct TypedArrays {
+  const int *fp, *fi, *bp, *bi, *lp, *li;
+  const T *fc, *bc, *g, *lv;
+};
+
+template <typename T>
+TypedArrays<T> arrays_of(const SolverImpl& S);
+template <>
+TypedArrays<double> arrays_of<double>(const SolverImpl& S) {
+  return {S.f_ptr.p, S.f_idx.p, S.b_ptr.p, S.b_idx.p, S.l_ptr.p, S.l_idx.p, S.f_c64.p, S.b_c64.p, S.g64.p, S.l_v64.p};
+}
+template <>
+TypedArrays<float> arrays_of<float>(const SolverImpl& S) {
+  return {S.f_ptr.p, S.f_idx.p, S.b_ptr.p, S.b_idx.p, S.l_ptr.p, S.l_idx.p, S.f_c32.p, S.b_c32.p, S.g32.p, S.l_v32.p};
+}
+
+#define ACG_VL_SWITCH(vl, FN, ...)                   \
+  switch (vl) {                                      \
+    case 2: FN<T, 2>(__VA_ARGS__); break;            \
+    case 4: FN<T, 4>(__VA_ARGS__); break;            \
+    case 8: FN<T, 8>(__VA_ARGS__); break;            \
+    default: FN<T, 16>(__VA_ARGS__); break;          \
+  }
+
+template <typename T, int VL>
+void thin_fwd_vl(cudaStream_t s, const SweepStep& st_, const int* lo, const TypedArrays<T>& A, const T* r, T* y,
+                 const PcgState* st) {
+  k_fwd_thin<T, VL><<<1, kThinThreads, 0, s>>>(st_.l0, st_.l1, lo, A.fp, A.fi, A.fc, r, y, st);
+}
+template <typename T, int VL>
+void thin_bwd_vl(cudaStream_t s, const SweepStep& st_, const int* lo, const TypedArrays<T>& A, T* y, const PcgState* st) {
+  k_bwd_thin<T, VL><<<1, kThinThreads, 0, s>>>(st_.l0, st_.l1, lo, A.bp, A.bi, A.bc, A.g, y, st);
+}
+template <typename T, int VL>
+void wide_fwd_vl(cudaStream_t s, const SweepStep& st_, const TypedArrays<T>& A, const T* r, T* y, const PcgState* st) {
+  const long long threads = (long long)(st_.v1 - st_.v0) * VL;
+  k_fwd_level<T, VL><<<(int)((threads + 255) / 256), 256, 0, s>>>(st_.v0, st_.v1, A.fp, A.fi, A.fc, r, y, st);
+}
+template <typename T, int VL>
+void wide_bwd_vl(cudaStream_t s, const SweepStep& st_, const TypedArrays<T>& A, T* y, const PcgState* st) {
+  const long long threads = (long long)(st_.v1 - st_.v0) * VL;
+  k_bwd_level<T, VL><<<(int)((threads + 255) / 256), 256, 0, s>>>(st_.v0, st_.v1, A.bp, A.bi, A.bc, A.g, y, st);
+}
+
+// Forward sweep: y = s (forward values) of r.
+template <typename T>
+void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* y, const PcgState* st) {
+  const TypedArrays<T> A = arrays_of<T>(S);
+  const int vl = S.vl_sweep;
+  for (const SweepStep& step : S.plan) {
+    if (step.thin) {
+      ACG_VL_SWITCH(vl, thin_fwd_vl, s, step, S.lvl_off_d.p, A, r, y, st);
+    } else {
+      ACG_VL_SWITCH(vl, wide_fwd_vl, s, step, A, r, y, st);
+    }
+  }
+}
+// Backward sweep, in place on the forward values.
+template <typename T>
+void enqueue_backward(cudaStream_t s, const SolverImpl& S, T* y, const PcgState* st) {
+  const TypedArrays<T> A = arrays_of<T>(S);
+  const int vl = S.vl_sweep;
+  for (auto it = S.plan.rbegin(); it != S.plan.rend(); ++it) {
+    const SweepStep& step = *it;
+    if (step.thin) {
+      ACG_VL_SWITCH(vl, thin_bwd_vl, s, step, S.lvl_off_d.p, A, y, st);
+    } else {
+      ACG_VL_SWITCH(vl, wide_bwd_vl, s, step, A, y, st);
+    }
+  }
+}
+// y = (forward, then backward) LDLinv sweeps of r; y is also the forward scratch.
+template <typename T>
+void enqueue_sweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* y, const PcgState* st) {
+  enqueue_forward<T>(s, S, r, y, st);
+  enqueue_backward<T>(s, S, y, st);
+}
+
+template <typename T, int VL>
+void spmv_pq_vl(cudaStream_t s, const SolverImpl& S, const TypedArrays<T>& A, const T* p, T* q, PcgState* st,
+                double eps, LoopCtl ctl) {
+  k_spmv_pq<T, VL><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, A.lp, A.li, A.lv, p, q, st, S.partials.p, eps, ctl);
+}
+template <typename T, int VL>
+void true_res_vl(cudaStream_t s, const SolverImpl& S, const double* x, const double* bm, double* rout, PcgState* st) {
+  k_true_residual<VL><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, S.l_ptr.p, S.l_idx.p, S.l_v64.p, x, bm, rout, st,
+                                                          S.partials.p);
+}
+
+// The body of one PCG iteration on vectors of type T.
+template <typename T>
+void enqueue_pcg_iteration(cudaStream_t s, const SolverImpl& S, T* r, T* y, T* p, T* q, T* x3, double eps, LoopCtl ctl) {
+  const TypedArrays<T> A = arrays_of<T>(S);
+  ACG_VL_SWITCH(S.vl_spmv, spmv_pq_vl, s, S, A, p, q, S.st, eps, ctl);
+  k_update<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, x3, p, q, r, S.st, S.partials.p, ctl);
+  enqueue_sweeps<T>(s, S, r, y, S.st);
+  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p);
+  k_zdot<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, r, p, S.st, S.partials.p, eps, 0, ctl);
+  k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, p, S.st);
+}
+
+// ---- graph construction -----------------------------------------------------
+
+// Current leaf nodes of a capture in progress.
+std::vector<cudaGraphNode_t> capture_leaves(cudaStream_t s) {
+  cudaStreamCaptureStatus status;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  ACG_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, nullptr, &deps, &ndeps));
+  return std::vector<cudaGraphNode_t>(deps, deps + ndeps);
+}
+
+cudaGraphNode_t add_while(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, cudaGraphConditionalHandle h,
+                          cudaGraph_t* body) {
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  ACG_CUDA(cudaGraphAddNode(&node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &cp));
+  *body = cp.conditional.phGraph_out[0];
+  return node;
+}
+
+void begin_into(cudaStream_t s, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps) {
+  ACG_CUDA(cudaStreamBeginCaptureToGraph(s, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                         cudaStreamCaptureModeThreadLocal));
+}
+void end_into(cudaStream_t s) {
+  cudaGraph_t g;
+  ACG_CUDA(cudaStreamEndCapture(s, &g));
+}
+
+// Plain FP64 PCG, the reference algorithm end to end.
+cudaGraphExec_t build_fp64_graph(SolverImpl& S) {
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  cudaGraph_t top;
+  ACG_CUDA(cudaGraphCreate(&top, 0));
+  cudaGraphConditionalHandle h;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&h, top, 1u, cudaGraphCondAssignDefault));
+  LoopCtl ctl{h, 1};
+
+  begin_into(s, top, {});
+  k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
+  k_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, S.r64.p, S.x3_64.p, S.st, S.partials.p, ctl);
+  enqueue_sweeps<double>(s, S, S.r64.p, S.y64.p, S.st);
+  k_ysum<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.st, S.partials.p);
+  k_zdot<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.r64.p, S.p64.p, S.st, S.partials.p, kEps64, 1, ctl);
+  std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
+  end_into(s);
+
+  cudaGraph_t body;
+  cudaGraphNode_t wnode = add_while(top, leaves, h, &body);
+  begin_into(s, body, {});
+  enqueue_pcg_iteration<double>(s, S, S.r64.p, S.y64.p, S.p64.p, S.q64.p, S.x3_64.p, kEps64, ctl);
+  end_into(s);
+
+  begin_into(s, top, {wnode});
+  k_take_best<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.x3_64.p, S.xf.p, S.st);
+  {
+    using T = double;
+    ACG_VL_SWITCH(S.vl_spmv, true_res_vl, s, S, S.xf.p, S.bm.p, nullptr, S.st);
+  }
+  k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
+  end_into(s);
+
+  cudaGraphExec_t exec;
+  ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
+  cudaGraphDestroy(top);
+  return exec;
+}
+
+// FP32 PCG (SpMV, sweeps, vectors) inside FP64 iterative refinement.
+cudaGraphExec_t build_mixed_graph(SolverImpl& S) {
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  const double eps32 = 1.1920928955078125e-07;
+  cudaGraph_t top;
+  ACG_CUDA(cudaGraphCreate(&top, 0));
+  cudaGraphConditionalHandle ho;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&ho, top, 1u, cudaGraphCondAssignDefault));
+  LoopCtl octl{ho, 1};
+
+  begin_into(s, top, {});
+  k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
+  // r64 = bm, x64 (xf) = 0
+  k_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, S.r64.p, S.xf.p, S.st, S.partials.p, octl);
+  std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
+  end_into(s);
+
+  cudaGraph_t obody;
+  cudaGraphNode_t onode = add_while(top, leaves, ho, &obody);
+  cudaGraphConditionalHandle hi;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&hi, obody, 1u, cudaGraphCondAssignDefault));
+  LoopCtl ictl{hi, 1};
+
+  begin_into(s, obody, {});
+  k_outer_prep<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.r64.p, S.r32.p, S.x3_32.p, S.st, S.partials.p, ictl);
+  enqueue_sweeps<float>(s, S, S.r32.p, S.y32.p, S.st);
+  k_ysum<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.st, S.partials.p);
+  k_zdot<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.r32.p, S.p32.p, S.st, S.partials.p, eps32, 2, ictl);
+  std::vector<cudaGraphNode_t> ol = capture_leaves(s);
+  end_into(s);
+
+  cudaGraph_t ibody;
+  cudaGraphNode_t inode = add_while(obody, ol, hi, &ibody);
+  begin_into(s, ibody, {});
+  enqueue_pcg_iteration<float>(s, S, S.r32.p, S.y32.p, S.p32.p, S.q32.p, S.x3_32.p, eps32, ictl);
+  end_into(s);
+
+  begin_into(s, obody, {inode});
+  k_outer_correct<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.x3_32.p, S.xf.p, S.st);
+  {
+    using T = double;
+    ACG_VL_SWITCH(S.vl_spmv, true_res_vl, s, S, S.xf.p, S.bm.p, S.r64.p, S.st);
+  }
+  k_outer_decide<<<1, 32, 0, s>>>(S.st, octl);
+  end_into(s);
+
+  begin_into(s, top, {onode});
+  k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
+  end_into(s);
+
+  cudaGraphExec_t exec;
+  ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
+  cudaGraphDestroy(top);
+  return exec;
+}
+
+}  // namespace
+}  // namespace acg
+
+// ============================================================================
+// Upload: validate the factor, level-schedule it, build device structures.
+// ============================================================================
+namespace acg {
+namespace {
+
+template <typename T>
+std::vector<float> to_f32(const std::vector<T>& v) {
+  std::vector<float> o(v.size());
+  for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
+  return o;
+}
+
+void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int64_t* a_rowval, const double* a_nzval,
+                  const int64_t* col, const int64_t* colptr, const int64_t* rowval, const double* fval,
+                  const double* d, int64_t F, int base, const acg_options* opts) {
+  if (n64 < 2 || n64 >= (int64_t)INT32_MAX) throw InputError("n must be in [2, 2^31-1)");
+  if (base != 0 && base != 1) throw InputError("index_base must be 0 or 1");
+  const int n = (int)n64;
+  S.n = n;
+  // ---- adjacency
+  const int64_t abase = a_colptr[0];
+  if (abase != 0 && abase != 1) throw InputError("adjacency colptr[0] must be 0 or 1");
+  const int64_t m = a_colptr[n] - abase;
+  if (m < 0 || m + n >= (int64_t)INT32_MAX) throw InputError("adjacency too large for 32-bit indices");
+  for (int c = 0; c < n; ++c)
+    if (a_colptr[c + 1] < a_colptr[c]) throw InputError("adjacency colptr not monotone");
+  // ---- factor validation
+  if (F < n - 1 || F >= (int64_t)INT32_MAX) throw InputError("factor size F out of range");
+  std::vector<int> step(n, -1);
+  for (int ii = 0; ii < n - 1; ++ii) {
+    int64_t u = col[ii] - base;
+    if (u < 0 || u >= n) throw InputError("ldli.col entry out of range");
+    if (step[u] != -1) throw InputError("ldli.col repeats a vertex");
+    step[u] = ii;
+  }
+  int root = -1;
+  for (int v = 0; v < n; ++v)
+    if (step[v] == -1) root = v;
+  step[root] = n - 1;
+  if (colptr[0] - base != 0) throw InputError("ldli.colptr[1] must point at the first entry");
+  for (int ii = 0; ii < n - 1; ++ii)
+    if (colptr[ii + 1] <= colptr[ii]) throw InputError("ldli column " + std::to_string(ii + 1) + " is empty");
+  if (colptr[n - 1] - base != F) throw InputError("ldli.colptr[n] must equal F+1 (1-based)");
+  // ---- levels
+  std::vector<int> lev(n, 0);
+  for (int ii = 0; ii < n - 1; ++ii) {
+    const int u = (int)(col[ii] - base);
+    for (int64_t e = colptr[ii] - base; e < colptr[ii + 1] - base; ++e) {
+      const int64_t j = rowval[e] - base;
+      if (j < 0 || j >= n) throw InputError("ldli.rowval entry out of range");
+      if (step[j] <= ii) throw InputError("ldli.rowval names a vertex eliminated earlier (not an elimination order)");
+      const double f = fval[e];
+      if (!(f >= 0.0 && f <= 1.0)) throw InputError("ldli.fval entries must lie in [0, 1]");
+      if (lev[j] < lev[u] + 1) lev[j] = lev[u] + 1;
+    }
+  }
+  for (int v = 0; v < n; ++v)
+    if (!(d[v] >= 0.0) || std::isinf(d[v])) throw InputError("ldli.d must be finite and non-negative");
+  int nlev = 0;
+  for (int v = 0; v < n; ++v) nlev = std::max(nlev, lev[v] + 1);
+  S.nlev = nlev;
+  S.lvl_off.assign(nlev + 1, 0);
+  for (int v = 0; v < n; ++v) S.lvl_off[lev[v] + 1]++;
+  for (int l = 0; l < nlev; ++l) S.lvl_off[l + 1] += S.lvl_off[l];
+  std::vector<int> perm(n), e2i(n);
+  {
+    std::vector<int> pos(S.lvl_off.begin(), S.lvl_off.end() - 1);
+    for (int t = 0; t < n; ++t) {
+      const int v = t < n - 1 ? (int)(col[t] - base) : root;
+      const int id = pos[lev[v]]++;
+      perm[id] = v;
+      e2i[v] = id;
+    }
+  }
+  // ---- folded coefficients
+  std::vector<double> coef(F);
+  std::vector<double> g(n, 1.0);
+  for (int ii = 0; ii < n - 1; ++ii) {
+    const int u = (int)(col[ii] - base);
+    const int64_t j0 = colptr[ii] - base, j1 = colptr[ii + 1] - base - 1;
+    double prod = 1.0;
+    for (int64_t e = j0; e < j1; ++e) {
+      coef[e] = fval[e] * prod;
+      prod = prod * (1.0 - fval[e]);
+    }
+    coef[j1] = prod;
+    g[u] = d[u] != 0.0 ? prod * prod / d[u] : prod * prod;
+  }
+  // forward: in-edges by internal target, in elimination order of the source
+  std::vector<int> fptr(n + 1, 0), fidx(F);
+  std::vector<double> fc(F);
+  for (int64_t e = 0; e < F; ++e) fptr[e2i[rowval[e] - base] + 1]++;
+  for (int v = 0; v < n; ++v) fptr[v + 1] += fptr[v];
+  {
+    std::vector<int> pos(fptr.begin(), fptr.end() - 1);
+    for (int ii = 0; ii < n - 1; ++ii) {
+      const int us = e2i[col[ii] - base];
+      for (int64_t e = colptr[ii] - base; e < colptr[ii + 1] - base; ++e) {
+        const int t = e2i[rowval[e] - base];
+        fidx[pos[t]] = us;
+        fc[pos[t]] = coef[e];
+        pos[t]++;
+      }
+    }
+  }
+  // backward: column entries by internal source
+  std::vector<int> bptr(n + 1, 0), bidx(F);
+  std::vector<double> bc(F), gi(n);
+  for (int v = 0; v < n; ++v) {
+    const int u = perm[v];
+    gi[v] = g[u];
+    bptr[v + 1] = bptr[v];
+    if (u == root) continue;
+    const int ii = step[u];
+    for (int64_t e = colptr[ii] - base; e < colptr[ii + 1] - base; ++e) {
+      bidx[bptr[v + 1]] = e2i[rowval[e] - base];
+      bc[bptr[v + 1]] = coef[e];
+      bptr[v + 1]++;
+    }
+  }
+  // Laplacian rows in internal order; diagonal = a*ones summed in column order
+  std::vector<int> lptr(n + 1, 0), lidx(m + n);
+  std::vector<double> lv(m + n);
+  {
+    std::vector<std::pair<int, double>> row;
+    for (int i = 0; i < n; ++i) {
+      const int u = perm[i];
+      row.clear();
+      double deg = 0.0;
+      for (int64_t k = a_colptr[u] - abase; k < a_colptr[u + 1] - abase; ++k) {
+        const int64_t c = a_rowval[k] - abase;
+        if (c < 0 || c >= n) throw InputError("adjacency row index out of range");
+        if (c == u) throw InputError("adjacency matrix has a diagonal entry");
+        const double w = a_nzval[k];
+        if (!(w >= 0.0) || std::isinf(w)) throw InputError("Adjacency matrix can not have negative edge weights");
+        deg += w;
+        row.emplace_back(e2i[c], 0.0 - w);
+      }
+      row.emplace_back(i, deg);
+      std::sort(row.begin(), row.end(),
+                [](const std::pair<int, double>& x, const std::pair<int, double>& y) { return x.first < y.first; });
+      lptr[i + 1] = lptr[i] + (int)row.size();
+      for (size_t k = 0; k < row.size(); ++k) {
+        lidx[lptr[i] + k] = row[k].first;
+        lv[lptr[i] + k] = row[k].second;
+      }
+    }
+  }
+  S.nnz_l = m + n;
+  S.nnz_f = F;
+  // ---- tuning knobs
+  S.vl_sweep = choose_vl((double)F / n);
+  S.vl_spmv = choose_vl((double)(m + n) / n);
+  S.wide_min = 2048;
+  if (opts) {
+    if (opts->sweep_lanes > 0) S.vl_sweep = opts->sweep_lanes;
+    if (opts->spmv_lanes > 0) S.vl_spmv = opts->spmv_lanes;
+    if (opts->wide_level_min > 0) S.wide_min = opts->wide_level_min;
+  }
+  for (int vl : {S.vl_sweep, S.vl_spmv})
+    if (vl != 2 && vl != 4 && vl != 8 && vl != 16) throw InputError("lane counts must be 2, 4, 8 or 16");
+  // ---- sweep plan
+  S.plan.clear();
+  for (int l = 0; l < nlev;) {
+    const int w = S.lvl_off[l + 1] - S.lvl_off[l];
+    if (w >= S.wide_min) {
+      S.plan.push_back({0, l, l + 1, S.lvl_off[l], S.lvl_off[l + 1]});
+      ++l;
+      continue;
+    }
+    int l1 = l;
+    while (l1 < nlev && l1 - l < kMaxThinLevels && S.lvl_off[l1 + 1] - S.lvl_off[l1] < S.wide_min) ++l1;
+    S.plan.push_back({1, l, l1, S.lvl_off[l], S.lvl_off[l1]});
+    l = l1;
+  }
+  // ---- upload
+  cudaStream_t s = S.stream;
+  S.perm.upload(perm, s);
+  S.lvl_off_d.upload(S.lvl_off, s);
+  S.l_ptr.upload(lptr, s);
+  S.l_idx.upload(lidx, s);
+  S.l_v64.upload(lv, s);
+  S.l_v32.upload(to_f32(lv), s);
+  S.f_ptr.upload(fptr, s);
+  S.f_idx.upload(fidx, s);
+  S.f_c64.upload(fc, s);
+  S.f_c32.upload(to_f32(fc), s);
+  S.b_ptr.upload(bptr, s);
+  S.b_idx.upload(bidx, s);
+  S.b_c64.upload(bc, s);
+  S.b_c32.upload(to_f32(bc), s);
+  S.g64.upload(gi, s);
+  S.g32.upload(to_f32(gi), s);
+  for (DevBuf<double>* b : {&S.b_ext, &S.x_ext, &S.bm, &S.r64, &S.y64, &S.p64, &S.q64, &S.xf}) b->alloc(n);
+  S.x3_64.alloc((size_t)3 * n);
+  for (DevBuf<float>* b : {&S.r32, &S.y32, &S.p32, &S.q32}) b->alloc(n);
+  S.x3_32.alloc((size_t)3 * n);
+  S.partials.alloc((size_t)4 * kMaxPartialBlocks);
+  ACG_CUDA(cudaMalloc(&S.st, sizeof(PcgState)));
+  ACG_CUDA(cudaMemsetAsync(S.st, 0, sizeof(PcgState), s));
+  ACG_CUDA(cudaMallocHost(&S.h_st, sizeof(PcgState)));
+  std::memset(S.h_st, 0, sizeof(PcgState));
+  ACG_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---- small kernels for the one-shot entry points ---------------------------
+
+template <typename T>
+__global__ void k_cast_from64(int n, const double* __restrict__ a, T* __restrict__ b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (T)a[i];
+}
+template <typename T>
+__global__ void k_minus_mean(int n, const T* __restrict__ y, const PcgState* st, double* __restrict__ out) {
+  const double mu = st->mean;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (double)y[i] - mu;
+}
+template <typename T, int VL>
+__global__ void __launch_bounds__(kVecThreads) k_spmv_plain(int n, const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                            const T* __restrict__ val, const T* __restrict__ x, double* __restrict__ y) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = gt & (VL - 1);
+  const int groups = gridDim.x * blockDim.x / VL;
+  for (int base = (gt & ~31) / VL; base < n; base += groups) {
+    const int row = base + (gt & 31) / VL;
+    const bool active = row < n;
+    T s = row_dot<T, VL>(ptr, idx, val, x, row, active, lane);
+    if (active && lane == 0) y[row] = (double)s;
+  }
+}
+template <typename T, int VL>
+void spmv_plain_vl(cudaStream_t s, const SolverImpl& S, const TypedArrays<T>& A, const T* x, double* y) {
+  k_spmv_plain<T, VL><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, A.lp, A.li, A.lv, x, y);
+}
+
+void reset_state_for_direct_use(SolverImpl& S) {
+  std::memset(S.h_st, 0, sizeof(PcgState));
+  ACG_CUDA(cudaMemcpyAsync(S.st, S.h_st, sizeof(PcgState), cudaMemcpyHostToDevice, S.stream));
+}
+
+template <typename T>
+void ldlsolve_impl(SolverImpl& S, T* rbuf, T* ybuf) {
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  reset_state_for_direct_use(S);
+  k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
+  k_cast_from64<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, rbuf);
+  enqueue_sweeps<T>(s, S, rbuf, ybuf, S.st);
+  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.partials.p);
+  k_minus_mean<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.xf.p);
+  k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
+}
+
+template <typename T>
+void lapmul_impl(SolverImpl& S, T* xbuf) {
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  reset_state_for_direct_use(S);
+  k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
+  k_cast_from64<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, xbuf);
+  const TypedArrays<T> A = arrays_of<T>(S);
+  ACG_VL_SWITCH(S.vl_spmv, spmv_plain_vl, s, S, A, xbuf, S.xf.p);
+  k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
+}
+
+
+// Device time per call of the solve's kernels, each captured `reps` times in a
+// graph and timed with CUDA events on the solver's stream (inputs: the state
+// of the last solve's vectors, or zeros).
+template <typename T>
+void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* y, T* p, T* q) {
+  cudaStream_t s = S.stream;
+  reset_state_for_direct_use(S);
+  ACG_CUDA(cudaStreamSynchronize(s));
+  const TypedArrays<T> A = arrays_of<T>(S);
+  auto time_graph = [&](auto&& body) -> double {
+    cudaGraph_t g;
+    ACG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < reps; ++i) body();
+    ACG_CUDA(cudaStreamEndCapture(s, &g));
+    cudaGraphExec_t ge;
+    ACG_CUDA(cudaGraphInstantiate(&ge, g, 0));
+    ACG_CUDA(cudaGraphLaunch(ge, s));  // warm-up
+    cudaEvent_t e0, e1;
+    ACG_CUDA(cudaEventCreate(&e0));
+    ACG_CUDA(cudaEventCreate(&e1));
+    ACG_CUDA(cudaEventRecord(e0, s));
+    ACG_CUDA(cudaGraphLaunch(ge, s));
+    ACG_CUDA(cudaEventRecord(e1, s));
+    ACG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    ACG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    return (double)ms / reps;
+  };
+  out->spmv_ms = time_graph([&]() { ACG_VL_SWITCH(S.vl_spmv, spmv_plain_vl, s, S, A, p, S.xf.p); });
+  out->forward_ms = time_graph([&]() { enqueue_forward<T>(s, S, r, y, S.st); });
+  out->backward_ms = time_graph([&]() { enqueue_backward<T>(s, S, y, S.st); });
+  out->iteration_ms = time_graph([&]() {
+    // the kernels of one PCG iteration without the stop logic taking effect
+    ACG_VL_SWITCH(S.vl_spmv, spmv_plain_vl, s, S, A, p, S.xf.p);
+    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, p, S.st, S.partials.p);
+    enqueue_sweeps<T>(s, S, r, y, S.st);
+    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p);
+    k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, q, S.st);
+  });
+  out->launches_per_iteration = 6 + 2 * (int)S.plan.size();
+  out->forward_launches = (int)S.plan.size();
+}
+
+void time_kernels(SolverImpl& S, int precision, int reps, acg_kernel_times* out) {
+  if (precision == 0) time_kernels_t<double>(S, reps, out, S.r64.p, S.y64.p, S.p64.p, S.q64.p);
+  else time_kernels_t<float>(S, reps, out, S.r32.p, S.y32.p, S.p32.p, S.q32.p);
+}
+
+int status_to_rc(int status) { return status; }
+
+int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, cudaMemcpyKind kout, double tol,
+                 int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info) {
+  cudaStream_t s = S.stream;
+  if (!S.exec[precision]) S.exec[precision] = precision == 0 ? build_fp64_graph(S) : build_mixed_graph(S);
+  PcgState& h = *S.h_st;
+  std::memset(&h, 0, sizeof(PcgState));
+  h.tol = tol;
+  h.maxtime_s = maxtime;
+  h.maxits = maxits;
+  h.stag_test = stag_test;
+  h.tol_user = tol;
+  h.maxits_user = maxits;
+  h.min_inner_tol = 1e-5;
+  h.max_outer = 40;
+  double it0 = 0.5 * tol;
+  h.inner_tol = std::min(0.25, std::max(h.min_inner_tol, it0));
+  ACG_CUDA(cudaMemcpyAsync(S.st, &h, sizeof(PcgState), cudaMemcpyHostToDevice, s));
+  ACG_CUDA(cudaMemcpyAsync(S.b_ext.p, b, sizeof(double) * S.n, kin, s));
+  cudaEvent_t e0, e1;
+  ACG_CUDA(cudaEventCreate(&e0));
+  ACG_CUDA(cudaEventCreate(&e1));
+  ACG_CUDA(cudaEventRecord(e0, s));
+  ACG_CUDA(cudaGraphLaunch(S.exec[precision], s));
+  ACG_CUDA(cudaEventRecord(e1, s));
+  ACG_CUDA(cudaMemcpyAsync(x, S.x_ext.p, sizeof(double) * S.n, kout, s));
+  ACG_CUDA(cudaMemcpyAsync(&h, S.st, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+  ACG_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (info) {
+    info->iterations = precision == 0 ? h.itcnt : h.total_its;
+    info->refinements = precision == 0 ? 0 : h.outer_its;
+    info->relres = h.nr;
+    info->best_relres = precision == 0 ? h.bestnr : h.nr_true;
+    info->true_relres = h.nr_true;
+    info->solve_ms = ms;
+    info->status = h.status;
+    info->levels = S.nlev;
+  }
+  return status_to_rc(h.status);
+}
+
+}  // namespace
+}  // namespace acg
+
+// ============================================================================
+// C ABI
+// ============================================================================
+struct acg_solver {
+  acg::SolverImpl impl;
+};
+
+namespace {
+
+template <class F>
+int guarded(const char* where, F&& fn) {
+  try {
+    return fn();
+  } catch (const acg::InputError& e) {
+    acg::set_last_error(std::string(where) + ": " + e.what());
+    return ACG_ERR_INVALID;
+  } catch (const acg::DeviceNoMem& e) {
+    acg::set_last_error(std::string(where) + ": " + e.what());
+    return ACG_ERR_NOMEM;
+  } catch (const std::bad_alloc&) {
+    acg::set_last_error(std::string(where) + ": host out of memory");
+    return ACG_ERR_NOMEM;
+  } catch (const acg::CudaError& e) {
+    acg::set_last_error(std::string(where) + ": " + e.what());
+    return ACG_ERR_CUDA;
+  } catch (const std::exception& e) {
+    acg::set_last_error(std::string(where) + ": " + e.what());
+    return ACG_ERR_INVALID;
+  }
+}
+
+int check_device() {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    acg::set_last_error(std::string("no CUDA device: ") + cudaGetErrorString(e));
+    return ACG_ERR_NODEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+    cudaGetLastError();
+    acg::set_last_error("cudaGetDeviceProperties failed");
+    return ACG_ERR_NODEVICE;
+  }
+  if (prop.major != 10) {
+    acg::set_last_error("libacgpu is built for sm_100a (B200); device " + std::string(prop.name) + " is sm_" +
+                        std::to_string(prop.major) + std::to_string(prop.minor));
+    return ACG_ERR_NODEVICE;
+  }
+  return ACG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int acg_device_check(void) { return check_device(); }
+
+int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, const double* a_nzval,
+               const int64_t* ldli_col, const int64_t* ldli_colptr, const int64_t* ldli_rowval,
+               const double* ldli_fval, const double* ldli_d, int64_t ldli_nnz, int index_base,
+               const acg_options* opts, acg_solver** out) {
+  if (!out || !a_colptr || !a_rowval || !a_nzval || !ldli_col || !ldli_colptr || !ldli_rowval || !ldli_fval ||
+      !ldli_d) {
+    acg::set_last_error("acg_create: null argument");
+    return ACG_ERR_INVALID;
+  }
+  *out = nullptr;
+  int rc = check_device();
+  if (rc != ACG_OK) return rc;
+  return guarded("acg_create", [&]() {
+    auto* h = new acg_solver();
+    try {
+      ACG_CUDA(cudaGetDevice(&h->impl.device));
+      ACG_CUDA(cudaStreamCreateWithFlags(&h->impl.stream, cudaStreamNonBlocking));
+      acg::build_solver(h->impl, n, a_colptr, a_rowval, a_nzval, ldli_col, ldli_colptr, ldli_rowval, ldli_fval,
+                        ldli_d, ldli_nnz, index_base, opts);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return ACG_OK;
+  });
+}
+
+void acg_destroy(acg_solver* h) {
+  if (!h) return;
+  cudaStreamSynchronize(h->impl.stream);
+  delete h;
+}
+
+int acg_solver_stats(const acg_solver* h, acg_stats* out) {
+  if (!h || !out) {
+    acg::set_last_error("acg_solver_stats: null argument");
+    return ACG_ERR_INVALID;
+  }
+  const acg::SolverImpl& S = h->impl;
+  out->n = S.n;
+  out->nnz_lap = S.nnz_l;
+  out->nnz_factor = S.nnz_f;
+  out->levels = S.nlev;
+  int wide = 0, thin = 0;
+  for (const auto& st : S.plan) (st.thin ? thin : wide)++;
+  out->wide_levels = wide;
+  out->thin_runs = thin;
+  out->sweep_lanes = S.vl_sweep;
+  out->spmv_lanes = S.vl_spmv;
+  return ACG_OK;
+}
+
+int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol, int64_t maxits,
+              double maxtime, int stag_test, int precision, acg_solve_info* info) {
+  if (!h || !b || !x || nrhs < 0 || (nrhs > 1 && ldb < h->impl.n) || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_solve: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_solve", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    int worst = ACG_OK;
+    const int64_t ld = nrhs > 1 ? ldb : h->impl.n;
+    for (int64_t c = 0; c < nrhs; ++c) {
+      int rc = acg::solve_column(h->impl, b + c * ld, x + c * ld, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol,
+                                 maxits, maxtime, stag_test, precision, info ? info + c : nullptr);
+      worst = std::max(worst, rc);
+    }
+    return worst;
+  });
+}
+
+int acg_solve_device(acg_solver* h, const double* b_dev, double* x_dev, double tol, int64_t maxits, double maxtime,
+                     int stag_test, int precision, acg_solve_info* info) {
+  if (!h || !b_dev || !x_dev || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_solve_device: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_solve_device", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    ACG_CUDA(cudaDeviceSynchronize());
+    return acg::solve_column(h->impl, b_dev, x_dev, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice, tol, maxits,
+                             maxtime, stag_test, precision, info);
+  });
+}
+
+int acg_ldlsolve(acg_solver* h, const double* r, double* y, int precision) {
+  if (!h || !r || !y || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_ldlsolve: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_ldlsolve", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    acg::SolverImpl& S = h->impl;
+    ACG_CUDA(cudaMemcpyAsync(S.b_ext.p, r, sizeof(double) * S.n, cudaMemcpyHostToDevice, S.stream));
+    if (precision == 0) acg::ldlsolve_impl<double>(S, S.r64.p, S.y64.p);
+    else acg::ldlsolve_impl<float>(S, S.r32.p, S.y32.p);
+    ACG_CUDA(cudaGetLastError());
+    ACG_CUDA(cudaMemcpyAsync(y, S.x_ext.p, sizeof(double) * S.n, cudaMemcpyDeviceToHost, S.stream));
+    ACG_CUDA(cudaStreamSynchronize(S.stream));
+    return ACG_OK;
+  });
+}
+
+int acg_lap_mul(acg_solver* h, const double* x, double* y, int precision) {
+  if (!h || !x || !y || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_lap_mul: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_lap_mul", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    acg::SolverImpl& S = h->impl;
+    ACG_CUDA(cudaMemcpyAsync(S.b_ext.p, x, sizeof(double) * S.n, cudaMemcpyHostToDevice, S.stream));
+    if (precision == 0) acg::lapmul_impl<double>(S, S.r64.p);
+    else acg::lapmul_impl<float>(S, S.r32.p);
+    ACG_CUDA(cudaGetLastError());
+    ACG_CUDA(cudaMemcpyAsync(y, S.x_ext.p, sizeof(double) * S.n, cudaMemcpyDeviceToHost, S.stream));
+    ACG_CUDA(cudaStreamSynchronize(S.stream));
+    return ACG_OK;
+  });
+}
+
+
+int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* out) {
+  if (!h || !out || reps < 1 || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_time_kernels: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_time_kernels", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    acg::SolverImpl& S = h->impl;
+    acg::time_kernels(S, precision, reps, out);
+    return ACG_OK;
+  });
+}
+
+}  // extern "C"
+

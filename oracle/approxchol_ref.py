@@ -1,0 +1,283 @@
+"""ORACLE — test infrastructure only (checker, never shipped or measured).
+
+Pure-Python restatement of the reference's :deg elimination, written with
+mutable record objects like the Julia source so that it shares no code or
+data layout with the product's C++ elimination:
+  LLp / LLmatp            src/approxCholTypes.jl:14-39, src/approxChol.jl:102-136
+  flipIndex               src/graphUtils.jl:49-55
+  get_ll_col              src/approxChol.jl:354-385
+  compressCol!            src/approxChol.jl:415-449
+  approxChol(::LLmatp)    src/approxChol.jl:864-977
+  ApproxCholPQ + ops      src/approxChol.jl:2085-2239
+  sort!(…, QuickSort, o)  Julia 1.8 Base.Sort (median-of-three quicksort,
+                          insertion sort for ranges of at most 21 elements)
+Small graphs only (pure Python loops).  Returns the LDLinv arrays, 1-based.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from julia_rng import JuliaRng
+
+
+class LLp:
+    __slots__ = ("row", "val", "next", "reverse")
+
+    def __init__(self, row, val):
+        self.row = row
+        self.val = val
+        self.next = self
+        self.reverse = self
+
+
+# ---- Julia 1.8 Base.Sort.QuickSort on v[lo..hi] (1-based, inclusive) ----------
+
+def _insertion(v, lo, hi, lt):
+    for i in range(lo + 1, hi + 1):
+        j = i
+        x = v[i]
+        while j > lo:
+            if lt(x, v[j - 1]):
+                v[j] = v[j - 1]
+                j -= 1
+                continue
+            break
+        v[j] = x
+
+
+def _selectpivot(v, lo, hi, lt):
+    mi = lo + ((hi - lo) >> 1)
+    if lt(v[lo], v[mi]):
+        v[mi], v[lo] = v[lo], v[mi]
+    if lt(v[hi], v[lo]):
+        if lt(v[hi], v[mi]):
+            v[hi], v[lo], v[mi] = v[lo], v[mi], v[hi]
+        else:
+            v[hi], v[lo] = v[lo], v[hi]
+    return v[lo]
+
+
+def _partition(v, lo, hi, lt):
+    pivot = _selectpivot(v, lo, hi, lt)
+    i, j = lo, hi
+    while True:
+        i += 1
+        j -= 1
+        while lt(v[i], pivot):
+            i += 1
+        while lt(pivot, v[j]):
+            j -= 1
+        if i >= j:
+            break
+        v[i], v[j] = v[j], v[i]
+    v[j], v[lo] = pivot, v[j]
+    return j
+
+
+def quicksort(v, lo, hi, lt):
+    while lo < hi:
+        if hi - lo <= 20:
+            _insertion(v, lo, hi, lt)
+            return
+        j = _partition(v, lo, hi, lt)
+        if j - lo < hi - j:
+            if lo < j - 1:
+                quicksort(v, lo, j - 1, lt)
+            lo = j + 1
+        else:
+            if j + 1 < hi:
+                quicksort(v, j + 1, hi, lt)
+            hi = j - 1
+
+
+# ---- ApproxCholPQ -------------------------------------------------------------
+
+class PQ:
+    def __init__(self, degs, n):
+        self.n = n
+        self.prev = [0] * (n + 1)
+        self.next = [0] * (n + 1)
+        self.key = [0] * (n + 1)
+        self.lists = [0] * (2 * n + 2)
+        self.minlist = 1
+        self.nitems = n
+        for i in range(1, n + 1):
+            key = degs[i]
+            head = self.lists[key]
+            if head > 0:
+                self.prev[i], self.next[i], self.key[i] = 0, head, key
+                self.prev[head] = i
+            else:
+                self.prev[i], self.next[i], self.key[i] = 0, 0, key
+            self.lists[key] = i
+
+    def keymap(self, x):
+        k, upper = self.n, 2 * self.n + 1
+        return x if x <= k else min(upper, k + x // k)
+
+    def pop(self):
+        assert self.nitems > 0, "ApproxPQ is empty"
+        while self.lists[self.minlist] == 0:
+            self.minlist += 1
+        i = self.lists[self.minlist]
+        nx = self.next[i]
+        self.lists[self.minlist] = nx
+        if nx > 0:
+            self.prev[nx] = 0
+        self.nitems -= 1
+        return i
+
+    def move(self, i, newkey, oldlist, newlist):
+        pv, nx = self.prev[i], self.next[i]
+        if nx > 0:
+            self.prev[nx] = pv
+        if pv > 0:
+            self.next[pv] = nx
+        else:
+            self.lists[oldlist] = nx
+        head = self.lists[newlist]
+        if head > 0:
+            self.prev[head] = i
+        self.lists[newlist] = i
+        self.prev[i], self.next[i], self.key[i] = 0, head, newkey
+
+    def dec(self, i):
+        oldlist = self.keymap(self.key[i])
+        newlist = self.keymap(self.key[i] - 1)
+        if newlist != oldlist:
+            self.move(i, self.key[i] - 1, oldlist, newlist)
+            if newlist < self.minlist:
+                self.minlist = newlist
+        else:
+            self.key[i] -= 1
+
+    def inc(self, i):
+        oldlist = self.keymap(self.key[i])
+        newlist = self.keymap(self.key[i] + 1)
+        if newlist != oldlist:
+            self.move(i, self.key[i] + 1, oldlist, newlist)
+        else:
+            self.key[i] += 1
+
+
+def approx_chol(colptr, rowval, nzval, rng: JuliaRng):
+    """colptr/rowval 1-based (Julia CSC, rows sorted), nzval weights."""
+    n = len(colptr) - 1
+    m = colptr[n] - 1
+    # LLmatp(a)
+    degs = [0] * (n + 1)
+    llelems = [None] * (m + 1)
+    cols = [None] * (n + 1)
+    for i in range(1, n + 1):
+        degs[i] = colptr[i] - colptr[i - 1]
+        ind = colptr[i - 1]
+        nxt = llelems[ind] = LLp(rowval[ind - 1], nzval[ind - 1])
+        for ind in range(colptr[i - 1] + 1, colptr[i]):
+            e = LLp(rowval[ind - 1], nzval[ind - 1])
+            e.next = nxt
+            llelems[ind] = e
+            nxt = e
+        cols[i] = nxt
+    # flipIndex: position of the transposed entry
+    pos = {}
+    for c in range(1, n + 1):
+        for ind in range(colptr[c - 1], colptr[c]):
+            pos[(rowval[ind - 1], c)] = ind
+    for c in range(1, n + 1):
+        for ind in range(colptr[c - 1], colptr[c]):
+            r = rowval[ind - 1]
+            llelems[ind].reverse = llelems[pos[(c, r)]]
+
+    pq = PQ(degs, n)
+    col = [0] * (n - 1)
+    ldcolptr = [0] * n
+    ldrowval, ldfval = [], []
+    d = [0.0] * n
+    ptr_row = 1
+    it = 1
+    by_row = lambda x, y: x.row < y.row
+    by_val = lambda x, y: x.val < y.val
+    while it < n:
+        i = pq.pop()
+        col[it - 1] = i
+        ldcolptr[it - 1] = ptr_row
+        it += 1
+        # get_ll_col
+        colspace = [None]
+        ll = cols[i]
+        while ll.next is not ll:
+            if ll.val > 0:
+                colspace.append(ll)
+            ll = ll.next
+        if ll.val > 0:
+            colspace.append(ll)
+        ln = len(colspace) - 1
+        # compressCol!
+        quicksort(colspace, 1, ln, by_row)
+        ptr = 0
+        currow = 0
+        for k in range(1, ln + 1):
+            if colspace[k].row != currow:
+                currow = colspace[k].row
+                ptr += 1
+                colspace[ptr] = colspace[k]
+            else:
+                colspace[ptr].val = colspace[ptr].val + colspace[k].val
+                colspace[k].reverse.val = 0.0
+                pq.dec(currow)
+        ln = ptr
+        quicksort(colspace, 1, ln, by_val)
+        vals = [0.0] * (ln + 1)
+        cum = [0.0] * (ln + 1)
+        csum = 0.0
+        for k in range(1, ln + 1):
+            vals[k] = colspace[k].val
+            csum = csum + colspace[k].val
+            cum[k] = csum
+        wdeg = csum
+        col_scale = 1.0
+        for jo in range(1, ln):
+            ll = colspace[jo]
+            w = vals[jo] * col_scale
+            j = ll.row
+            revj = ll.reverse
+            f = w / wdeg
+            vals[jo] = 0.0
+            r = rng.rand() * (csum - cum[jo]) + cum[jo]
+            koff = ln
+            for kk in range(1, ln + 1):  # searchsortedfirst on 1..len
+                if not (cum[kk] < r):
+                    koff = kk
+                    break
+            k = colspace[koff].row
+            pq.inc(k)
+            new_val = f * (1.0 - f) * wdeg
+            revj.row = k
+            revj.val = new_val
+            revj.reverse = ll
+            khead = cols[k]
+            cols[k] = ll
+            ll.next = khead
+            ll.reverse = revj
+            ll.val = new_val
+            ll.row = j
+            col_scale = col_scale * (1.0 - f)
+            omf = 1.0 - f
+            wdeg = wdeg * (omf * omf)
+            ldrowval.append(j)
+            ldfval.append(f)
+            ptr_row += 1
+        ll = colspace[ln]
+        w = vals[ln] * col_scale
+        j = ll.row
+        revj = ll.reverse
+        if it < n:
+            pq.dec(j)
+        revj.val = 0.0
+        ldrowval.append(j)
+        ldfval.append(1.0)
+        ptr_row += 1
+        d[i - 1] = w
+    ldcolptr[it - 1] = ptr_row
+    return (np.array(col, np.int64), np.array(ldcolptr, np.int64), np.array(ldrowval, np.int64),
+            np.array(ldfval, np.float64), np.array(d, np.float64))

@@ -1,0 +1,84 @@
+"""Host elimination (product C++) against the independent Python restatement
+of approxChol / ApproxCholPQ / Julia's QuickSort and rand() (oracle), bit for bit."""
+import numpy as np
+import pytest
+
+import acgpu
+from acgpu import generators as G
+import approxchol_ref
+from julia_rng import JuliaRng
+
+
+def _ref_factor(a, seed):
+    a = acgpu.solvers._csc(a)
+    cp = (a.indptr + 1).tolist()
+    rv = (a.indices + 1).tolist()
+    return approxchol_ref.approx_chol(cp, rv, a.data.tolist(), JuliaRng(seed))
+
+
+CASES = [
+    ("path7", lambda: G.path_graph(7)),
+    ("star9", lambda: G.star_graph(9)),
+    ("cycle12w", lambda: G.cycle_graph(12, np.linspace(0.5, 2.0, 12))),
+    ("complete8", lambda: G.complete_graph(8)),
+    ("grid2_9x7", lambda: G.grid2(9, 7)),
+    ("grid2_12_logw", lambda: G.grid2(12, weights="loguniform", seed=3)),
+    ("grid3_5", lambda: G.grid3(5)),
+    ("tree60", lambda: G.random_tree(60, seed=5)),
+    ("pm_200", lambda: G.path_plus_matchings(200, k=4, sigma=2.0, seed=1)),
+    ("rgg_300", lambda: _largest_comp(G.random_geometric(300, seed=2))),
+]
+
+
+def _largest_comp(a):
+    co = acgpu.components(a)
+    big = np.argmax(np.bincount(co))
+    ind = np.where(co == big)[0]
+    return a[ind][:, ind]
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("seed", [1, 7])
+def test_factor_matches_restatement(name, make, seed):
+    a = make()
+    acgpu.seed(seed)
+    f = acgpu.approx_chol(a)
+    col, colptr, rowval, fval, d = _ref_factor(a, seed)
+    np.testing.assert_array_equal(f.col, col)
+    np.testing.assert_array_equal(f.colptr, colptr)
+    np.testing.assert_array_equal(f.rowval, rowval)
+    assert np.array_equal(f.fval, fval), "fval differs bitwise"
+    assert np.array_equal(f.d, d), "d differs bitwise"
+
+
+def test_factor_shape_invariants():
+    a = G.grid2(30, weights="loguniform", seed=4)
+    acgpu.seed(3)
+    f = acgpu.approx_chol(a)
+    n = a.shape[0]
+    assert sorted(set(f.col.tolist())) == sorted(set(range(1, n + 1)) - {int(np.setdiff1d(np.arange(1, n + 1), f.col)[0])})
+    assert f.colptr[0] == 1 and f.colptr[-1] == f.nnz + 1
+    assert np.all(np.diff(f.colptr) >= 1)
+    assert np.all((f.fval > 0) & (f.fval <= 1))
+    # the last entry of every column has fval == 1 (src/approxChol.jl:964-966)
+    assert np.all(f.fval[f.colptr[1:] - 2] == 1.0)
+    root = np.setdiff1d(np.arange(1, n + 1), f.col)[0]
+    assert f.d[root - 1] == 0.0 and np.all(np.delete(f.d, root - 1) > 0)
+
+
+def test_seed_stream_advances_like_global_rng():
+    a = G.grid2(10)
+    acgpu.seed(11)
+    f1 = acgpu.approx_chol(a)
+    f2 = acgpu.approx_chol(a)  # continues the stream: a different factor
+    acgpu.seed(11)
+    f3 = acgpu.approx_chol(a)
+    assert np.array_equal(f1.fval, f3.fval)
+    assert not np.array_equal(f1.fval, f2.fval)
+
+
+def test_negative_weight_rejected():
+    a = G.grid2(4).tolil()
+    a[0, 1] = a[1, 0] = -1.0
+    with pytest.raises(Exception):
+        acgpu.approx_chol(a.tocsc())
