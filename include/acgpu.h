@@ -81,11 +81,14 @@ typedef struct acg_solver acg_solver;
 
 /* Optional tuning knobs of acg_create (0 = automatic). */
 typedef struct {
-  int sweep_lanes;     /* lanes per vertex in the LDLinv sweeps: 2, 4, 8 or 16      */
+  int sweep_lanes;     /* sweep engine: 0 = sync-free dataflow sweep (one cooperative
+                          launch per sweep), 1 = one launch per level          */
   int spmv_lanes;      /* lanes per row in the Laplacian mat-vec: 2, 4, 8 or 16     */
-  int wide_level_min;  /* levels at least this wide get a grid launch; thinner runs
-                          of levels run in one CTA with block barriers            */
-  int reserved[5];
+  int wide_level_min;  /* levels at least this wide get a grid launch each; runs of
+                          narrower levels whose values fit in shared memory run in
+                          one CTA with block barriers (default 2048)              */
+  int reserved[5];     /* [0]: resident sweep blocks per SM (0 = 1); [1]: poll mode + 1
+                          (1 tight+sleep, 2 tight only, 3 backoff); others 0      */
 } acg_options;
 
 /* Shape of an uploaded solver. */
@@ -94,8 +97,8 @@ typedef struct {
   int64_t nnz_lap;     /* stored entries of lap(a) = nnz(a) + n       */
   int64_t nnz_factor;  /* F = length(ldli.fval)                       */
   int64_t levels;      /* depth of the LDLinv dependency DAG          */
-  int64_t wide_levels; /* levels swept with one grid launch each      */
-  int64_t thin_runs;   /* runs of thin levels swept by one CTA        */
+  int64_t wide_levels; /* levels swept with one grid launch each (FP32 plan) */
+  int64_t thin_runs;   /* runs of thin levels swept by one CTA (FP32 plan) */
   int sweep_lanes, spmv_lanes;
 } acg_stats;
 

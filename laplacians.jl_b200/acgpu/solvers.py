@@ -172,7 +172,11 @@ class DeviceLapSolver:
                              precision=precision)
         opts = AcgOptions()
         for k, v in (options or {}).items():
-            setattr(opts, k, int(v))
+            if k == "reserved":
+                for i, x in enumerate(v):
+                    opts.reserved[i] = int(x)
+            else:
+                setattr(opts, k, int(v))
         h = ctypes.c_void_p()
         check(lib().acg_create(self.n, a.indptr.astype(np.int64), a.indices.astype(np.int64),
                                np.ascontiguousarray(a.data), ldli.col, ldli.colptr, ldli.rowval, ldli.fval, ldli.d,

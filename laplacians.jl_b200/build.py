@@ -54,7 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         obj = objdir / (src + ".o")
         cmd = [NVCC, *common, *GENCODE, "-lineinfo", "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
-            cmd += ["-Xptxas", "-v"]
+            cmd += ["-Xptxas", "-v", "-Wno-deprecated-gpu-targets"]
         _run(cmd, verbose)
         objs.append(obj)
     tmp = OUT.with_suffix(".so.tmp")

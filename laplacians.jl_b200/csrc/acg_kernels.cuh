@@ -57,7 +57,7 @@ struct PcgState {
   long long total_its;
   int outer_its, outer_done;
   int max_outer;
-  int pad1;
+  int sweep_error;             // a bounded wait of a sync-free sweep gave up
   unsigned int counter[16];    // last-block tickets of the reducing kernels
 };
 
@@ -131,104 +131,392 @@ __device__ __forceinline__ T group_sum(T x) {
 
 // ---- sparse kernels --------------------------------------------------------
 
-// One row / vertex per VL-lane group.  All lanes of a warp stay converged in
-// the shuffles because the row loop bound is uniform per warp (rows are
-// assigned in warp-aligned strides and the loop runs while any lane of the
-// warp has work).
+// Programmatic dependent launch: the part of a kernel before pdl_wait() may
+// overlap the previous kernel in the stream; it must read only data that no
+// kernel since the last full (non-PDL) launch writes.  pdl_trigger() lets the
+// next kernel start its own prologue.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Sum over the lanes of an aligned group of `width` lanes (width 4, 8 or 32).
+template <typename T>
+__device__ __forceinline__ T group_sum_w(T x, int width) {
+  if (width == 32) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  } else {
+    for (int o = width >> 1; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  }
+  return x;
+}
+
+// One row / vertex per VL-lane group, U entries per lane in flight.
 template <typename T, int VL>
 __device__ __forceinline__ T row_dot(const int* __restrict__ ptr, const int* __restrict__ idx,
                                      const T* __restrict__ val, const T* x, int row, bool active, int lane) {
+  constexpr int U = 4;
   T acc = T(0);
   if (active) {
     const int k1 = __ldg(&ptr[row + 1]);
-    for (int k = __ldg(&ptr[row]) + lane; k < k1; k += VL) acc += __ldg(&val[k]) * x[__ldg(&idx[k])];
+    for (int k = __ldg(&ptr[row]) + lane; k < k1; k += VL * U) {
+      int id[U];
+      T c[U];
+#pragma unroll
+      for (int j = 0; j < U; ++j) {
+        const int kk = k + j * VL;
+        id[j] = kk < k1 ? __ldg(&idx[kk]) : -1;
+        c[j] = kk < k1 ? __ldg(&val[kk]) : T(0);
+      }
+#pragma unroll
+      for (int j = 0; j < U; ++j)
+        if (id[j] >= 0) acc += c[j] * x[id[j]];
+    }
   }
   return group_sum<VL>(acc);
 }
 
-// Forward sweep, one level: s[v] = r[v] + sum coef * s[src], v in [v0, v1).
-template <typename T, int VL>
-__global__ void __launch_bounds__(256) k_fwd_level(int v0, int v1, const int* __restrict__ fptr,
-                                                   const int* __restrict__ fidx, const T* __restrict__ fc,
-                                                   const T* __restrict__ r, T* s, const PcgState* st) {
-  if (st && st->done) return;
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = gt & (VL - 1);
-  const int v = v0 + gt / VL;
-  const int wv = v0 + (gt & ~31) / VL;  // first vertex of this warp
-  if (wv >= v1) return;                  // whole warp out of range
+// ---- LDLinv sweep, one wide level per launch ---------------------------------
+//
+// Vertices of a level are ordered by decreasing forward in-degree; the first
+// `nw` of a forward level (in-degree > 32) get a whole warp each, the others
+// share a warp four at a time (8 lanes each).  Each lane keeps 4 entries in
+// flight.  The constant structure and the per-vertex aux value (r for the
+// forward sweep, g for the backward one) are loaded before pdl_wait().
+constexpr int kLevelThreads = 256;
+constexpr int kLightLanes = 8;
+constexpr int kEntryUnroll = 4;
+
+template <typename T, bool kForward>
+__global__ void __launch_bounds__(kLevelThreads) k_level(int v0, int v1, int nw, const int* __restrict__ ptr,
+                                                         const int* __restrict__ idx, const T* __restrict__ coef,
+                                                         const T* __restrict__ aux, const T* __restrict__ sfwd, T* vals,
+                                                         const PcgState* st) {
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  int v, gl, gw;
+  if (warp < nw) {
+    v = v0 + warp;
+    gl = lane;
+    gw = 32;
+  } else {
+    v = v0 + nw + (warp - nw) * (32 / kLightLanes) + lane / kLightLanes;
+    gl = lane & (kLightLanes - 1);
+    gw = kLightLanes;
+  }
   const bool active = v < v1;
-  T acc = row_dot<T, VL>(fptr, fidx, fc, s, v, active, lane);
-  if (active && lane == 0) s[v] = r[v] + acc;
+  int k0 = 0, k1 = 0;
+  if (active) {
+    k0 = __ldg(&ptr[v]);
+    k1 = __ldg(&ptr[v + 1]);
+  }
+  int id[kEntryUnroll];
+  T c[kEntryUnroll];
+#pragma unroll
+  for (int j = 0; j < kEntryUnroll; ++j) {
+    const int k = k0 + gl + j * gw;
+    id[j] = k < k1 ? __ldg(&idx[k]) : -1;
+    c[j] = k < k1 ? __ldg(&coef[k]) : T(0);
+  }
+  const T a = active ? __ldg(&aux[v]) : T(0);
+  pdl_wait();
+  pdl_trigger();
+  if (st && st->done) return;
+  T acc = T(0);
+#pragma unroll
+  for (int j = 0; j < kEntryUnroll; ++j)
+    if (id[j] >= 0) acc += c[j] * vals[id[j]];
+  for (int k = k0 + gl + kEntryUnroll * gw; k < k1; k += gw) acc += __ldg(&coef[k]) * vals[__ldg(&idx[k])];
+  acc = group_sum_w(acc, gw);
+  if (active && gl == 0) vals[v] = kForward ? a + acc : a * sfwd[v] + acc;
 }
 
-// Backward sweep, one level (in place): y[v] = g[v]*y[v] + sum coef * y[dst].
-template <typename T, int VL>
-__global__ void __launch_bounds__(256) k_bwd_level(int v0, int v1, const int* __restrict__ bptr,
-                                                   const int* __restrict__ bidx, const T* __restrict__ bc,
-                                                   const T* __restrict__ g, T* y, const PcgState* st) {
-  if (st && st->done) return;
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = gt & (VL - 1);
-  const int v = v0 + gt / VL;
-  const int wv = v0 + (gt & ~31) / VL;
-  if (wv >= v1) return;
-  const bool active = v < v1;
-  T acc = row_dot<T, VL>(bptr, bidx, bc, y, v, active, lane);
-  if (active && lane == 0) y[v] = g[v] * y[v] + acc;
+// ---- LDLinv sweep, a run of thin levels in one CTA ----------------------------
+//
+// The run covers levels [l0, l1) = vertices [V0, V1).  Their values live in
+// shared memory for the whole run (and are written through to global memory
+// for later kernels); values of vertices outside the run are final before the
+// kernel starts and are read from global memory.  Groups of kThinLanes lanes
+// take one vertex; the structure of the next level's first step is loaded
+// into registers while the current level finishes, so a level costs one
+// shared-memory gather and a block barrier.
+constexpr int kThinThreads = 1024;
+constexpr int kThinLanes = 4;
+constexpr int kThinGroups = kThinThreads / kThinLanes;
+
+template <typename T>
+struct ThinPrefetch {
+  int v, k0, k1;
+  int id[kEntryUnroll];
+  T c[kEntryUnroll];
+  T a;
+};
+
+template <typename T>
+__device__ __forceinline__ void thin_fetch(ThinPrefetch<T>& f, int v, int vend, const int* __restrict__ sptr, int V0,
+                                          const int* __restrict__ idx, const T* __restrict__ coef,
+                                          const T* __restrict__ aux, int gl) {
+  f.v = v;
+  f.k0 = f.k1 = 0;
+  if (v < vend) {
+    f.k0 = sptr[v - V0];
+    f.k1 = sptr[v - V0 + 1];
+    f.a = __ldg(&aux[v]);
+  } else {
+    f.a = T(0);
+  }
+#pragma unroll
+  for (int j = 0; j < kEntryUnroll; ++j) {
+    const int k = f.k0 + gl + j * kThinLanes;
+    f.id[j] = k < f.k1 ? __ldg(&idx[k]) : -1;
+    f.c[j] = k < f.k1 ? __ldg(&coef[k]) : T(0);
+  }
 }
 
-// A run of thin levels [l0, l1) in one CTA: a block barrier between levels.
-constexpr int kThinThreads = 512;
-constexpr int kMaxThinLevels = 4096;
+template <typename T>
+__device__ __forceinline__ T thin_value(int id, int V0, int V1, const T* sv, const T* vals) {
+  return (id >= V0 && id < V1) ? sv[id - V0] : vals[id];
+}
 
-template <typename T, int VL>
-__global__ void __launch_bounds__(kThinThreads) k_fwd_thin(int l0, int l1, const int* __restrict__ lvl_off,
-                                                           const int* __restrict__ fptr, const int* __restrict__ fidx,
-                                                           const T* __restrict__ fc, const T* __restrict__ r, T* s,
-                                                           const PcgState* st) {
+// Shared memory: values (NV of T), then row pointers of the run (NV+1 ints),
+// then level offsets relative to V0 (L+1 ints).
+template <typename T, bool kForward>
+__global__ void __launch_bounds__(kThinThreads, 1) k_thin(int l0, int l1, const int* __restrict__ lvl_off,
+                                                           const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                           const T* __restrict__ coef, const T* __restrict__ aux,
+                                                           const T* __restrict__ sfwd, T* vals, const PcgState* st) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int V0 = __ldg(&lvl_off[l0]), V1 = __ldg(&lvl_off[l1]);
+  const int NV = V1 - V0, NL = l1 - l0;
+  T* sv = reinterpret_cast<T*>(smem_raw);
+  int* sptr = reinterpret_cast<int*>(sv + NV);
+  int* soff = sptr + NV + 1;
+  for (int i = threadIdx.x; i <= NV; i += blockDim.x) sptr[i] = __ldg(&ptr[V0 + i]);
+  for (int i = threadIdx.x; i <= NL; i += blockDim.x) soff[i] = __ldg(&lvl_off[l0 + i]);
+  pdl_wait();
+  pdl_trigger();
   if (st && st->done) return;
-  __shared__ int off[kMaxThinLevels + 1];
-  for (int i = threadIdx.x; i <= l1 - l0; i += blockDim.x) off[i] = lvl_off[l0 + i];
+  if (!kForward)
+    for (int i = threadIdx.x; i < NV; i += blockDim.x) sv[i] = sfwd[V0 + i];
   __syncthreads();
-  const int lane = threadIdx.x & (VL - 1);
-  const int grp = threadIdx.x / VL;
-  constexpr int kGroups = kThinThreads / VL;
-  for (int l = 0; l < l1 - l0; ++l) {
-    const int v0 = off[l], v1 = off[l + 1];
-    for (int base = v0; base < v1; base += kGroups) {
-      const int v = base + grp;
-      const bool active = v < v1;
-      T acc = row_dot<T, VL>(fptr, fidx, fc, s, v, active, lane);
-      if (active && lane == 0) s[v] = r[v] + acc;
+  const int gl = threadIdx.x & (kThinLanes - 1);
+  const int grp = threadIdx.x / kThinLanes;
+  ThinPrefetch<T> f;
+  {
+    const int lf = kForward ? 0 : NL - 1;
+    thin_fetch(f, soff[lf] + grp, soff[lf + 1], sptr, V0, idx, coef, aux, gl);
+  }
+  for (int step = 0; step < NL; ++step) {
+    const int l = kForward ? step : NL - 1 - step;
+    const int vs = soff[l], ve = soff[l + 1];
+    for (int base = vs; base < ve; base += kThinGroups) {
+      if (base != vs) thin_fetch(f, base + grp, ve, sptr, V0, idx, coef, aux, gl);
+      const bool active = f.v < ve;
+      T acc = T(0);
+#pragma unroll
+      for (int j = 0; j < kEntryUnroll; ++j)
+        if (f.id[j] >= 0) acc += f.c[j] * thin_value(f.id[j], V0, V1, sv, vals);
+      for (int k = f.k0 + gl + kEntryUnroll * kThinLanes; k < f.k1; k += kThinLanes)
+        acc += __ldg(&coef[k]) * thin_value(__ldg(&idx[k]), V0, V1, sv, vals);
+      acc = group_sum<kThinLanes>(acc);
+      if (active && gl == 0) {
+        const T out = kForward ? f.a + acc : f.a * sv[f.v - V0] + acc;
+        sv[f.v - V0] = out;
+        vals[f.v] = out;
+      }
+    }
+    // prefetch the first step of the next level before the barrier
+    if (step + 1 < NL) {
+      const int ln = kForward ? step + 1 : NL - 2 - step;
+      thin_fetch(f, soff[ln] + grp, soff[ln + 1], sptr, V0, idx, coef, aux, gl);
     }
     __syncthreads();
   }
 }
 
-template <typename T, int VL>
-__global__ void __launch_bounds__(kThinThreads) k_bwd_thin(int l0, int l1, const int* __restrict__ lvl_off,
-                                                           const int* __restrict__ bptr, const int* __restrict__ bidx,
-                                                           const T* __restrict__ bc, const T* __restrict__ g, T* y,
-                                                           const PcgState* st) {
-  if (st && st->done) return;
-  // walks levels l1-1 down to l0
-  __shared__ int off[kMaxThinLevels + 1];
-  for (int i = threadIdx.x; i <= l1 - l0; i += blockDim.x) off[i] = lvl_off[l0 + i];
-  __syncthreads();
-  const int lane = threadIdx.x & (VL - 1);
-  const int grp = threadIdx.x / VL;
-  constexpr int kGroups = kThinThreads / VL;
-  for (int l = l1 - l0 - 1; l >= 0; --l) {
-    const int v0 = off[l], v1 = off[l + 1];
-    for (int base = v0; base < v1; base += kGroups) {
-      const int v = base + grp;
-      const bool active = v < v1;
-      T acc = row_dot<T, VL>(bptr, bidx, bc, y, v, active, lane);
-      if (active && lane == 0) y[v] = g[v] * y[v] + acc;
+// ---- LDLinv sweep, sync-free (one cooperative launch per sweep) -----------
+//
+// Every value of the sweep's output vector starts as a "pending" sentinel (a
+// NaN with a payload arithmetic never produces); computing a vertex replaces
+// it, so the value is its own ready flag.  Warps take tasks round-robin in
+// level order (task t by warp t mod W); a task's inputs come from strictly
+// earlier tasks, so with all warps co-resident (cooperative launch) the
+// earliest unfinished task can always proceed.  Each wait polls the L2 copy
+// with relaxed GPU-scope loads and gives up after kSpinLimit polls, raising
+// PcgState::sweep_error instead of hanging.
+constexpr unsigned int kPendingF32 = 0x7fc0deadu;
+constexpr unsigned long long kPendingF64 = 0x7ff8dead0000deadull;
+constexpr unsigned int kSpinLimit = 1u << 22;
+constexpr int kSweepThreads = 256;
+
+__device__ __forceinline__ bool is_pending(float x) { return __float_as_uint(x) == kPendingF32; }
+__device__ __forceinline__ bool is_pending(double x) {
+  return (unsigned long long)__double_as_longlong(x) == kPendingF64;
+}
+template <typename T>
+__device__ __forceinline__ T pending_value();
+template <>
+__device__ __forceinline__ float pending_value<float>() { return __uint_as_float(kPendingF32); }
+template <>
+__device__ __forceinline__ double pending_value<double>() { return __longlong_as_double((long long)kPendingF64); }
+
+__device__ __forceinline__ float ld_relaxed(const float* p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ double ld_relaxed(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(float* p, float v) {
+  asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
+// Poll until the value is no longer pending.  poll_mode 0: tight polls, then
+// 64 ns sleeps; 1: tight polls only; 2: exponential backoff 32 ns .. 1 us.
+template <typename T>
+__device__ __noinline__ T wait_value_slow(const T* p, PcgState* st, int poll_mode) {
+  unsigned int sleep_ns = 32;
+  for (unsigned int spins = 1;; ++spins) {
+    if (poll_mode == 0) {
+      if (spins >= 64) __nanosleep(64);
+    } else if (poll_mode == 2) {
+      if (spins >= 4) {
+        __nanosleep(sleep_ns);
+        if (sleep_ns < 1024) sleep_ns <<= 1;
+      }
     }
-    __syncthreads();
+    const T x = ld_relaxed(p);
+    if (!is_pending(x)) return x;
+    if ((spins & 1023u) == 0 && *((volatile int*)&st->sweep_error)) return T(0);
+    if (spins >= kSpinLimit) {
+      atomicExch(&st->sweep_error, 1);
+      return T(0);
+    }
   }
+}
+
+template <typename T>
+__device__ __forceinline__ T wait_value(const T* p, PcgState* st, int poll_mode) {
+  const T x = ld_relaxed(p);
+  return is_pending(x) ? wait_value_slow(p, st, poll_mode) : x;
+}
+
+// A task record (32 bytes): {first vertex, (count << 1) | heavy, p[0..4]} with
+// p[i] = ptr[first + i], so a lane finds its entry range without another
+// dependent load.  A heavy task is one vertex on 32 lanes, a light task up to
+// 4 consecutive vertices of one level on 8 lanes each.
+struct alignas(16) SweepTask {
+  int v, cnt_heavy;
+  int p[6];
+};
+
+template <typename T>
+struct SweepEntries {
+  int v, k0, k1, gw;
+  bool active;
+  int id[kEntryUnroll];
+  T c[kEntryUnroll];
+  T a, own;
+};
+
+__device__ __forceinline__ SweepTask load_task(const SweepTask* __restrict__ tasks, int t, int ntasks) {
+  SweepTask r;
+  if (t < ntasks) {
+    const int4* q = reinterpret_cast<const int4*>(tasks + t);
+    const int4 x = __ldg(q), y = __ldg(q + 1);
+    r.v = x.x; r.cnt_heavy = x.y; r.p[0] = x.z; r.p[1] = x.w;
+    r.p[2] = y.x; r.p[3] = y.y; r.p[4] = y.z; r.p[5] = y.w;
+  } else {
+    r.v = 0; r.cnt_heavy = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) r.p[i] = 0;
+  }
+  return r;
+}
+
+template <typename T, bool kForward>
+__device__ __forceinline__ void load_entries(SweepEntries<T>& e, const SweepTask& r, int lane,
+                                             const int* __restrict__ idx, const T* __restrict__ coef,
+                                             const T* __restrict__ aux, const T* __restrict__ sfwd) {
+  const bool heavy = r.cnt_heavy & 1;
+  const int cnt = r.cnt_heavy >> 1;
+  const int sub = heavy ? 0 : (lane >> 3);
+  const int gw = heavy ? 32 : 8;
+  const int gl = heavy ? lane : (lane & 7);
+  e.active = sub < cnt;
+  e.gw = gw;
+  e.v = r.v + sub;
+  int k0 = 0, k1 = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (i == sub) { k0 = r.p[i]; k1 = r.p[i + 1]; }
+  if (!e.active) k0 = k1 = 0;
+  e.k0 = k0 + gl;
+  e.k1 = k1;
+  e.a = e.active ? __ldg(&aux[e.v]) : T(0);
+  e.own = (!kForward && e.active) ? __ldg(&sfwd[e.v]) : T(0);
+#pragma unroll
+  for (int j = 0; j < kEntryUnroll; ++j) {
+    const int k = e.k0 + j * gw;
+    e.id[j] = k < k1 ? __ldg(&idx[k]) : -1;
+    e.c[j] = k < k1 ? __ldg(&coef[k]) : T(0);
+  }
+}
+
+// Warp w runs tasks w, w+W, w+2W, ... (W warps in the grid).  Task records
+// are loaded two tasks ahead and entries one task ahead, so only the waits on
+// input values sit on the dependency chain.
+template <typename T, bool kForward>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const SweepTask* __restrict__ tasks,
+                                                         const int* __restrict__ idx, const T* __restrict__ coef,
+                                                         const T* __restrict__ aux, const T* __restrict__ sfwd, T* out,
+                                                         PcgState* st, int poll_mode) {
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int W = (int)((gridDim.x * blockDim.x) >> 5);
+  int t = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  SweepTask r1 = load_task(tasks, t + W, ntasks);
+  SweepEntries<T> e0;
+  {
+    const SweepTask r0 = load_task(tasks, t, ntasks);
+    load_entries<T, kForward>(e0, r0, lane, idx, coef, aux, sfwd);
+  }
+  for (; t < ntasks; t += W) {
+    const SweepTask r2 = load_task(tasks, t + 2 * W, ntasks);
+    SweepEntries<T> e1;
+    load_entries<T, kForward>(e1, r1, lane, idx, coef, aux, sfwd);
+    const int gw = e0.gw;  // uniform across the warp: one task per warp
+    T acc = T(0);
+#pragma unroll
+    for (int j = 0; j < kEntryUnroll; ++j)
+      if (e0.id[j] >= 0) acc += e0.c[j] * wait_value(&out[e0.id[j]], st, poll_mode);
+    for (int k = e0.k0 + kEntryUnroll * gw; k < e0.k1; k += gw)
+      acc += __ldg(&coef[k]) * wait_value(&out[__ldg(&idx[k])], st, poll_mode);
+    acc = group_sum_w(acc, gw);
+    if (e0.active && (lane & (gw - 1)) == 0) st_relaxed(&out[e0.v], kForward ? e0.a + acc : e0.a * e0.own + acc);
+    e0 = e1;
+    r1 = r2;
+  }
+}
+
+template <typename T>
+__global__ void k_fill_pending(int n, T* a, T* b) {
+  const T pv = pending_value<T>();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    a[i] = pv;
+    if (b) b[i] = pv;
+  }
+}
+
+// Shared memory bytes of a thin run with nv vertices and nl levels.
+template <typename T>
+constexpr size_t thin_smem_bytes(int nv, int nl) {
+  return (size_t)nv * sizeof(T) + (size_t)(nv + 1) * sizeof(int) + (size_t)(nl + 1) * sizeof(int);
 }
 
 }  // namespace acg

@@ -21,7 +21,10 @@
 
 namespace acg {
 
-enum StopCode { kConverged = 0, kMaxits = 1, kStagX = 2, kStagR = 3, kStagRho = 4, kInf = 5, kStagP = 6, kMaxtime = 7 };
+enum StopCode {
+  kConverged = 0, kMaxits = 1, kStagX = 2, kStagR = 3, kStagRho = 4, kInf = 5, kStagP = 6, kMaxtime = 7,
+  kSweepTimeout = 100  // a bounded device wait of a sweep gave up (reported as an error)
+};
 
 struct LoopCtl {
   cudaGraphConditionalHandle handle;
@@ -76,10 +79,13 @@ __global__ void __launch_bounds__(kVecThreads) k_spmv_pq(int n, const int* __res
   }
 }
 
+// Also marks the two sweep output vectors (s, y) pending for the next sweeps.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_update(int n, T* x3, const T* __restrict__ p, const T* __restrict__ q,
-                                                        T* __restrict__ r, PcgState* st, double* partials, LoopCtl ctl) {
+                                                        T* __restrict__ r, T* __restrict__ s_out, T* __restrict__ y_out,
+                                                        PcgState* st, double* partials, LoopCtl ctl) {
   if (st->done) return;
+  const T pend = pending_value<T>();
   const double al = st->alpha;
   const T* xc = x3 + (size_t)st->xcur * n;
   T* xn = x3 + (size_t)st->xnext * n;
@@ -89,6 +95,8 @@ __global__ void __launch_bounds__(kVecThreads) k_update(int n, T* x3, const T* _
     const T rv = (T)((double)r[i] + (-al) * (double)q[i]);
     xn[i] = xv;
     r[i] = rv;
+    s_out[i] = pend;
+    y_out[i] = pend;
     acc[0] += (double)rv * (double)rv;
     acc[1] += fabs((double)xv);
     acc[2] += fabs((double)rv);
@@ -110,11 +118,15 @@ __global__ void __launch_bounds__(kVecThreads) k_update(int n, T* x3, const T* _
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_ysum(int n, const T* __restrict__ y, PcgState* st, double* partials) {
+__global__ void __launch_bounds__(kVecThreads) k_ysum(int n, const T* __restrict__ y, PcgState* st, double* partials,
+                                                     LoopCtl ctl) {
   if (st->done) return;
   double acc[1] = {0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] += (double)y[i];
-  if (grid_reduce<1>(acc, partials, &st->counter[2]) && threadIdx.x == 0) st->mean = acc[0] / (double)n;
+  if (grid_reduce<1>(acc, partials, &st->counter[2]) && threadIdx.x == 0) {
+    st->mean = acc[0] / (double)n;
+    if (st->sweep_error) pcg_stop(st, kSweepTimeout, ctl);
+  }
 }
 
 // z = y - mean (in place); rho = z.r; the rest of the iteration's scalar logic.
@@ -196,14 +208,18 @@ __global__ void __launch_bounds__(kVecThreads) k_gather_in(int n, const int* __r
 // bm = b - mean(b); r = bm (cast to T); x buffer 0 = 0; |bm|, |bm|_1; PCG scalars reset.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_center(int n, double* __restrict__ bm, T* __restrict__ r, T* __restrict__ x0,
-                                                        PcgState* st, double* partials, LoopCtl ctl) {
+                                                        T* __restrict__ s_out, T* __restrict__ y_out, PcgState* st,
+                                                        double* partials, LoopCtl ctl) {
   const double mu = st->mean;
+  const T pend = pending_value<T>();
   double acc[2] = {0.0, 0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double v = bm[i] - mu;
     bm[i] = v;
     r[i] = (T)v;
     x0[i] = T(0);
+    if (s_out) s_out[i] = pend;
+    if (y_out) y_out[i] = pend;
     acc[0] += v * v;
     acc[1] += fabs(v);
   }
@@ -226,6 +242,7 @@ __global__ void __launch_bounds__(kVecThreads) k_center(int n, double* __restric
     st->xbest = 0;
     st->xnext = 1;
     st->outer_done = 0;
+    st->sweep_error = 0;
     st->t_start = globaltimer_ns();
     if (st->nb == 0.0) {
       st->nr_true = 0.0;
@@ -279,14 +296,17 @@ __global__ void __launch_bounds__(kVecThreads) k_scatter_out(int n, const int* _
 // Start of a refinement step: r_in = r64 / scale (FP32); inner PCG state reset.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_outer_prep(int n, const double* __restrict__ r64, T* __restrict__ rin,
-                                                            T* __restrict__ x0, PcgState* st, double* partials,
-                                                            LoopCtl inner_ctl) {
+                                                            T* __restrict__ x0, T* __restrict__ s_out, T* __restrict__ y_out,
+                                                            PcgState* st, double* partials, LoopCtl inner_ctl) {
   const double inv = 1.0 / st->scale;
+  const T pend = pending_value<T>();
   double acc[2] = {0.0, 0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const T v = (T)(r64[i] * inv);
     rin[i] = v;
     x0[i] = T(0);
+    s_out[i] = pend;
+    y_out[i] = pend;
     acc[0] += (double)v * (double)v;
     acc[1] += fabs((double)v);
   }
@@ -327,7 +347,8 @@ __global__ void k_outer_decide(PcgState* st, LoopCtl outer_ctl) {
   const int inner_status = st->status;
   const bool progressed = st->itcnt > 0 && st->bestnr < 1.0;
   int stop = -1;
-  if (st->nr_true <= st->tol_user) stop = kConverged;
+  if (st->sweep_error || inner_status == kSweepTimeout) stop = kSweepTimeout;
+  else if (st->nr_true <= st->tol_user) stop = kConverged;
   else if (st->total_its >= st->maxits_user) stop = kMaxits;
   else if (st->outer_its >= st->max_outer) stop = kStagX;
   else if (!progressed) stop = inner_status == kMaxits ? kStagRho : inner_status;

@@ -65,11 +65,13 @@ struct DevBuf {
 };
 
 // One step of a sweep plan: a single wide level (grid launch) or a run of
-// thin levels executed by one CTA.
+// thin levels executed by one CTA with the run's values in shared memory.
 struct SweepStep {
   int thin;
-  int l0, l1;  // levels [l0, l1)
-  int v0, v1;  // vertex range of the levels
+  int l0, l1;   // levels [l0, l1)
+  int v0, v1;   // vertex range of the levels
+  int nw;       // forward: leading vertices with in-degree > 32 (a warp each)
+  size_t smem;  // thin runs: dynamic shared memory bytes
 };
 
 struct SolverImpl {
@@ -78,10 +80,17 @@ struct SolverImpl {
   int n = 0;
   int64_t nnz_l = 0, nnz_f = 0;
   int nlev = 0;
-  int vl_sweep = 8, vl_spmv = 8;
-  int wide_min = 2048;
-  std::vector<int> lvl_off;  // host copy
-  std::vector<SweepStep> plan;
+  int vl_spmv = 8;
+  int thin_max_width = 2048;
+  size_t smem_optin = 0;
+  std::vector<int> lvl_off;        // host copy
+  std::vector<int> heavy;          // per level: vertices with forward in-degree > 32
+  std::vector<SweepStep> plan[2];  // [0] FP64 values, [1] FP32 values
+  int sweep_mode = 0;              // 0 sync-free cooperative sweep, 1 one launch per level
+  int ntasks_f = 0, ntasks_b = 0;
+  int sweep_blocks[2] = {0, 0};    // co-resident grid of k_sweep per value type
+  int poll_mode = 0;
+  DevBuf<SweepTask> tasks_f, tasks_b;
 
   DevBuf<int> perm, lvl_off_d;
   DevBuf<int> l_ptr, l_idx, f_ptr, f_idx, b_ptr, b_idx;
@@ -89,8 +98,8 @@ struct SolverImpl {
   DevBuf<float> l_v32, f_c32, b_c32, g32;
 
   // work vectors
-  DevBuf<double> b_ext, x_ext, bm, r64, y64, p64, q64, x3_64, xf;
-  DevBuf<float> r32, y32, p32, q32, x3_32;
+  DevBuf<double> b_ext, x_ext, bm, r64, s64, y64, p64, q64, x3_64, xf;
+  DevBuf<float> r32, s32, y32, p32, q32, x3_32;
   DevBuf<double> partials;
   PcgState* st = nullptr;    // device
   PcgState* h_st = nullptr;  // pinned host mirror
@@ -143,58 +152,92 @@ TypedArrays<float> arrays_of<float>(const SolverImpl& S) {
     default: FN<T, 16>(__VA_ARGS__); break;          \
   }
 
-template <typename T, int VL>
-void thin_fwd_vl(cudaStream_t s, const SweepStep& st_, const int* lo, const TypedArrays<T>& A, const T* r, T* y,
-                 const PcgState* st) {
-  k_fwd_thin<T, VL><<<1, kThinThreads, 0, s>>>(st_.l0, st_.l1, lo, A.fp, A.fi, A.fc, r, y, st);
-}
-template <typename T, int VL>
-void thin_bwd_vl(cudaStream_t s, const SweepStep& st_, const int* lo, const TypedArrays<T>& A, T* y, const PcgState* st) {
-  k_bwd_thin<T, VL><<<1, kThinThreads, 0, s>>>(st_.l0, st_.l1, lo, A.bp, A.bi, A.bc, A.g, y, st);
-}
-template <typename T, int VL>
-void wide_fwd_vl(cudaStream_t s, const SweepStep& st_, const TypedArrays<T>& A, const T* r, T* y, const PcgState* st) {
-  const long long threads = (long long)(st_.v1 - st_.v0) * VL;
-  k_fwd_level<T, VL><<<(int)((threads + 255) / 256), 256, 0, s>>>(st_.v0, st_.v1, A.fp, A.fi, A.fc, r, y, st);
-}
-template <typename T, int VL>
-void wide_bwd_vl(cudaStream_t s, const SweepStep& st_, const TypedArrays<T>& A, T* y, const PcgState* st) {
-  const long long threads = (long long)(st_.v1 - st_.v0) * VL;
-  k_bwd_level<T, VL><<<(int)((threads + 255) / 256), 256, 0, s>>>(st_.v0, st_.v1, A.bp, A.bi, A.bc, A.g, y, st);
+template <typename T>
+constexpr int plan_index() {
+  return sizeof(T) == sizeof(double) ? 0 : 1;
 }
 
-// Forward sweep: y = s (forward values) of r.
-template <typename T>
-void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* y, const PcgState* st) {
+// Launch with programmatic stream serialisation (PDL): the kernel's prologue
+// (constant structure loads) overlaps the previous launch in the stream.
+template <typename... KArgs, typename... Args>
+void launch_pdl(cudaStream_t s, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ACG_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+}
+
+template <typename T, bool kForward>
+void enqueue_step(cudaStream_t s, const SolverImpl& S, const SweepStep& st_, const T* aux, const T* sfwd, T* vals,
+                  const PcgState* st) {
   const TypedArrays<T> A = arrays_of<T>(S);
-  const int vl = S.vl_sweep;
-  for (const SweepStep& step : S.plan) {
-    if (step.thin) {
-      ACG_VL_SWITCH(vl, thin_fwd_vl, s, step, S.lvl_off_d.p, A, r, y, st);
-    } else {
-      ACG_VL_SWITCH(vl, wide_fwd_vl, s, step, A, r, y, st);
-    }
+  const int* ptr = kForward ? A.fp : A.bp;
+  const int* idx = kForward ? A.fi : A.bi;
+  const T* coef = kForward ? A.fc : A.bc;
+  if (st_.thin) {
+    launch_pdl(s, k_thin<T, kForward>, dim3(1), dim3(kThinThreads), st_.smem, st_.l0, st_.l1,
+               (const int*)S.lvl_off_d.p, ptr, idx, coef, aux, sfwd, vals, st);
+  } else {
+    const int nw = kForward ? st_.nw : 0;
+    const long long per_warp = 32 / kLightLanes;
+    const long long warps = nw + ((long long)(st_.v1 - st_.v0 - nw) + per_warp - 1) / per_warp;
+    const int blocks = (int)((warps * 32 + kLevelThreads - 1) / kLevelThreads);
+    launch_pdl(s, k_level<T, kForward>, dim3(blocks), dim3(kLevelThreads), 0, st_.v0, st_.v1, nw, ptr, idx, coef,
+               aux, sfwd, vals, st);
   }
 }
-// Backward sweep, in place on the forward values.
-template <typename T>
-void enqueue_backward(cudaStream_t s, const SolverImpl& S, T* y, const PcgState* st) {
+
+// One sync-free sweep as a cooperative launch (all blocks co-resident).
+template <typename T, bool kForward>
+void enqueue_syncfree(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sfwd, T* out, PcgState* st) {
   const TypedArrays<T> A = arrays_of<T>(S);
-  const int vl = S.vl_sweep;
-  for (auto it = S.plan.rbegin(); it != S.plan.rend(); ++it) {
-    const SweepStep& step = *it;
-    if (step.thin) {
-      ACG_VL_SWITCH(vl, thin_bwd_vl, s, step, S.lvl_off_d.p, A, y, st);
-    } else {
-      ACG_VL_SWITCH(vl, wide_bwd_vl, s, step, A, y, st);
-    }
-  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(S.sweep_blocks[plan_index<T>()]);
+  cfg.blockDim = dim3(kSweepThreads);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const int ntasks = kForward ? S.ntasks_f : S.ntasks_b;
+  const SweepTask* tasks = kForward ? S.tasks_f.p : S.tasks_b.p;
+  ACG_CUDA(cudaLaunchKernelEx(&cfg, k_sweep<T, kForward>, ntasks, tasks, kForward ? A.fi : A.bi,
+                              kForward ? A.fc : A.bc, aux, sfwd, out, st, S.poll_mode));
 }
-// y = (forward, then backward) LDLinv sweeps of r; y is also the forward scratch.
+
+// Forward sweep: s = forward values of r (s must be pending in sync-free mode).
 template <typename T>
-void enqueue_sweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* y, const PcgState* st) {
-  enqueue_forward<T>(s, S, r, y, st);
-  enqueue_backward<T>(s, S, y, st);
+void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, PcgState* st) {
+  if (S.sweep_mode == 0) {
+    enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st);
+    return;
+  }
+  for (const SweepStep& step : S.plan[plan_index<T>()]) enqueue_step<T, true>(s, S, step, r, (const T*)nullptr, sv, st);
+}
+// Backward sweep: y from the forward values s (y pending in sync-free mode).
+template <typename T>
+void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, PcgState* st) {
+  const T* g = arrays_of<T>(S).g;
+  if (S.sweep_mode == 0) {
+    enqueue_syncfree<T, false>(s, S, g, sv, y, st);
+    return;
+  }
+  const auto& plan = S.plan[plan_index<T>()];
+  for (auto it = plan.rbegin(); it != plan.rend(); ++it) enqueue_step<T, false>(s, S, *it, g, sv, y, st);
+}
+// y = LDLinv sweeps of r (without the final mean removal); sv is scratch.
+template <typename T>
+void enqueue_sweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y, PcgState* st) {
+  enqueue_forward<T>(s, S, r, sv, st);
+  enqueue_backward<T>(s, S, sv, y, st);
 }
 
 template <typename T, int VL>
@@ -210,12 +253,13 @@ void true_res_vl(cudaStream_t s, const SolverImpl& S, const double* x, const dou
 
 // The body of one PCG iteration on vectors of type T.
 template <typename T>
-void enqueue_pcg_iteration(cudaStream_t s, const SolverImpl& S, T* r, T* y, T* p, T* q, T* x3, double eps, LoopCtl ctl) {
+void enqueue_pcg_iteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* y, T* p, T* q, T* x3, double eps,
+                           LoopCtl ctl) {
   const TypedArrays<T> A = arrays_of<T>(S);
   ACG_VL_SWITCH(S.vl_spmv, spmv_pq_vl, s, S, A, p, q, S.st, eps, ctl);
-  k_update<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, x3, p, q, r, S.st, S.partials.p, ctl);
-  enqueue_sweeps<T>(s, S, r, y, S.st);
-  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p);
+  k_update<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, x3, p, q, r, sv, y, S.st, S.partials.p, ctl);
+  enqueue_sweeps<T>(s, S, r, sv, y, S.st);
+  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, ctl);
   k_zdot<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, r, p, S.st, S.partials.p, eps, 0, ctl);
   k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, p, S.st);
 }
@@ -265,9 +309,10 @@ cudaGraphExec_t build_fp64_graph(SolverImpl& S) {
 
   begin_into(s, top, {});
   k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
-  k_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, S.r64.p, S.x3_64.p, S.st, S.partials.p, ctl);
-  enqueue_sweeps<double>(s, S, S.r64.p, S.y64.p, S.st);
-  k_ysum<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.st, S.partials.p);
+  k_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, S.r64.p, S.x3_64.p, S.s64.p, S.y64.p, S.st,
+                                                      S.partials.p, ctl);
+  enqueue_sweeps<double>(s, S, S.r64.p, S.s64.p, S.y64.p, S.st);
+  k_ysum<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.st, S.partials.p, ctl);
   k_zdot<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.r64.p, S.p64.p, S.st, S.partials.p, kEps64, 1, ctl);
   std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
   end_into(s);
@@ -275,7 +320,7 @@ cudaGraphExec_t build_fp64_graph(SolverImpl& S) {
   cudaGraph_t body;
   cudaGraphNode_t wnode = add_while(top, leaves, h, &body);
   begin_into(s, body, {});
-  enqueue_pcg_iteration<double>(s, S, S.r64.p, S.y64.p, S.p64.p, S.q64.p, S.x3_64.p, kEps64, ctl);
+  enqueue_pcg_iteration<double>(s, S, S.r64.p, S.s64.p, S.y64.p, S.p64.p, S.q64.p, S.x3_64.p, kEps64, ctl);
   end_into(s);
 
   begin_into(s, top, {wnode});
@@ -307,7 +352,8 @@ cudaGraphExec_t build_mixed_graph(SolverImpl& S) {
   begin_into(s, top, {});
   k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
   // r64 = bm, x64 (xf) = 0
-  k_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, S.r64.p, S.xf.p, S.st, S.partials.p, octl);
+  k_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, S.r64.p, S.xf.p, (double*)nullptr,
+                                                      (double*)nullptr, S.st, S.partials.p, octl);
   std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
   end_into(s);
 
@@ -318,9 +364,10 @@ cudaGraphExec_t build_mixed_graph(SolverImpl& S) {
   LoopCtl ictl{hi, 1};
 
   begin_into(s, obody, {});
-  k_outer_prep<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.r64.p, S.r32.p, S.x3_32.p, S.st, S.partials.p, ictl);
-  enqueue_sweeps<float>(s, S, S.r32.p, S.y32.p, S.st);
-  k_ysum<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.st, S.partials.p);
+  k_outer_prep<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.r64.p, S.r32.p, S.x3_32.p, S.s32.p, S.y32.p, S.st,
+                                                         S.partials.p, ictl);
+  enqueue_sweeps<float>(s, S, S.r32.p, S.s32.p, S.y32.p, S.st);
+  k_ysum<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.st, S.partials.p, ictl);
   k_zdot<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.r32.p, S.p32.p, S.st, S.partials.p, eps32, 2, ictl);
   std::vector<cudaGraphNode_t> ol = capture_leaves(s);
   end_into(s);
@@ -328,7 +375,7 @@ cudaGraphExec_t build_mixed_graph(SolverImpl& S) {
   cudaGraph_t ibody;
   cudaGraphNode_t inode = add_while(obody, ol, hi, &ibody);
   begin_into(s, ibody, {});
-  enqueue_pcg_iteration<float>(s, S, S.r32.p, S.y32.p, S.p32.p, S.q32.p, S.x3_32.p, eps32, ictl);
+  enqueue_pcg_iteration<float>(s, S, S.r32.p, S.s32.p, S.y32.p, S.p32.p, S.q32.p, S.x3_32.p, eps32, ictl);
   end_into(s);
 
   begin_into(s, obody, {inode});
@@ -418,15 +465,25 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   S.lvl_off.assign(nlev + 1, 0);
   for (int v = 0; v < n; ++v) S.lvl_off[lev[v] + 1]++;
   for (int l = 0; l < nlev; ++l) S.lvl_off[l + 1] += S.lvl_off[l];
+  // Internal order: by level; inside a level by decreasing forward in-degree
+  // (then elimination step), so the level's heavy vertices come first.
+  std::vector<int> indeg(n, 0);
+  for (int64_t e = 0; e < F; ++e) indeg[rowval[e] - base]++;
   std::vector<int> perm(n), e2i(n);
   {
     std::vector<int> pos(S.lvl_off.begin(), S.lvl_off.end() - 1);
     for (int t = 0; t < n; ++t) {
       const int v = t < n - 1 ? (int)(col[t] - base) : root;
-      const int id = pos[lev[v]]++;
-      perm[id] = v;
-      e2i[v] = id;
+      perm[pos[lev[v]]++] = v;
     }
+    S.heavy.assign(nlev, 0);
+    for (int l = 0; l < nlev; ++l) {
+      std::stable_sort(perm.begin() + S.lvl_off[l], perm.begin() + S.lvl_off[l + 1],
+                       [&](int x, int y) { return indeg[x] > indeg[y]; });
+      for (int i = S.lvl_off[l]; i < S.lvl_off[l + 1]; ++i)
+        if (indeg[perm[i]] > 32) S.heavy[l]++;
+    }
+    for (int i = 0; i < n; ++i) e2i[perm[i]] = i;
   }
   // ---- folded coefficients
   std::vector<double> coef(F);
@@ -505,30 +562,103 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   S.nnz_l = m + n;
   S.nnz_f = F;
   // ---- tuning knobs
-  S.vl_sweep = choose_vl((double)F / n);
   S.vl_spmv = choose_vl((double)(m + n) / n);
-  S.wide_min = 2048;
+  S.thin_max_width = 2048;
   if (opts) {
-    if (opts->sweep_lanes > 0) S.vl_sweep = opts->sweep_lanes;
     if (opts->spmv_lanes > 0) S.vl_spmv = opts->spmv_lanes;
-    if (opts->wide_level_min > 0) S.wide_min = opts->wide_level_min;
+    if (opts->wide_level_min > 0) S.thin_max_width = opts->wide_level_min;
   }
-  for (int vl : {S.vl_sweep, S.vl_spmv})
-    if (vl != 2 && vl != 4 && vl != 8 && vl != 16) throw InputError("lane counts must be 2, 4, 8 or 16");
-  // ---- sweep plan
-  S.plan.clear();
-  for (int l = 0; l < nlev;) {
-    const int w = S.lvl_off[l + 1] - S.lvl_off[l];
-    if (w >= S.wide_min) {
-      S.plan.push_back({0, l, l + 1, S.lvl_off[l], S.lvl_off[l + 1]});
-      ++l;
-      continue;
+  if (S.vl_spmv != 2 && S.vl_spmv != 4 && S.vl_spmv != 8 && S.vl_spmv != 16)
+    throw InputError("lane counts must be 2, 4, 8 or 16");
+  // ---- sweep plans: runs of consecutive levels narrower than thin_max_width
+  // whose values fit in shared memory go to one CTA; other levels get a
+  // grid launch each.
+  {
+    int optin = 0;
+    ACG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, S.device));
+    S.smem_optin = (size_t)optin;
+  }
+  const size_t smem_cap = S.smem_optin > 4096 ? S.smem_optin - 2048 : 0;
+  for (int pi = 0; pi < 2; ++pi) {
+    auto& plan = S.plan[pi];
+    plan.clear();
+    auto bytes = [&](int nv, int nl) {
+      return pi == 0 ? thin_smem_bytes<double>(nv, nl) : thin_smem_bytes<float>(nv, nl);
+    };
+    for (int l = 0; l < nlev;) {
+      const int w = S.lvl_off[l + 1] - S.lvl_off[l];
+      if (w >= S.thin_max_width || bytes(w, 1) > smem_cap) {
+        plan.push_back({0, l, l + 1, S.lvl_off[l], S.lvl_off[l + 1], S.heavy[l], 0});
+        ++l;
+        continue;
+      }
+      int l1 = l;
+      while (l1 < nlev && S.lvl_off[l1 + 1] - S.lvl_off[l1] < S.thin_max_width &&
+             bytes(S.lvl_off[l1 + 1] - S.lvl_off[l], l1 + 1 - l) <= smem_cap)
+        ++l1;
+      plan.push_back({1, l, l1, S.lvl_off[l], S.lvl_off[l1], 0, bytes(S.lvl_off[l1] - S.lvl_off[l], l1 - l)});
+      l = l1;
     }
-    int l1 = l;
-    while (l1 < nlev && l1 - l < kMaxThinLevels && S.lvl_off[l1 + 1] - S.lvl_off[l1] < S.wide_min) ++l1;
-    S.plan.push_back({1, l, l1, S.lvl_off[l], S.lvl_off[l1]});
-    l = l1;
   }
+  // ---- sync-free task tables: tasks in level order (backward: reverse level
+  // order); a vertex with more than 32 entries is a task of its own on a
+  // whole warp, other vertices go four to a task within one level.
+  {
+    std::vector<int> outdeg(n, 0);
+    for (int v = 0; v < n; ++v) outdeg[v] = bptr[v + 1] - bptr[v];
+    auto emit_level = [](std::vector<SweepTask>& tasks, int vs, int ve, const std::vector<int>& deg,
+                         const std::vector<int>& ptr) {
+      int run = -1, cnt = 0;
+      auto push = [&](int v, int c, int heavy) {
+        SweepTask t = {};
+        t.v = v;
+        t.cnt_heavy = (c << 1) | heavy;
+        for (int i = 0; i <= c; ++i) t.p[i] = ptr[v + i];
+        tasks.push_back(t);
+      };
+      auto flush = [&]() {
+        if (cnt) push(run, cnt, 0);
+        cnt = 0;
+      };
+      for (int v = vs; v < ve; ++v) {
+        if (deg[v] > 32) {
+          flush();
+          push(v, 1, 1);
+          continue;
+        }
+        if (cnt == 0) run = v;
+        if (++cnt == 4) flush();
+      }
+      flush();
+    };
+    std::vector<int> fdeg(n);
+    for (int v = 0; v < n; ++v) fdeg[v] = fptr[v + 1] - fptr[v];
+    std::vector<SweepTask> tf, tb;
+    for (int l = 0; l < nlev; ++l) emit_level(tf, S.lvl_off[l], S.lvl_off[l + 1], fdeg, fptr);
+    for (int l = nlev - 1; l >= 0; --l) emit_level(tb, S.lvl_off[l], S.lvl_off[l + 1], outdeg, bptr);
+    S.ntasks_f = (int)tf.size();
+    S.ntasks_b = (int)tb.size();
+    S.tasks_f.upload(tf, S.stream);
+    S.tasks_b.upload(tb, S.stream);
+    int sms = 0;
+    ACG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S.device));
+    int occ[4] = {0, 0, 0, 0};
+    ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_sweep<double, true>, kSweepThreads, 0));
+    ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_sweep<double, false>, kSweepThreads, 0));
+    ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], k_sweep<float, true>, kSweepThreads, 0));
+    ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_sweep<float, false>, kSweepThreads, 0));
+    // One resident block (8 warps) per SM by default: more warps mostly add
+    // polling traffic on the L2 without shortening the dependency chains.
+    const int cap = (opts && opts->reserved[0] > 0) ? opts->reserved[0] : 1;
+    S.sweep_blocks[0] = sms * std::max(1, std::min(cap, std::min(occ[0], occ[1])));
+    S.sweep_blocks[1] = sms * std::max(1, std::min(cap, std::min(occ[2], occ[3])));
+    S.sweep_mode = (opts && opts->sweep_lanes == 1) ? 1 : 0;
+    if (opts && opts->reserved[1] > 0) S.poll_mode = opts->reserved[1] - 1;
+  }
+  ACG_CUDA(cudaFuncSetAttribute(k_thin<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+  ACG_CUDA(cudaFuncSetAttribute(k_thin<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+  ACG_CUDA(cudaFuncSetAttribute(k_thin<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+  ACG_CUDA(cudaFuncSetAttribute(k_thin<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
   // ---- upload
   cudaStream_t s = S.stream;
   S.perm.upload(perm, s);
@@ -547,9 +677,9 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   S.b_c32.upload(to_f32(bc), s);
   S.g64.upload(gi, s);
   S.g32.upload(to_f32(gi), s);
-  for (DevBuf<double>* b : {&S.b_ext, &S.x_ext, &S.bm, &S.r64, &S.y64, &S.p64, &S.q64, &S.xf}) b->alloc(n);
+  for (DevBuf<double>* b : {&S.b_ext, &S.x_ext, &S.bm, &S.r64, &S.s64, &S.y64, &S.p64, &S.q64, &S.xf}) b->alloc(n);
   S.x3_64.alloc((size_t)3 * n);
-  for (DevBuf<float>* b : {&S.r32, &S.y32, &S.p32, &S.q32}) b->alloc(n);
+  for (DevBuf<float>* b : {&S.r32, &S.s32, &S.y32, &S.p32, &S.q32}) b->alloc(n);
   S.x3_32.alloc((size_t)3 * n);
   S.partials.alloc((size_t)4 * kMaxPartialBlocks);
   ACG_CUDA(cudaMalloc(&S.st, sizeof(PcgState)));
@@ -594,14 +724,16 @@ void reset_state_for_direct_use(SolverImpl& S) {
 }
 
 template <typename T>
-void ldlsolve_impl(SolverImpl& S, T* rbuf, T* ybuf) {
+void ldlsolve_impl(SolverImpl& S, T* rbuf, T* sbuf, T* ybuf) {
   cudaStream_t s = S.stream;
   const int n = S.n;
   reset_state_for_direct_use(S);
+  LoopCtl none{0, 0};
   k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
   k_cast_from64<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, rbuf);
-  enqueue_sweeps<T>(s, S, rbuf, ybuf, S.st);
-  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.partials.p);
+  k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, sbuf, ybuf);
+  enqueue_sweeps<T>(s, S, rbuf, sbuf, ybuf, S.st);
+  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.partials.p, none);
   k_minus_mean<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.xf.p);
   k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
 }
@@ -620,14 +752,16 @@ void lapmul_impl(SolverImpl& S, T* xbuf) {
 
 
 // Device time per call of the solve's kernels, each captured `reps` times in a
-// graph and timed with CUDA events on the solver's stream (inputs: the state
-// of the last solve's vectors, or zeros).
+// graph and timed with CUDA events on the solver's stream.  Sweeps are timed
+// together with the kernel that marks their output pending, minus that
+// kernel's own time.
 template <typename T>
-void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* y, T* p, T* q) {
+void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T* y, T* p, T* q) {
   cudaStream_t s = S.stream;
   reset_state_for_direct_use(S);
   ACG_CUDA(cudaStreamSynchronize(s));
   const TypedArrays<T> A = arrays_of<T>(S);
+  LoopCtl none{0, 0};
   auto time_graph = [&](auto&& body) -> double {
     cudaGraph_t g;
     ACG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -651,27 +785,48 @@ void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* y, 
     cudaGraphDestroy(g);
     return (double)ms / reps;
   };
+  auto fill_s = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, sv, (T*)nullptr); };
+  auto fill_y = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, (T*)nullptr); };
+  const double t_fill = time_graph(fill_s);
   out->spmv_ms = time_graph([&]() { ACG_VL_SWITCH(S.vl_spmv, spmv_plain_vl, s, S, A, p, S.xf.p); });
-  out->forward_ms = time_graph([&]() { enqueue_forward<T>(s, S, r, y, S.st); });
-  out->backward_ms = time_graph([&]() { enqueue_backward<T>(s, S, y, S.st); });
+  out->forward_ms = time_graph([&]() {
+    fill_s();
+    enqueue_forward<T>(s, S, r, sv, S.st);
+  }) - t_fill;
+  out->backward_ms = time_graph([&]() {
+    fill_y();
+    enqueue_backward<T>(s, S, sv, y, S.st);
+  }) - t_fill;
   out->iteration_ms = time_graph([&]() {
     // the kernels of one PCG iteration without the stop logic taking effect
     ACG_VL_SWITCH(S.vl_spmv, spmv_plain_vl, s, S, A, p, S.xf.p);
-    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, p, S.st, S.partials.p);
-    enqueue_sweeps<T>(s, S, r, y, S.st);
-    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p);
+    k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, sv, y);
+    enqueue_sweeps<T>(s, S, r, sv, y, S.st);
+    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, none);
+    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, none);
     k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, q, S.st);
   });
-  out->launches_per_iteration = 6 + 2 * (int)S.plan.size();
-  out->forward_launches = (int)S.plan.size();
+  const int sweep_launches = S.sweep_mode == 0 ? 1 : (int)S.plan[plan_index<T>()].size();
+  out->launches_per_iteration = 6 + 2 * sweep_launches;
+  out->forward_launches = sweep_launches;
+  ACG_CUDA(cudaStreamSynchronize(s));
+  PcgState hs;
+  ACG_CUDA(cudaMemcpy(&hs, S.st, sizeof(PcgState), cudaMemcpyDeviceToHost));
+  if (hs.sweep_error) throw CudaError("a sync-free sweep wait gave up while timing");
 }
 
 void time_kernels(SolverImpl& S, int precision, int reps, acg_kernel_times* out) {
-  if (precision == 0) time_kernels_t<double>(S, reps, out, S.r64.p, S.y64.p, S.p64.p, S.q64.p);
-  else time_kernels_t<float>(S, reps, out, S.r32.p, S.y32.p, S.p32.p, S.q32.p);
+  if (precision == 0) time_kernels_t<double>(S, reps, out, S.r64.p, S.s64.p, S.y64.p, S.p64.p, S.q64.p);
+  else time_kernels_t<float>(S, reps, out, S.r32.p, S.s32.p, S.y32.p, S.p32.p, S.q32.p);
 }
 
-int status_to_rc(int status) { return status; }
+int status_to_rc(int status) {
+  if (status == kSweepTimeout) {
+    set_last_error("a bounded wait of a sync-free LDLinv sweep gave up; the solve was abandoned");
+    return ACG_ERR_TIMEOUT;
+  }
+  return status;
+}
 
 int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, cudaMemcpyKind kout, double tol,
                  int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info) {
@@ -824,10 +979,10 @@ int acg_solver_stats(const acg_solver* h, acg_stats* out) {
   out->nnz_factor = S.nnz_f;
   out->levels = S.nlev;
   int wide = 0, thin = 0;
-  for (const auto& st : S.plan) (st.thin ? thin : wide)++;
+  for (const auto& st : S.plan[1]) (st.thin ? thin : wide)++;
   out->wide_levels = wide;
   out->thin_runs = thin;
-  out->sweep_lanes = S.vl_sweep;
+  out->sweep_lanes = acg::kLightLanes;
   out->spmv_lanes = S.vl_spmv;
   return ACG_OK;
 }
@@ -845,6 +1000,7 @@ int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t l
     for (int64_t c = 0; c < nrhs; ++c) {
       int rc = acg::solve_column(h->impl, b + c * ld, x + c * ld, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol,
                                  maxits, maxtime, stag_test, precision, info ? info + c : nullptr);
+      if (rc < 0) return rc;
       worst = std::max(worst, rc);
     }
     return worst;
@@ -874,8 +1030,15 @@ int acg_ldlsolve(acg_solver* h, const double* r, double* y, int precision) {
     std::lock_guard<std::mutex> lk(h->impl.mu);
     acg::SolverImpl& S = h->impl;
     ACG_CUDA(cudaMemcpyAsync(S.b_ext.p, r, sizeof(double) * S.n, cudaMemcpyHostToDevice, S.stream));
-    if (precision == 0) acg::ldlsolve_impl<double>(S, S.r64.p, S.y64.p);
-    else acg::ldlsolve_impl<float>(S, S.r32.p, S.y32.p);
+    if (precision == 0) acg::ldlsolve_impl<double>(S, S.r64.p, S.s64.p, S.y64.p);
+    else acg::ldlsolve_impl<float>(S, S.r32.p, S.s32.p, S.y32.p);
+    ACG_CUDA(cudaStreamSynchronize(S.stream));
+    acg::PcgState hs;
+    ACG_CUDA(cudaMemcpy(&hs, S.st, sizeof(acg::PcgState), cudaMemcpyDeviceToHost));
+    if (hs.sweep_error) {
+      acg::set_last_error("acg_ldlsolve: a bounded sweep wait gave up");
+      return ACG_ERR_TIMEOUT;
+    }
     ACG_CUDA(cudaGetLastError());
     ACG_CUDA(cudaMemcpyAsync(y, S.x_ext.p, sizeof(double) * S.n, cudaMemcpyDeviceToHost, S.stream));
     ACG_CUDA(cudaStreamSynchronize(S.stream));
