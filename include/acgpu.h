@@ -122,6 +122,9 @@ typedef struct {
   double iteration_ms;      /* the kernels of one PCG iteration              */
   int launches_per_iteration;
   int forward_launches;
+  /* algorithmic bytes per call: every structure entry, task record and vector
+     element the kernel must touch once (re-reads not counted) */
+  double spmv_bytes, forward_bytes, backward_bytes;
 } acg_kernel_times;
 
 /* 0 if the current CUDA device is usable (sm_100), else an error code. */

@@ -47,7 +47,8 @@ class AcgSolveInfo(ctypes.Structure):
 class AcgKernelTimes(ctypes.Structure):
     _fields_ = [("spmv_ms", ctypes.c_double), ("forward_ms", ctypes.c_double), ("backward_ms", ctypes.c_double),
                 ("iteration_ms", ctypes.c_double), ("launches_per_iteration", ctypes.c_int),
-                ("forward_launches", ctypes.c_int)]
+                ("forward_launches", ctypes.c_int), ("spmv_bytes", ctypes.c_double),
+                ("forward_bytes", ctypes.c_double), ("backward_bytes", ctypes.c_double)]
 
 
 # (name, restype, argtypes) for every entry point of include/acgpu.h

@@ -806,6 +806,13 @@ void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv,
     k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, none);
     k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, q, S.st);
   });
+  const double vb = sizeof(T), nv = S.n, F = (double)S.nnz_f;
+  // mat-vec: row pointers, (index, value) per entry, x once, y (FP64) out
+  out->spmv_bytes = 4.0 * (nv + 1) + (double)S.nnz_l * (4.0 + vb) + nv * vb + nv * 8.0;
+  // sweeps: (index, coefficient) per entry, one 32-byte task record per task,
+  // aux (r or g) in, own forward value (backward), each input value once, output
+  out->forward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_f + nv * vb * 3.0;
+  out->backward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_b + nv * vb * 4.0;
   const int sweep_launches = S.sweep_mode == 0 ? 1 : (int)S.plan[plan_index<T>()].size();
   out->launches_per_iteration = 6 + 2 * sweep_launches;
   out->forward_launches = sweep_launches;

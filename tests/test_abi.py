@@ -1,0 +1,55 @@
+"""The C-ABI library loads without a GPU and exports every entry point that
+include/acgpu.h declares; the Python binding declares each of them."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from acgpu import _lib
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_functions():
+    text = (ROOT / "include" / "acgpu.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(acg_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "acg_create" in names and "acg_solve" in names and len(names) >= 15
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_symbol_exported(name):
+    L = ctypes.CDLL(str(_lib.LIB_PATH))
+    assert hasattr(L, name), f"{name} declared in include/acgpu.h but not exported"
+
+
+def test_binding_covers_header():
+    bound = {s[0] for s in _lib.SIGNATURES}
+    missing = set(declared_functions()) - bound
+    assert not missing, f"not bound in acgpu/_lib.py: {sorted(missing)}"
+
+
+def test_no_device_is_reported_not_crashed():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    rc = _lib.lib().acg_device_check()
+    assert rc == -5  # ACG_ERR_NODEVICE
+    assert _lib.lib().acg_last_error()
+
+
+def test_bad_arguments_are_errors():
+    import numpy as np
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    z = np.zeros(1, np.int64)
+    f = np.zeros(1)
+    rc = L.acg_create(1, z, z, f, z, z, z, f, f, 0, 1, None, ctypes.byref(h))
+    assert rc < 0
+    st = np.zeros(4, np.uint64)
+    assert L.acg_approxchol(1, z, z, f, st, ctypes.byref(h)) == -1
