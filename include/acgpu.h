@@ -169,6 +169,25 @@ int acg_lap_mul(acg_solver* h, const double* x, double* y, int precision);
  * timed with CUDA events on the solver's stream (no reference counterpart). */
 int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* out);
 
+/* ---- allocation-free preconditioner application ------------------------ */
+/* No counterpart in the reference (its Julia LDLsolver allocates freely).
+ * y_dev = LDLsolver(ldli, r_dev), as acg_ldlsolve computes it, for vectors
+ * already in device memory, without allocating: every piece of scratch comes
+ * from one fixed device array inside the library (ACG_NOALLOC_MAX_N vertices
+ * at most, about 4.1 MB, reserved on each GPU that loads the library until
+ * the process exits).  Meant for callers that must not allocate at that
+ * moment, e.g. work enqueued while a stream is captured into a CUDA graph, or
+ * a serving loop whose device memory is a fixed pool.  The scratch address is
+ * looked up once per device inside acg_create (set-up).  Work is enqueued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream); outside stream
+ * capture the call also waits for it and reports a sweep that gave up as
+ * ACG_ERR_TIMEOUT.  Every call shares the one array: calls whose work
+ * overlaps on the GPU (different streams, or different solvers, at the same
+ * time) race and corrupt each other's results.  Graphs with more than
+ * ACG_NOALLOC_MAX_N vertices are rejected with ACG_ERR_INVALID. */
+#define ACG_NOALLOC_MAX_N 131072
+int acg_ldlsolve_noalloc(acg_solver* h, const double* r_dev, double* y_dev, int precision, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,8 @@ SIGNATURES = [
     ("acg_lap_mul", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_int]),
     ("acg_time_kernels", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                         ctypes.POINTER(AcgKernelTimes)]),
+    ("acg_ldlsolve_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_void_p]),
 ]
 
 _lib = None

@@ -106,6 +106,7 @@ struct SolverImpl {
 
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   std::mutex mu;
+  unsigned char* noalloc_scratch = nullptr;  // device address of the fixed scratch array
 
   ~SolverImpl() {
     for (auto& e : exec)
@@ -738,6 +739,67 @@ void ldlsolve_impl(SolverImpl& S, T* rbuf, T* sbuf, T* ybuf) {
   k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
 }
 
+// ---- allocation-free LDLsolver ----------------------------------------------
+//
+// Some callers cannot allocate device memory at the moment they apply the
+// preconditioner: work enqueued while a stream is being captured into a CUDA
+// graph (the allocator may not be called then), or a serving loop whose device
+// memory comes from a pool that must not grow after start-up.  For them
+// acg_ldlsolve_noalloc keeps every piece of its scratch (the input in solver
+// order, the forward and backward sweep vectors, the reduction partials and
+// the scalar state) in the one fixed array below, which the library reserves
+// on every GPU it is loaded on, for as long as the process lives.
+constexpr int kNoAllocMaxN = ACG_NOALLOC_MAX_N;
+constexpr size_t kNoAllocVec = (size_t)kNoAllocMaxN * sizeof(double);
+constexpr size_t kNoAllocPartials = (size_t)4 * kMaxPartialBlocks * sizeof(double);
+constexpr size_t kNoAllocBytes = 4 * kNoAllocVec + kNoAllocPartials + ((sizeof(PcgState) + 255) / 256) * 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[256] = {};
+
+// Device address of the scratch array on the current device.  Host code must
+// not use g_noalloc_scratch itself: on the host that name is only a stand-in.
+unsigned char* noalloc_scratch_for_current_device(int device) {
+  if (device < 0 || device >= 256) throw InputError("device ordinal out of range for the no-alloc scratch table");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* ptr = nullptr;
+    ACG_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_addr[device] = static_cast<unsigned char*>(ptr);
+  }
+  return g_noalloc_addr[device];
+}
+
+template <typename T>
+void ldlsolve_noalloc_impl(const SolverImpl& S, cudaStream_t s, const double* r_ext, double* y_ext,
+                           unsigned char* base) {
+  const int n = S.n;
+  double* r64 = reinterpret_cast<double*>(base);
+  T* rT = reinterpret_cast<T*>(base + kNoAllocVec);
+  T* sv = reinterpret_cast<T*>(base + 2 * kNoAllocVec);
+  T* yv = reinterpret_cast<T*>(base + 3 * kNoAllocVec);
+  double* partials = reinterpret_cast<double*>(base + 4 * kNoAllocVec);
+  PcgState* st = reinterpret_cast<PcgState*>(base + 4 * kNoAllocVec + kNoAllocPartials);
+  LoopCtl none{0, 0};
+  // the state (done flag, sweep error flag, reduction tickets) must start at zero
+  ACG_CUDA(cudaMemsetAsync(st, 0, sizeof(PcgState), s));
+  k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, r_ext, r64, st, partials);
+  k_cast_from64<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, r64, rT);
+  k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, sv, yv);
+  enqueue_sweeps<T>(s, S, rT, sv, yv, st);
+  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, yv, st, partials, none);
+  k_minus_mean<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, yv, st, r64);
+  k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, r64, y_ext);
+}
+
+int noalloc_sweep_error(unsigned char* base) {
+  PcgState hs;
+  ACG_CUDA(cudaMemcpy(&hs, base + 4 * kNoAllocVec + kNoAllocPartials, sizeof(PcgState), cudaMemcpyDeviceToHost));
+  return hs.sweep_error;
+}
+
 template <typename T>
 void lapmul_impl(SolverImpl& S, T* xbuf) {
   cudaStream_t s = S.stream;
@@ -960,6 +1022,8 @@ int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, cons
       ACG_CUDA(cudaStreamCreateWithFlags(&h->impl.stream, cudaStreamNonBlocking));
       acg::build_solver(h->impl, n, a_colptr, a_rowval, a_nzval, ldli_col, ldli_colptr, ldli_rowval, ldli_fval,
                         ldli_d, ldli_nnz, index_base, opts);
+      // set-up of the allocation-free entry point, with this device current
+      h->impl.noalloc_scratch = acg::noalloc_scratch_for_current_device(h->impl.device);
     } catch (...) {
       delete h;
       throw;
@@ -1071,6 +1135,38 @@ int acg_lap_mul(acg_solver* h, const double* x, double* y, int precision) {
   });
 }
 
+int acg_ldlsolve_noalloc(acg_solver* h, const double* r_dev, double* y_dev, int precision, void* stream) {
+  if (!h || !r_dev || !y_dev || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_ldlsolve_noalloc: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  if (h->impl.n > ACG_NOALLOC_MAX_N) {
+    acg::set_last_error("acg_ldlsolve_noalloc: the graph has " + std::to_string(h->impl.n) +
+                        " vertices; the fixed scratch array holds at most " + std::to_string(ACG_NOALLOC_MAX_N));
+    return ACG_ERR_INVALID;
+  }
+  if (!h->impl.noalloc_scratch) {
+    acg::set_last_error("acg_ldlsolve_noalloc: scratch address was not resolved at acg_create");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_ldlsolve_noalloc", [&]() {
+    acg::SolverImpl& S = h->impl;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (precision == 0) acg::ldlsolve_noalloc_impl<double>(S, s, r_dev, y_dev, S.noalloc_scratch);
+    else acg::ldlsolve_noalloc_impl<float>(S, s, r_dev, y_dev, S.noalloc_scratch);
+    ACG_CUDA(cudaGetLastError());
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    ACG_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (cap == cudaStreamCaptureStatusNone) {
+      ACG_CUDA(cudaStreamSynchronize(s));
+      if (acg::noalloc_sweep_error(S.noalloc_scratch)) {
+        acg::set_last_error("acg_ldlsolve_noalloc: a bounded sweep wait gave up");
+        return ACG_ERR_TIMEOUT;
+      }
+    }
+    return ACG_OK;
+  });
+}
 
 int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* out) {
   if (!h || !out || reps < 1 || (precision != 0 && precision != 1)) {
