@@ -1,9 +1,10 @@
 #!/usr/bin/env python
 """Benchmark of the approxchol_lap solve phase on B200.
 
-Workload (one step = one solve): the 100x100x100 3D grid (1,000,000 vertices,
-6-neighbour) with edge weights log-uniform in [1e-3, 1] (seeded), one
-zero-mean Gaussian right-hand side per step, tol 1e-8 on the true relative
+Workload: the 100x100x100 3D grid (1,000,000 vertices, 6-neighbour) with
+edge weights log-uniform in [1e-3, 1] (seeded); each solve has one zero-mean
+Gaussian right-hand side; one step solves --rhs (default 64) independent
+right-hand sides in one batched launch; tol 1e-8 on the true relative
 residual |L x - b| / |b|, FP32 PCG (SpMV and LDLinv sweeps) inside FP64
 iterative refinement.  The factor is built once on the host with the
 reference's :deg elimination (not timed; its time is reported as factor_s).
@@ -63,7 +64,7 @@ def rhs(n, seed):
 
 def config(n, extra=None):
     c = {"workload": f"grid3({GRID_SIDE}) log-uniform weights [1e-3,1], 1 zero-mean Gaussian RHS per solve, tol 1e-8",
-         "n": n, "rhs_per_step": 1, "precision": "fp32 PCG in fp64 refinement",
+         "n": n, "precision": "fp32 PCG in fp64 refinement",
          "l2": "inputs larger than L2 (factor + Laplacian > 126 MB), no flush"}
     if extra:
         c.update(extra)
@@ -190,67 +191,85 @@ def run_acgpu(args):
     upload_s = time.perf_counter() - t
     L = lib()
     prec = 1 if args.precision == "mixed" else 0
+    k = args.rhs
 
-    # device-resident right-hand sides, one per step, distinct per rank
-    nsol = args.warmup + args.steps
-    B = torch.empty((nsol, n), dtype=torch.float64, device="cuda")
-    for i in range(nsol):
-        B[i] = torch.from_numpy(rhs(n, 1000 * rank + i))
-    X = torch.empty((n,), dtype=torch.float64, device="cuda")
-    info = AcgSolveInfo()
+    # device-resident right-hand sides: k independent columns per step, distinct per rank
+    nsteps = args.warmup + args.steps
+    B = torch.empty((nsteps, k, n), dtype=torch.float64, device="cuda")
+    for i in range(nsteps):
+        for c in range(k):
+            B[i, c] = torch.from_numpy(rhs(n, 1_000_000 * rank + 1000 * i + c))
+    X = torch.empty((k, n), dtype=torch.float64, device="cuda")
+    infos = (AcgSolveInfo * k)()
 
-    def solve_dev(i):
-        check(L.acg_solve_device(dev._h, ctypes.c_void_p(B[i].data_ptr()), ctypes.c_void_p(X.data_ptr()), TOL,
-                                 MAXITS, float("inf"), 5, prec, ctypes.byref(info)))
-        return info.iterations, info.refinements, info.true_relres, info.status
+    def solve_step(i):
+        if k == 1:
+            rc = L.acg_solve_device(dev._h, ctypes.c_void_p(B[i].data_ptr()), ctypes.c_void_p(X.data_ptr()), TOL,
+                                    MAXITS, float("inf"), 5, prec, infos)
+        else:
+            rc = L.acg_solve_batch_device(dev._h, ctypes.c_void_p(B[i].data_ptr()), ctypes.c_void_p(X.data_ptr()),
+                                          k, n, TOL, MAXITS, float("inf"), 5, prec, infos)
+        check(rc)
+        return [(infos[c].iterations, infos[c].refinements, infos[c].true_relres, infos[c].status) for c in range(k)]
 
     for i in range(args.warmup):
-        solve_dev(i)
+        solve_step(i)
     torch.cuda.synchronize()
     barrier(world)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    its_list, ref_list, res_list = [], [], []
+    results = []
     with ClockSampler(local) as clk:
         time.sleep(0.5)  # let the sampler start before the timed region
         torch.cuda.synchronize()
         e0.record()
-        for i in range(args.warmup, nsol):
-            its, ref, res, stt = solve_dev(i)
-            its_list.append(its)
-            ref_list.append(ref)
-            res_list.append(res)
-            if stt != 0:
-                raise RuntimeError(f"solve {i} did not converge (status {stt}, relres {res})")
+        for i in range(args.warmup, nsteps):
+            results += solve_step(i)
         e1.record()
         torch.cuda.synchronize()
     barrier(world)
-    ms = e0.elapsed_time(e1)
-    ms = max_over_ranks(ms, world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
     clocks = clk.summary()
+    bad = [r for r in results if r[3] != 0 or r[2] > TOL]
+    if bad:
+        raise RuntimeError(f"{len(bad)} solves missed the tolerance: {bad[:3]}")
+    its = np.array([r[0] for r in results], dtype=float)
+    refs = np.array([r[1] for r in results], dtype=float)
+    res = np.array([r[2] for r in results])
 
-    # end to end: pinned host buffers through acg_solve (H2D + D2H timed)
-    hb = torch.empty((args.steps, n), dtype=torch.float64, pin_memory=True)
-    hx = torch.empty((n,), dtype=torch.float64, pin_memory=True)
+    # end to end: pinned host blocks through acg_solve (H2D + D2H inside the timed region)
+    hb = torch.empty((args.steps, k, n), dtype=torch.float64, pin_memory=True)
+    hx = torch.empty((k, n), dtype=torch.float64, pin_memory=True)
     hb_np = hb.numpy()
     hx_np = hx.numpy()
     for i in range(args.steps):
-        hb_np[i] = rhs(n, 5000 + 1000 * rank + i)
-    check(L.acg_solve(dev._h, hb_np[0], hx_np, 1, n, TOL, MAXITS, float("inf"), 5, prec, ctypes.byref(info)))
+        for c in range(k):
+            hb_np[i, c] = rhs(n, 5_000_000 + 1_000_000 * rank + 1000 * i + c)
+    hb_flat = [np.ascontiguousarray(hb_np[i]).reshape(-1) for i in range(args.steps)]
+    hx_flat = hx_np.reshape(-1)
+    check(L.acg_solve(dev._h, hb_flat[0], hx_flat, k, n, TOL, MAXITS, float("inf"), 5, prec, infos))
     barrier(world)
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     e2.record()
     for i in range(args.steps):
-        check(L.acg_solve(dev._h, hb_np[i], hx_np, 1, n, TOL, MAXITS, float("inf"), 5, prec, ctypes.byref(info)))
+        check(L.acg_solve(dev._h, hb_flat[i], hx_flat, k, n, TOL, MAXITS, float("inf"), 5, prec, infos))
     e3.record()
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
 
+    # one right-hand side alone: latency of a single solve
+    single = []
+    for i in range(3):
+        t0 = time.perf_counter()
+        check(L.acg_solve_device(dev._h, ctypes.c_void_p(B[i, 0].data_ptr()), ctypes.c_void_p(X.data_ptr()), TOL,
+                                 MAXITS, float("inf"), 5, prec, infos))
+        single.append(infos[0].solve_ms)
+
     # roofline of the dominant kernel (the forward LDLinv sweep), timed live
-    kt = dev.time_kernels(args.precision, reps=5)
+    kt = dev.time_kernels_batch(k, args.precision, reps=5) if k > 1 else dev.time_kernels(args.precision, reps=5)
     stats = dev.stats()
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
@@ -261,38 +280,39 @@ def run_acgpu(args):
     peak = peak or 6650.0
     achieved = kt["forward_bytes"] / (kt["forward_ms"] * 1e-3) / 1e9
     traffic = None
-    prof = ROOT / "profiles" / "k_sweep_forward_grid3_100.md"
+    prof = ROOT / "profiles" / ("kb_sweep_forward_grid3_100_k64.md" if k > 1 else "k_sweep_forward_grid3_100.md")
     if prof.exists() and GRID_SIDE == 100:
         import re
         m = re.search(r"dram_bytes_per_launch:\s*(\d+)", prof.read_text())
         traffic = int(m.group(1)) if m else None
 
-    its_mean = float(np.mean(its_list))
-    ref_mean = float(np.mean(ref_list))
-    # our kernels per solve: 3 set-up/wrap-up + per refinement 8 + per inner iteration
-    launches_iter = kt["launches_per_iteration"]
-    launches = args.steps * (3 + ref_mean * 8 + its_mean * launches_iter)
+    # our kernel launches per step: set-up/wrap-up 3, per refinement 8, per inner iteration 8 (9 for k = 1)
+    per_it = kt["launches_per_iteration"] if k == 1 else 8
+    launches = args.steps * (3 + refs.max() * 8 + its.max() * per_it)
 
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            t_cpu, sample = cpu_solve_time(a, ldli, rhs(n, 424242), int(round(its_mean)))
+            t_cpu, sample = cpu_solve_time(a, ldli, rhs(n, 424242), int(round(its.mean())))
             cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": 1, "kind": "port", "sample": sample}
-        value = world * args.steps / (ms * 1e-3)
+        value = world * args.steps * k / (ms * 1e-3)
+        kern = (f"kb_sweep<float,{k // 8 if k >= 8 else 1},forward> (batched LDLinv forward sweep, {k} columns)"
+                if k > 1 else "k_sweep<float,forward> (LDLinv forward sweep)")
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (SpMV, sweeps) / f64 (residual, dots, correction)",
-            "data": "synthetic (seeded grid weights and Gaussian RHS)",
-            "config": config(n, {"parallelism": f"replicas x{world}", "pcg_iterations_mean": its_mean,
-                                 "refinements_mean": ref_mean, "true_relres_max": max(res_list),
-                                 "factor_s": factor_s, "upload_s": upload_s, "levels": stats["levels"],
-                                 "factor_nnz": stats["nnz_factor"]}),
-            "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
-                    "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
-            "roofline": {"bound": "hbm", "kernel": "k_sweep<float,forward> (LDLinv forward sweep)",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_src, "traffic": traffic,
+            "vs_baseline": None, "dtype": "f32 (SpMV, sweeps) / f64 (residual, dots, correction)"
+            if prec == 1 else "f64", "data": "synthetic (seeded grid weights and Gaussian RHS)",
+            "config": config(n, {"parallelism": f"replicas x{world}", "rhs_per_step": k,
+                                 "batching": f"{k} independent single-RHS solves per step in one batched launch",
+                                 "pcg_iterations_mean": float(its.mean()), "refinements_mean": float(refs.mean()),
+                                 "true_relres_max": float(res.max()), "factor_s": factor_s, "upload_s": upload_s,
+                                 "levels": stats["levels"], "factor_nnz": stats["nnz_factor"]}),
+            "single_rhs": {"latency_ms": float(np.median(single)), "solves_per_s": 1e3 / float(np.median(single))},
+            "e2e": {"value": world * args.steps * k / (e2e_ms * 1e-3), "unit": "solves/s",
+                    "h2d_bytes_per_step": 8 * n * k, "d2h_bytes_per_step": 8 * n * k},
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                          "algorithmic_bytes_per_launch": kt["forward_bytes"], "launch_ms": kt["forward_ms"],
                          "backward_ms": kt["backward_ms"], "spmv_ms": kt["spmv_ms"],
                          "spmv_gbs": kt["spmv_bytes"] / (kt["spmv_ms"] * 1e-3) / 1e9},
@@ -368,6 +388,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--side", type=int, default=GRID_SIDE, help="grid side (100 = the benchmark workload)")
+    ap.add_argument("--rhs", type=int, default=64, help="independent right-hand sides per step (batched)")
     args = ap.parse_args()
     globals()["GRID_SIDE"] = args.side
     if args.warmup < 3 and args.impl == "acgpu":

@@ -150,7 +150,8 @@ int acg_solver_stats(const acg_solver* h, acg_stats* out);
  * pcg(la, b .- mean(b), LDLsolver; tol, maxits, maxtime, stag_test) with the
  * stop rules of src/pcg.jl:256-445, returning bestx.  Host arrays; nrhs
  * right-hand sides stored column-major with leading dimension ldb (>= n when
- * nrhs > 1), info[nrhs] optional.
+ * nrhs > 1), info[nrhs] optional; more than one right-hand side is solved in
+ * batched launches of up to 64 columns (each column its own PCG system).
  *   precision 0: FP64 PCG (the reference algorithm).
  *   precision 1: FP32 PCG (SpMV, LDLinv sweeps, vectors) inside FP64 iterative
  *                refinement on the true residual; tol is then on
@@ -161,6 +162,12 @@ int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t l
 /* As acg_solve for one right-hand side already in device memory. */
 int acg_solve_device(acg_solver* h, const double* b_dev, double* x_dev, double tol, int64_t maxits, double maxtime,
                      int stag_test, int precision, acg_solve_info* info);
+/* Block of nrhs right-hand sides already in device memory (column-major,
+ * leading dimension ld >= n): solved 64 at a time in one batched launch, each
+ * column its own PCG system with the same stop rules as acg_solve; info[nrhs]
+ * optional.  The reference solves one vector per call (src/pcg.jl:256). */
+int acg_solve_batch_device(acg_solver* h, const double* b_dev, double* x_dev, int64_t nrhs, int64_t ld, double tol,
+                           int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info);
 /* y = LDLsolver(ldli, r) (src/approxChol.jl:1347-1366) on the device; host arrays. */
 int acg_ldlsolve(acg_solver* h, const double* r, double* y, int precision);
 /* y = lap(a) * x on the device (FP64 or FP32 values); host arrays. */
@@ -168,6 +175,9 @@ int acg_lap_mul(acg_solver* h, const double* x, double* y, int precision);
 /* Time the solve's kernels: each captured `reps` times into a CUDA graph and
  * timed with CUDA events on the solver's stream (no reference counterpart). */
 int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* out);
+/* The same for the batched kernels with nrhs (<= 64) right-hand sides
+ * (iteration_ms is not measured there). */
+int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg_kernel_times* out);
 
 /* ---- allocation-free preconditioner application ------------------------ */
 /* No counterpart in the reference (its Julia LDLsolver allocates freely).

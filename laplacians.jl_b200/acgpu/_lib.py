@@ -72,10 +72,15 @@ SIGNATURES = [
     ("acg_solve_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                         ctypes.c_int64, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                         ctypes.POINTER(AcgSolveInfo)]),
+    ("acg_solve_batch_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                              ctypes.c_int64, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
+                                              ctypes.c_int, ctypes.c_int, ctypes.POINTER(AcgSolveInfo)]),
     ("acg_ldlsolve", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_int]),
     ("acg_lap_mul", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_int]),
     ("acg_time_kernels", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                         ctypes.POINTER(AcgKernelTimes)]),
+    ("acg_time_kernels_batch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.POINTER(AcgKernelTimes)]),
     ("acg_ldlsolve_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                             ctypes.c_void_p]),
 ]

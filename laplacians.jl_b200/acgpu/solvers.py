@@ -237,6 +237,11 @@ class DeviceLapSolver:
         check(lib().acg_time_kernels(self._h, _PRECISIONS[precision], int(reps), ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in _lib.AcgKernelTimes._fields_}
 
+    def time_kernels_batch(self, nrhs, precision="mixed", reps=5) -> dict:
+        t = _lib.AcgKernelTimes()
+        check(lib().acg_time_kernels_batch(self._h, _PRECISIONS[precision], int(nrhs), int(reps), ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in _lib.AcgKernelTimes._fields_}
+
     def lap_mul(self, x, precision="fp64"):
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty_like(x)

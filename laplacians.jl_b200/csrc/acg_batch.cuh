@@ -1,0 +1,725 @@
+// Batched solves: k right-hand sides of one graph in the same kernels.
+//
+// Vectors are vertex-major blocks n x kp (kp = k rounded up to 8, 16, 32 or
+// 64): element (v, c) at v*kp + c, so one vertex's kp values are contiguous
+// and a sweep reads each factor entry once for all columns.  Padding columns
+// carry a zero right-hand side and stop at set-up.  Every column is its own
+// PCG system with its own PcgState (the same scalar logic as the
+// one-right-hand-side kernels, run by thread c for column c); a launch ends
+// early only when every column has stopped.
+#pragma once
+#include "acg_pcg.cuh"
+
+namespace acg {
+
+constexpr int kMaxBatch = 64;
+constexpr int kBatchLanes = 8;  // lanes per vertex in the batched sweeps and mat-vec
+
+struct BatchShared {
+  int all_done;     // every column stopped
+  int sweep_error;  // a bounded sweep wait gave up
+  int k;            // right-hand sides in this launch (the rest of kp is padding)
+  int pad;
+  unsigned int counter[16];
+};
+
+// ---- vector relaxed loads/stores of CPL consecutive values -----------------
+
+template <typename T, int CPL>
+struct Row {
+  T v[CPL];
+};
+
+template <typename T, int CPL>
+__device__ __forceinline__ void ld_row(Row<T, CPL>& r, const T* p) {
+#pragma unroll
+  for (int j = 0; j < CPL; ++j) r.v[j] = ld_relaxed(p + j);
+}
+
+template <int CPL>
+__device__ __forceinline__ void ld_row(Row<float, CPL>& r, const float* p) {
+  if constexpr (CPL % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < CPL / 4; ++q)
+      asm volatile("ld.relaxed.gpu.global.v4.f32 {%0,%1,%2,%3}, [%4];"
+                   : "=f"(r.v[4 * q]), "=f"(r.v[4 * q + 1]), "=f"(r.v[4 * q + 2]), "=f"(r.v[4 * q + 3])
+                   : "l"(p + 4 * q)
+                   : "memory");
+  } else {
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) r.v[j] = ld_relaxed(p + j);
+  }
+}
+
+template <int CPL>
+__device__ __forceinline__ void ld_row(Row<double, CPL>& r, const double* p) {
+  if constexpr (CPL % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < CPL / 2; ++q)
+      asm volatile("ld.relaxed.gpu.global.v2.f64 {%0,%1}, [%2];"
+                   : "=d"(r.v[2 * q]), "=d"(r.v[2 * q + 1])
+                   : "l"(p + 2 * q)
+                   : "memory");
+  } else {
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) r.v[j] = ld_relaxed(p + j);
+  }
+}
+
+template <typename T, int CPL>
+__device__ __forceinline__ bool row_pending(const Row<T, CPL>& r) {
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < CPL; ++j) any |= is_pending(r.v[j]);
+  return any;
+}
+
+// Slow path: poll the row (in L2) until no value is pending or the bound is
+// hit; returns false when the wait gave up.  Keeps the caller's row in
+// registers (the caller reloads it).
+template <typename T, int CPL>
+__device__ __noinline__ bool wait_row_ready(const T* p, BatchShared* bs) {
+  for (unsigned int spins = 1;; ++spins) {
+    if (spins >= 64) __nanosleep(64);
+    Row<T, CPL> r;
+    ld_row<CPL>(r, p);
+    if (!row_pending(r)) return true;
+    if ((spins & 1023u) == 0 && *((volatile int*)&bs->sweep_error)) return false;
+    if (spins >= kSpinLimit) {
+      atomicExch(&bs->sweep_error, 1);
+      return false;
+    }
+  }
+}
+
+template <typename T, int CPL>
+__device__ __forceinline__ void wait_row(Row<T, CPL>& r, const T* p, BatchShared* bs) {
+  ld_row<CPL>(r, p);
+  if (row_pending(r)) {
+    if (wait_row_ready<T, CPL>(p, bs)) {
+      ld_row<CPL>(r, p);
+    } else {
+#pragma unroll
+      for (int j = 0; j < CPL; ++j) r.v[j] = T(0);
+    }
+  }
+}
+
+template <int CPL>
+__device__ __forceinline__ void st_row(float* p, const float (&v)[CPL]) {
+  if constexpr (CPL % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < CPL / 4; ++q)
+      asm volatile("st.relaxed.gpu.global.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(p + 4 * q), "f"(v[4 * q]),
+                   "f"(v[4 * q + 1]), "f"(v[4 * q + 2]), "f"(v[4 * q + 3])
+                   : "memory");
+  } else {
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) st_relaxed(p + j, v[j]);
+  }
+}
+template <int CPL>
+__device__ __forceinline__ void st_row(double* p, const double (&v)[CPL]) {
+  if constexpr (CPL % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < CPL / 2; ++q)
+      asm volatile("st.relaxed.gpu.global.v2.f64 [%0], {%1,%2};" ::"l"(p + 2 * q), "d"(v[2 * q]), "d"(v[2 * q + 1])
+                   : "memory");
+  } else {
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) st_relaxed(p + j, v[j]);
+  }
+}
+
+// ---- batched sync-free sweep -----------------------------------------------
+//
+// Task records as in k_sweep.  Groups of 8 lanes; lane l of a group owns
+// columns [l*CPL, (l+1)*CPL).  A light task puts one vertex on each group;
+// a heavy task puts its one vertex on all four groups, group g taking the
+// entries 8g..8g+7 of every round of 32, and the four partial sums are
+// combined with shuffles.  In round j lane l of a group holds entry
+// gl + j*gw of the vertex (the first four rounds are prefetched with the
+// task), broadcasts it to its group, and the group loads the input rows in
+// batches of EB with every load issued before any is checked.
+template <typename T, int CPL, bool kForward>
+__global__ void __launch_bounds__(kSweepThreads) kb_sweep(int ntasks, const SweepTask* __restrict__ tasks,
+                                                          const int* __restrict__ idx, const T* __restrict__ coef,
+                                                          const T* __restrict__ aux, const T* __restrict__ sfwd,
+                                                          T* out, BatchShared* bs) {
+  if (bs->all_done) return;
+  constexpr int kp = CPL * kBatchLanes;
+  constexpr int EB = (CPL * sizeof(T) >= 32) ? 2 : (CPL * sizeof(T) >= 16 ? 4 : 8);
+  const int lane = threadIdx.x & 31;
+  const int gl = lane & 7;
+  const int W = (int)((gridDim.x * blockDim.x) >> 5);
+  int t = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  SweepTask r1 = load_task(tasks, t + W, ntasks);
+  SweepEntries<T> e0;
+  {
+    const SweepTask r0 = load_task(tasks, t, ntasks);
+    load_entries<T, true, false>(e0, r0, lane, idx, coef, coef, coef);
+  }
+  for (; t < ntasks; t += W) {
+    const SweepTask r2 = load_task(tasks, t + 2 * W, ntasks);
+    SweepEntries<T> e1;
+    load_entries<T, true, false>(e1, r1, lane, idx, coef, coef, coef);
+    const int gw = e0.gw;  // 32 for a heavy task, 8 for a light one (uniform per warp)
+    const int k0 = e0.k0 - (gw == 32 ? lane : gl);  // first entry of this lane's vertex
+    T acc[CPL];
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) acc[j] = T(0);
+    Row<T, CPL> a;
+    if (e0.active && (gw == 8 || lane < 8)) {
+#pragma unroll
+      for (int j = 0; j < CPL; ++j)
+        a.v[j] = kForward ? __ldg(&aux[(size_t)e0.v * kp + gl * CPL + j])
+                          : __ldg(&aux[e0.v]) * __ldg(&sfwd[(size_t)e0.v * kp + gl * CPL + j]);
+    }
+    int rounds = e0.active ? (e0.k1 - k0 + gw - 1) / gw : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) rounds = max(rounds, __shfl_xor_sync(0xffffffffu, rounds, o));
+    for (int j = 0; j < rounds; ++j) {
+      int myid;
+      T myc;
+      if (j < kEntryUnroll) {
+        myid = e0.id[0];
+        myc = e0.c[0];
+#pragma unroll
+        for (int q = 1; q < kEntryUnroll; ++q)
+          if (q == j) {
+            myid = e0.id[q];
+            myc = e0.c[q];
+          }
+      } else {
+        const int k = e0.k0 + j * gw;
+        myid = (e0.active && k < e0.k1) ? __ldg(&idx[k]) : -1;
+        myc = (e0.active && k < e0.k1) ? __ldg(&coef[k]) : T(0);
+      }
+#pragma unroll
+      for (int l0 = 0; l0 < 8; l0 += EB) {
+        Row<T, CPL> vals[EB];
+        T cs[EB];
+        int ids[EB];
+#pragma unroll
+        for (int u = 0; u < EB; ++u) {
+          ids[u] = __shfl_sync(0xffffffffu, myid, (lane & ~7) | (l0 + u));
+          cs[u] = __shfl_sync(0xffffffffu, myc, (lane & ~7) | (l0 + u));
+        }
+#pragma unroll
+        for (int u = 0; u < EB; ++u)
+          if (ids[u] >= 0) ld_row<CPL>(vals[u], out + (size_t)ids[u] * kp + gl * CPL);
+#pragma unroll
+        for (int u = 0; u < EB; ++u) {
+          if (ids[u] < 0) continue;
+          if (row_pending(vals[u])) {
+            const T* pr = out + (size_t)ids[u] * kp + gl * CPL;
+            if (wait_row_ready<T, CPL>(pr, bs)) {
+              ld_row<CPL>(vals[u], pr);
+            } else {
+#pragma unroll
+              for (int q = 0; q < CPL; ++q) vals[u].v[q] = T(0);
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) acc[q] += cs[u] * vals[u].v[q];
+        }
+      }
+    }
+    if (gw == 32) {  // combine the four groups of a heavy task
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) {
+        acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], 8);
+        acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], 16);
+      }
+    }
+    if (e0.active && (gw == 8 || lane < 8)) {
+      T res[CPL];
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) res[q] = a.v[q] + acc[q];
+      st_row<CPL>(out + (size_t)e0.v * kp + gl * CPL, res);
+    }
+    e0 = e1;
+    r1 = r2;
+  }
+}
+
+// ---- batched mat-vec: q = L p for kp columns -------------------------------
+
+template <typename T, int CPL>
+__global__ void __launch_bounds__(kVecThreads) kb_spmv(int n, const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                       const T* __restrict__ val, const T* __restrict__ p,
+                                                       T* __restrict__ q, const BatchShared* bs) {
+  if (bs && bs->all_done) return;
+  constexpr int kp = CPL * kBatchLanes;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gl = gt & 7;
+  const int groups = gridDim.x * blockDim.x / 8;
+  for (int row = gt / 8; row < n; row += groups) {
+    const int k0 = __ldg(&ptr[row]), k1 = __ldg(&ptr[row + 1]);
+    T acc[CPL];
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) acc[j] = T(0);
+    for (int k = k0; k < k1; ++k) {
+      const int id = __ldg(&idx[k]);
+      const T c = __ldg(&val[k]);
+      const T* pr = p + (size_t)id * kp + gl * CPL;
+#pragma unroll
+      for (int j = 0; j < CPL; ++j) acc[j] += c * pr[j];
+    }
+    T* qr = q + (size_t)row * kp + gl * CPL;
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) qr[j] = acc[j];
+  }
+}
+
+// ---- per-column reductions ---------------------------------------------------
+//
+// Element i = v*kp + c is visited by threads of a fixed column (blockDim and
+// the grid stride are multiples of kp).  Block sums per column go through
+// shared memory in thread order, partials per (block, column) are summed by
+// the last block in block order: deterministic for a given n and kp.
+
+template <int NV>
+__device__ __forceinline__ bool batch_reduce(double (&v)[NV], int kp, double* partials, unsigned int* counter,
+                                             double (&out)[NV]) {
+  __shared__ double sm[NV][kVecThreads];
+  __shared__ bool am_last;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) sm[q][threadIdx.x] = v[q];
+  __syncthreads();
+  const int per = blockDim.x / kp;
+  if ((int)threadIdx.x < kp) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (int j = 0; j < per; ++j) s += sm[q][threadIdx.x + j * kp];
+      partials[((size_t)q * gridDim.x + blockIdx.x) * kp + threadIdx.x] = s;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  if ((int)threadIdx.x < kp) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(&partials[((size_t)q * gridDim.x + b) * kp + threadIdx.x]);
+      out[q] = s;
+    }
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
+// After the per-column scalar steps: end the launch's loop when all columns stopped.
+__device__ __forceinline__ void batch_check_all(PcgState* st, BatchShared* bs, int kp, const LoopCtl& ctl) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool all = true;
+    for (int c = 0; c < kp; ++c) all &= (st[c].done != 0);
+    if (all) {
+      bs->all_done = 1;
+      clear_loop(ctl);
+    }
+  }
+}
+
+// pq, |p|_1, |q|_1 per column -> alpha, stagnation tests 1 and 2
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_pq(int n, int kp, const T* __restrict__ p, const T* __restrict__ q,
+                                                     PcgState* st, BatchShared* bs, double* partials, double eps,
+                                                     LoopCtl ctl) {
+  if (bs->all_done) return;
+  const size_t N = (size_t)n * kp;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    const double pv = (double)p[i], qv = (double)q[i];
+    acc[0] += pv * qv;
+    acc[1] += fabs(pv);
+    acc[2] += fabs(qv);
+  }
+  double tot[3];
+  if (batch_reduce<3>(acc, kp, partials, &bs->counter[0], tot)) {
+    const int c = threadIdx.x;
+    if (c < kp && !st[c].done) pcg_scalar_pq(&st[c], tot[0], tot[1], tot[2], eps);
+    batch_check_all(st, bs, kp, ctl);
+  }
+}
+
+// x' = x + alpha p, r -= alpha q (active columns); s, y pending; |r|^2, |x'|_1, |r|_1
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_update(int n, int kp, T* x3, const T* __restrict__ p,
+                                                         const T* __restrict__ q, T* __restrict__ r, T* __restrict__ s_out,
+                                                         T* __restrict__ y_out, PcgState* st, BatchShared* bs,
+                                                         double* partials, LoopCtl ctl) {
+  if (bs->all_done) return;
+  const size_t N = (size_t)n * kp;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(i0 % kp);
+  const bool act = !st[c].done;
+  const double al = st[c].alpha;
+  const T* xc = x3 + (size_t)st[c].xcur * N;
+  T* xn = x3 + (size_t)st[c].xnext * N;
+  const T pend = pending_value<T>();
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (size_t i = i0; i < N; i += stride) {
+    s_out[i] = pend;
+    y_out[i] = pend;
+    if (!act) continue;
+    const T xv = (T)((double)xc[i] + al * (double)p[i]);
+    const T rv = (T)((double)r[i] + (-al) * (double)q[i]);
+    xn[i] = xv;
+    r[i] = rv;
+    acc[0] += (double)rv * (double)rv;
+    acc[1] += fabs((double)xv);
+    acc[2] += fabs((double)rv);
+  }
+  double tot[3];
+  if (batch_reduce<3>(acc, kp, partials, &bs->counter[1], tot)) {
+    const int cc = threadIdx.x;
+    if (cc < kp && !st[cc].done) pcg_scalar_update(&st[cc], tot[0], tot[1], tot[2]);
+    batch_check_all(st, bs, kp, ctl);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_ysum(int n, int kp, const T* __restrict__ y, PcgState* st,
+                                                       BatchShared* bs, double* partials, LoopCtl ctl) {
+  if (bs->all_done) return;
+  const size_t N = (size_t)n * kp;
+  double acc[1] = {0.0};
+  for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+    acc[0] += (double)y[i];
+  double tot[1];
+  if (batch_reduce<1>(acc, kp, partials, &bs->counter[2], tot)) {
+    const int c = threadIdx.x;
+    if (c < kp) {
+      st[c].mean = tot[0] / (double)n;
+      if (bs->sweep_error && !st[c].done) mark_stop(&st[c], kSweepTimeout);
+    }
+    batch_check_all(st, bs, kp, ctl);
+  }
+}
+
+// z = y - mean (in place); rho = z.r, |z|_1; the iteration's remaining scalar steps
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_zdot(int n, int kp, T* __restrict__ yz, const T* __restrict__ r,
+                                                       T* __restrict__ p, PcgState* st, BatchShared* bs,
+                                                       double* partials, double eps, int init, LoopCtl ctl) {
+  if (bs->all_done) return;
+  const size_t N = (size_t)n * kp;
+  const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(i0 % kp);
+  const double mu = st[c].mean;
+  double acc[2] = {0.0, 0.0};
+  for (size_t i = i0; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    const T z = (T)((double)yz[i] - mu);
+    yz[i] = z;
+    if (init) p[i] = z;
+    acc[0] += (double)z * (double)r[i];
+    acc[1] += fabs((double)z);
+  }
+  double tot[2];
+  if (batch_reduce<2>(acc, kp, partials, &bs->counter[3], tot)) {
+    const int cc = threadIdx.x;
+    if (cc < kp && !st[cc].done) pcg_scalar_zdot(&st[cc], tot[0], tot[1], eps, init);
+    batch_check_all(st, bs, kp, ctl);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_pupdate(int n, int kp, const T* __restrict__ z, T* __restrict__ p,
+                                                          const PcgState* st, const BatchShared* bs) {
+  if (bs->all_done) return;
+  const size_t N = (size_t)n * kp;
+  const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(i0 % kp);
+  if (st[c].done) return;
+  const double beta = st[c].beta;
+  for (size_t i = i0; i < N; i += (size_t)gridDim.x * blockDim.x) p[i] = (T)((double)z[i] + beta * (double)p[i]);
+}
+
+// ---- set-up and wrap-up ------------------------------------------------------
+
+// bint[v*kp + c] = B[c*ldb + perm[v]] for c < k, 0 for padding; per-column mean.
+__global__ void __launch_bounds__(kVecThreads) kb_gather_in(int n, int kp, const int* __restrict__ perm,
+                                                            const double* __restrict__ B, long long ldb,
+                                                            double* __restrict__ bint, PcgState* st, BatchShared* bs,
+                                                            double* partials) {
+  const size_t N = (size_t)n * kp;
+  const int k = bs->k;
+  double acc[1] = {0.0};
+  for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    const int v = (int)(i / kp), c = (int)(i % kp);
+    const double x = c < k ? B[(size_t)c * ldb + perm[v]] : 0.0;
+    bint[i] = x;
+    acc[0] += x;
+  }
+  double tot[1];
+  if (batch_reduce<1>(acc, kp, partials, &bs->counter[4], tot)) {
+    const int c = threadIdx.x;
+    if (c < kp) st[c].mean = tot[0] / (double)n;
+  }
+}
+
+// bm = b - mean; r = bm (as T); x0 = 0; s, y pending; per-column |b| and reset.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_center(int n, int kp, double* __restrict__ bm, T* __restrict__ r,
+                                                         T* __restrict__ x0, T* __restrict__ s_out, T* __restrict__ y_out,
+                                                         PcgState* st, BatchShared* bs, double* partials, LoopCtl ctl) {
+  const size_t N = (size_t)n * kp;
+  const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(i0 % kp);
+  const double mu = st[c].mean;
+  const T pend = pending_value<T>();
+  double acc[2] = {0.0, 0.0};
+  for (size_t i = i0; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = bm[i] - mu;
+    bm[i] = v;
+    r[i] = (T)v;
+    x0[i] = T(0);
+    if (s_out) s_out[i] = pend;
+    if (y_out) y_out[i] = pend;
+    acc[0] += v * v;
+    acc[1] += fabs(v);
+  }
+  double tot[2];
+  if (batch_reduce<2>(acc, kp, partials, &bs->counter[5], tot)) {
+    const int cc = threadIdx.x;
+    if (cc < kp) {
+      PcgState* s = &st[cc];
+      s->nb = sqrt(tot[0]);
+      s->nb64 = s->nb;
+      s->scale = s->nb;
+      s->sum_abs_r = tot[1];
+      s->sum_abs_x = 0.0;
+      s->bestnr = 1.0;
+      s->nr = 1.0;
+      s->nr_true = 1.0;
+      s->itcnt = 0;
+      s->total_its = 0;
+      s->outer_its = 0;
+      s->stag_count = 0;
+      s->status = kMaxits;
+      s->done = 0;
+      s->outer_done = 0;
+      s->xcur = 0;
+      s->xbest = 0;
+      s->xnext = 1;
+      s->t_start = globaltimer_ns();
+      if (s->nb == 0.0) {
+        s->nr_true = 0.0;
+        s->nr = 0.0;
+        s->outer_done = 1;
+        mark_stop(s, kConverged);
+      }
+    }
+    if (threadIdx.x == 0) {
+      bs->sweep_error = 0;
+      bs->all_done = 0;
+    }
+    batch_check_all(st, bs, kp, ctl);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_take_best(int n, int kp, const T* __restrict__ x3,
+                                                            double* __restrict__ xf, const PcgState* st) {
+  const size_t N = (size_t)n * kp;
+  const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(i0 % kp);
+  const T* xb = x3 + (size_t)st[c].xbest * N;
+  for (size_t i = i0; i < N; i += (size_t)gridDim.x * blockDim.x) xf[i] = (double)xb[i];
+}
+
+// t = bm - L x (FP64), optionally stored; per column |t| -> nr_true, scale.
+template <int CPL>
+__global__ void __launch_bounds__(kVecThreads) kb_true_residual(int n, const int* __restrict__ ptr,
+                                                                const int* __restrict__ idx,
+                                                                const double* __restrict__ val,
+                                                                const double* __restrict__ x,
+                                                                const double* __restrict__ bm, double* __restrict__ rout,
+                                                                PcgState* st, BatchShared* bs, double* partials) {
+  constexpr int kp = CPL * kBatchLanes;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gl = gt & 7;
+  const int groups = gridDim.x * blockDim.x / 8;
+  double acc[CPL];
+#pragma unroll
+  for (int j = 0; j < CPL; ++j) acc[j] = 0.0;
+  for (int row = gt / 8; row < n; row += groups) {
+    const int k0 = __ldg(&ptr[row]), k1 = __ldg(&ptr[row + 1]);
+    double s[CPL];
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) s[j] = 0.0;
+    for (int k = k0; k < k1; ++k) {
+      const int id = __ldg(&idx[k]);
+      const double c = __ldg(&val[k]);
+      const double* xr = x + (size_t)id * kp + gl * CPL;
+#pragma unroll
+      for (int j = 0; j < CPL; ++j) s[j] += c * xr[j];
+    }
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) {
+      const size_t e = (size_t)row * kp + gl * CPL + j;
+      const double t = bm[e] - s[j];
+      if (rout) rout[e] = t;
+      acc[j] += t * t;
+    }
+  }
+  // per column reduction: thread holds columns gl*CPL + j
+  __shared__ double sm[kVecThreads][CPL];
+  __shared__ bool am_last;
+#pragma unroll
+  for (int j = 0; j < CPL; ++j) sm[threadIdx.x][j] = acc[j];
+  __syncthreads();
+  if ((int)threadIdx.x < kp) {
+    const int lane8 = threadIdx.x / CPL, j = threadIdx.x % CPL;
+    double s = 0.0;
+    for (int t = lane8; t < (int)blockDim.x; t += 8) s += sm[t][j];
+    partials[(size_t)blockIdx.x * kp + threadIdx.x] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    am_last = atomicAdd(&bs->counter[6], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  if ((int)threadIdx.x < kp) {
+    double s = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(&partials[(size_t)b * kp + threadIdx.x]);
+    PcgState* p = &st[threadIdx.x];
+    p->scale = sqrt(s);
+    p->nr_true = p->nb64 > 0.0 ? p->scale / p->nb64 : 0.0;
+  }
+  if (threadIdx.x == 0) bs->counter[6] = 0u;
+}
+
+// X[c*ldx + perm[v]] = xf[v*kp + c], c < k
+__global__ void __launch_bounds__(kVecThreads) kb_scatter_out(int n, int kp, const int* __restrict__ perm,
+                                                              const double* __restrict__ xf, double* __restrict__ X,
+                                                              long long ldx, const BatchShared* bs) {
+  const size_t N = (size_t)n * kp;
+  const int k = bs->k;
+  for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    const int v = (int)(i / kp), c = (int)(i % kp);
+    if (c < k) X[(size_t)c * ldx + perm[v]] = xf[i];
+  }
+}
+
+// ---- mixed precision outer loop (per column) ---------------------------------
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_outer_prep(int n, int kp, const double* __restrict__ r64,
+                                                             T* __restrict__ rin, T* __restrict__ x0,
+                                                             T* __restrict__ s_out, T* __restrict__ y_out, PcgState* st,
+                                                             BatchShared* bs, double* partials, LoopCtl inner_ctl) {
+  const size_t N = (size_t)n * kp;
+  const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(i0 % kp);
+  const bool act = !st[c].outer_done;
+  const double inv = act ? 1.0 / st[c].scale : 0.0;
+  const T pend = pending_value<T>();
+  double acc[2] = {0.0, 0.0};
+  for (size_t i = i0; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    const T v = act ? (T)(r64[i] * inv) : T(0);
+    rin[i] = v;
+    x0[i] = T(0);
+    s_out[i] = pend;
+    y_out[i] = pend;
+    acc[0] += (double)v * (double)v;
+    acc[1] += fabs((double)v);
+  }
+  double tot[2];
+  if (batch_reduce<2>(acc, kp, partials, &bs->counter[7], tot)) {
+    const int cc = threadIdx.x;
+    if (cc < kp) {
+      PcgState* s = &st[cc];
+      if (s->outer_done) {
+        s->done = 1;
+      } else {
+        s->nb = sqrt(tot[0]);
+        s->sum_abs_r = tot[1];
+        s->sum_abs_x = 0.0;
+        s->bestnr = 1.0;
+        s->nr = 1.0;
+        s->itcnt = 0;
+        s->stag_count = 0;
+        s->status = kMaxits;
+        s->done = 0;
+        s->xcur = 0;
+        s->xbest = 0;
+        s->xnext = 1;
+        s->tol = s->inner_tol;
+        if (s->nb == 0.0) mark_stop(s, kConverged);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      bool all = true;
+      for (int q = 0; q < kp; ++q) all &= (st[q].done != 0);
+      bs->all_done = all ? 1 : 0;
+      if (inner_ctl.use_handle) cudaGraphSetConditional(inner_ctl.handle, all ? 0u : 1u);
+    }
+  }
+}
+
+// x64 += scale * x_in[best] for columns still refining
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kb_outer_correct(int n, int kp, const T* __restrict__ x3,
+                                                                double* __restrict__ x64, const PcgState* st) {
+  const size_t N = (size_t)n * kp;
+  const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(i0 % kp);
+  if (st[c].outer_done) return;
+  const T* xb = x3 + (size_t)st[c].xbest * N;
+  const double sc = st[c].scale;
+  for (size_t i = i0; i < N; i += (size_t)gridDim.x * blockDim.x) x64[i] += sc * (double)xb[i];
+}
+
+// per column: account iterations, decide, set the next inner tolerance
+__global__ void kb_outer_decide(PcgState* st, BatchShared* bs, int kp, LoopCtl outer_ctl) {
+  const int c = threadIdx.x;
+  if (c < kp) {
+    PcgState* s = &st[c];
+    if (!s->outer_done) {
+      s->total_its += s->itcnt;
+      s->outer_its += 1;
+      const int inner_status = s->status;
+      const bool progressed = s->itcnt > 0 && s->bestnr < 1.0;
+      int stop = -1;
+      if (bs->sweep_error || inner_status == kSweepTimeout) stop = kSweepTimeout;
+      else if (s->nr_true <= s->tol_user) stop = kConverged;
+      else if (s->total_its >= s->maxits_user) stop = kMaxits;
+      else if (s->outer_its >= s->max_outer) stop = kStagX;
+      else if (!progressed) stop = inner_status == kMaxits ? kStagRho : inner_status;
+      else if ((double)(globaltimer_ns() - s->t_start) * 1e-9 > s->maxtime_s) stop = kMaxtime;
+      if (stop >= 0) {
+        s->outer_done = 1;
+        s->status = stop;
+      } else {
+        double it = 0.5 * s->tol_user / s->nr_true;
+        if (it < s->min_inner_tol) it = s->min_inner_tol;
+        if (it > 0.25) it = 0.25;
+        s->inner_tol = it;
+        s->maxits = s->maxits_user - s->total_its;
+      }
+    }
+  }
+  __syncthreads();
+  if (c == 0) {
+    bool all = true;
+    for (int q = 0; q < kp; ++q) all &= (st[q].outer_done != 0);
+    if (all && outer_ctl.use_handle) cudaGraphSetConditional(outer_ctl.handle, 0u);
+  }
+}
+
+}  // namespace acg

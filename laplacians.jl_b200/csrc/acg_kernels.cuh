@@ -439,7 +439,7 @@ __device__ __forceinline__ SweepTask load_task(const SweepTask* __restrict__ tas
   return r;
 }
 
-template <typename T, bool kForward>
+template <typename T, bool kForward, bool kLoadAux = true>
 __device__ __forceinline__ void load_entries(SweepEntries<T>& e, const SweepTask& r, int lane,
                                              const int* __restrict__ idx, const T* __restrict__ coef,
                                              const T* __restrict__ aux, const T* __restrict__ sfwd) {
@@ -458,8 +458,8 @@ __device__ __forceinline__ void load_entries(SweepEntries<T>& e, const SweepTask
   if (!e.active) k0 = k1 = 0;
   e.k0 = k0 + gl;
   e.k1 = k1;
-  e.a = e.active ? __ldg(&aux[e.v]) : T(0);
-  e.own = (!kForward && e.active) ? __ldg(&sfwd[e.v]) : T(0);
+  e.a = (kLoadAux && e.active) ? __ldg(&aux[e.v]) : T(0);
+  e.own = (kLoadAux && !kForward && e.active) ? __ldg(&sfwd[e.v]) : T(0);
 #pragma unroll
   for (int j = 0; j < kEntryUnroll; ++j) {
     const int k = e.k0 + j * gw;
@@ -492,9 +492,16 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const Sweep
     load_entries<T, kForward>(e1, r1, lane, idx, coef, aux, sfwd);
     const int gw = e0.gw;  // uniform across the warp: one task per warp
     T acc = T(0);
+    // issue the loads of all prefetched entries before checking any of them
+    T xv[kEntryUnroll];
 #pragma unroll
-    for (int j = 0; j < kEntryUnroll; ++j)
-      if (e0.id[j] >= 0) acc += e0.c[j] * wait_value(&out[e0.id[j]], st, poll_mode);
+    for (int j = 0; j < kEntryUnroll; ++j) xv[j] = e0.id[j] >= 0 ? ld_relaxed(&out[e0.id[j]]) : T(0);
+#pragma unroll
+    for (int j = 0; j < kEntryUnroll; ++j) {
+      if (e0.id[j] < 0) continue;
+      if (is_pending(xv[j])) xv[j] = wait_value_slow(&out[e0.id[j]], st, poll_mode);
+      acc += e0.c[j] * xv[j];
+    }
     for (int k = e0.k0 + kEntryUnroll * gw; k < e0.k1; k += gw)
       acc += __ldg(&coef[k]) * wait_value(&out[__ldg(&idx[k])], st, poll_mode);
     acc = group_sum_w(acc, gw);

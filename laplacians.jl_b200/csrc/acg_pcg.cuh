@@ -43,6 +43,89 @@ __device__ __forceinline__ int pick_free_buffer(int cur, int best) {
   return (cur + 1) % 3;
 }
 
+__device__ __forceinline__ bool mark_stop(PcgState* st, int code) {
+  st->status = code;
+  st->done = 1;
+  return true;
+}
+
+// ---- scalar steps of one PCG iteration for one system ---------------------
+// Each returns true when the system stopped (status and done are then set).
+// Shared by the one-right-hand-side kernels (thread 0) and the batched
+// kernels (thread c for column c).
+
+// after q = L p: alpha and the first two L1 stagnation tests (src/pcg.jl:288-338)
+__device__ __forceinline__ bool pcg_scalar_pq(PcgState* st, double pq, double sum_abs_p, double sum_abs_q,
+                                              double eps) {
+  st->itcnt += 1;
+  st->sum_abs_p = sum_abs_p;
+  st->sum_abs_q = sum_abs_q;
+  const double al = st->rho / pq;
+  st->alpha = al;
+  if (st->itcnt % 10 == 0) {
+    if (al * st->sum_abs_p < eps * st->sum_abs_x) return mark_stop(st, kStagX);
+    if (al * st->sum_abs_q < eps * st->sum_abs_r) return mark_stop(st, kStagR);
+  }
+  return false;
+}
+
+// after x += alpha p, r -= alpha q: |r|/|b|, bestx, convergence (src/pcg.jl:348-361)
+__device__ __forceinline__ bool pcg_scalar_update(PcgState* st, double rr, double sum_abs_x, double sum_abs_r) {
+  const double nr = sqrt(rr) / st->nb;
+  st->nr = nr;
+  st->sum_abs_x = sum_abs_x;
+  st->sum_abs_r = sum_abs_r;
+  const int xc_new = st->xnext;
+  st->xcur = xc_new;
+  if (nr < st->bestnr) {
+    st->bestnr = nr;
+    st->xbest = xc_new;
+  }
+  st->xnext = pick_free_buffer(xc_new, st->xbest);
+  if (nr < st->tol) return mark_stop(st, kConverged);
+  return false;
+}
+
+// after z = pre(r), rho = z.r: stagnation, inf, beta, third L1 test, maxtime,
+// maxits (src/pcg.jl:365-432).  init: the pre-loop rho (1 also starts the clock).
+__device__ __forceinline__ bool pcg_scalar_zdot(PcgState* st, double zr, double sum_abs_z, double eps, int init) {
+  st->sum_abs_z = sum_abs_z;
+  if (init) {
+    st->rho = zr;
+    st->best_rho = zr;
+    st->stag_count = 0;
+    if (init == 1) st->t_start = globaltimer_ns();
+    if (st->itcnt >= st->maxits) return mark_stop(st, kMaxits);
+    return false;
+  }
+  const double oldrho = st->rho;
+  const double rho = zr;
+  st->rho = rho;
+  const double thr = 1.0 - 1.0 / (double)st->stag_test;
+  if (rho < st->best_rho * thr) {
+    st->best_rho = rho;
+    st->stag_count = 0;
+  } else if (st->stag_test > 0) {
+    if (st->best_rho > thr * rho) {
+      st->stag_count += 1;
+      if (st->stag_count > st->stag_test) return mark_stop(st, kStagRho);
+    }
+  }
+  if (isinf(rho)) return mark_stop(st, kInf);
+  const double beta = rho / oldrho;
+  st->beta = beta;
+  if (isinf(beta)) return mark_stop(st, kInf);
+  if (st->itcnt % 10 == 0 && beta * st->sum_abs_p < eps * st->sum_abs_z) return mark_stop(st, kStagP);
+  const double el = (double)(globaltimer_ns() - st->t_start) * 1e-9;
+  if (el > st->maxtime_s) return mark_stop(st, kMaxtime);
+  if (st->itcnt >= st->maxits) return mark_stop(st, kMaxits);
+  return false;
+}
+
+__device__ __forceinline__ void clear_loop(const LoopCtl& ctl) {
+  if (ctl.use_handle) cudaGraphSetConditional(ctl.handle, 0u);
+}
+
 // ---- iteration kernels ---------------------------------------------------
 
 template <typename T, int VL>
@@ -66,17 +149,8 @@ __global__ void __launch_bounds__(kVecThreads) k_spmv_pq(int n, const int* __res
       acc[2] += fabs((double)s);
     }
   }
-  if (grid_reduce<3>(acc, partials, &st->counter[0]) && threadIdx.x == 0) {
-    st->itcnt += 1;
-    st->sum_abs_p = acc[1];
-    st->sum_abs_q = acc[2];
-    const double al = st->rho / acc[0];
-    st->alpha = al;
-    if (st->itcnt % 10 == 0) {
-      if (al * st->sum_abs_p < eps * st->sum_abs_x) pcg_stop(st, kStagX, ctl);
-      else if (al * st->sum_abs_q < eps * st->sum_abs_r) pcg_stop(st, kStagR, ctl);
-    }
-  }
+  if (grid_reduce<3>(acc, partials, &st->counter[0]) && threadIdx.x == 0)
+    if (pcg_scalar_pq(st, acc[0], acc[1], acc[2], eps)) clear_loop(ctl);
 }
 
 // Also marks the two sweep output vectors (s, y) pending for the next sweeps.
@@ -101,20 +175,8 @@ __global__ void __launch_bounds__(kVecThreads) k_update(int n, T* x3, const T* _
     acc[1] += fabs((double)xv);
     acc[2] += fabs((double)rv);
   }
-  if (grid_reduce<3>(acc, partials, &st->counter[1]) && threadIdx.x == 0) {
-    const double nr = sqrt(acc[0]) / st->nb;
-    st->nr = nr;
-    st->sum_abs_x = acc[1];
-    st->sum_abs_r = acc[2];
-    const int xc_new = st->xnext;
-    st->xcur = xc_new;
-    if (nr < st->bestnr) {
-      st->bestnr = nr;
-      st->xbest = xc_new;
-    }
-    st->xnext = pick_free_buffer(xc_new, st->xbest);
-    if (nr < st->tol) pcg_stop(st, kConverged, ctl);
-  }
+  if (grid_reduce<3>(acc, partials, &st->counter[1]) && threadIdx.x == 0)
+    if (pcg_scalar_update(st, acc[0], acc[1], acc[2])) clear_loop(ctl);
 }
 
 template <typename T>
@@ -146,41 +208,8 @@ __global__ void __launch_bounds__(kVecThreads) k_zdot(int n, T* __restrict__ yz,
     acc[0] += (double)z * (double)r[i];
     acc[1] += fabs((double)z);
   }
-  if (grid_reduce<2>(acc, partials, &st->counter[3]) && threadIdx.x == 0) {
-    st->sum_abs_z = acc[1];
-    if (init) {
-      st->rho = acc[0];
-      st->best_rho = acc[0];
-      st->stag_count = 0;
-      if (init == 1) st->t_start = globaltimer_ns();
-      if (st->itcnt >= st->maxits) pcg_stop(st, kMaxits, ctl);
-      return;
-    }
-    const double oldrho = st->rho;
-    const double rho = acc[0];
-    st->rho = rho;
-    const double thr = 1.0 - 1.0 / (double)st->stag_test;
-    if (rho < st->best_rho * thr) {
-      st->best_rho = rho;
-      st->stag_count = 0;
-    } else if (st->stag_test > 0) {
-      if (st->best_rho > thr * rho) {
-        st->stag_count += 1;
-        if (st->stag_count > st->stag_test) {
-          pcg_stop(st, kStagRho, ctl);
-          return;
-        }
-      }
-    }
-    if (isinf(rho)) { pcg_stop(st, kInf, ctl); return; }
-    const double beta = rho / oldrho;
-    st->beta = beta;
-    if (isinf(beta)) { pcg_stop(st, kInf, ctl); return; }
-    if (st->itcnt % 10 == 0 && beta * st->sum_abs_p < eps * st->sum_abs_z) { pcg_stop(st, kStagP, ctl); return; }
-    const double el = (double)(globaltimer_ns() - st->t_start) * 1e-9;
-    if (el > st->maxtime_s) { pcg_stop(st, kMaxtime, ctl); return; }
-    if (st->itcnt >= st->maxits) { pcg_stop(st, kMaxits, ctl); return; }
-  }
+  if (grid_reduce<2>(acc, partials, &st->counter[3]) && threadIdx.x == 0)
+    if (pcg_scalar_zdot(st, acc[0], acc[1], eps, init)) clear_loop(ctl);
 }
 
 template <typename T>

@@ -15,7 +15,7 @@
 
 #include "../../include/acgpu.h"
 #include "acg_internal.h"
-#include "acg_pcg.cuh"
+#include "acg_batch.cuh"
 
 namespace acg {
 
@@ -108,9 +108,26 @@ struct SolverImpl {
   std::mutex mu;
   unsigned char* noalloc_scratch = nullptr;  // device address of the fixed scratch array
 
+  // batched solves: kp right-hand sides per launch (vertex-major n x kp blocks)
+  int batch_kp = 0;  // capacity of the batch buffers
+  DevBuf<double> bb_ext, bx_ext, bbm, br64, bxf, bpartials;
+  DevBuf<float> br32, bs32, by32, bp32, bq32, bx3_32;
+  DevBuf<double> bs64, by64, bp64, bq64, bx3_64;
+  PcgState* bst = nullptr;
+  BatchShared* bsh = nullptr;
+  PcgState* h_bst = nullptr;
+  int bsweep_blocks[2][4] = {};          // [precision][log2(kp/8)]
+  cudaGraphExec_t bexec[2][4] = {};
+
   ~SolverImpl() {
     for (auto& e : exec)
       if (e) cudaGraphExecDestroy(e);
+    for (auto& row : bexec)
+      for (auto& e : row)
+        if (e) cudaGraphExecDestroy(e);
+    if (bst) cudaFree(bst);
+    if (bsh) cudaFree(bsh);
+    if (h_bst) cudaFreeHost(h_bst);
     if (st) cudaFree(st);
     if (h_st) cudaFreeHost(h_st);
     if (stream) cudaStreamDestroy(stream);
@@ -608,7 +625,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     std::vector<int> outdeg(n, 0);
     for (int v = 0; v < n; ++v) outdeg[v] = bptr[v + 1] - bptr[v];
     auto emit_level = [](std::vector<SweepTask>& tasks, int vs, int ve, const std::vector<int>& deg,
-                         const std::vector<int>& ptr) {
+                         const std::vector<int>& ptr, int heavy_min) {
       int run = -1, cnt = 0;
       auto push = [&](int v, int c, int heavy) {
         SweepTask t = {};
@@ -622,7 +639,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
         cnt = 0;
       };
       for (int v = vs; v < ve; ++v) {
-        if (deg[v] > 32) {
+        if (deg[v] > heavy_min) {
           flush();
           push(v, 1, 1);
           continue;
@@ -635,8 +652,8 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     std::vector<int> fdeg(n);
     for (int v = 0; v < n; ++v) fdeg[v] = fptr[v + 1] - fptr[v];
     std::vector<SweepTask> tf, tb;
-    for (int l = 0; l < nlev; ++l) emit_level(tf, S.lvl_off[l], S.lvl_off[l + 1], fdeg, fptr);
-    for (int l = nlev - 1; l >= 0; --l) emit_level(tb, S.lvl_off[l], S.lvl_off[l + 1], outdeg, bptr);
+    for (int l = 0; l < nlev; ++l) emit_level(tf, S.lvl_off[l], S.lvl_off[l + 1], fdeg, fptr, 32);
+    for (int l = nlev - 1; l >= 0; --l) emit_level(tb, S.lvl_off[l], S.lvl_off[l + 1], outdeg, bptr, 32);
     S.ntasks_f = (int)tf.size();
     S.ntasks_b = (int)tb.size();
     S.tasks_f.upload(tf, S.stream);
@@ -897,6 +914,264 @@ int status_to_rc(int status) {
   return status;
 }
 
+// ============================================================================
+// Batched solves: up to 64 right-hand sides per launch
+// ============================================================================
+
+int kp_index(int kp) { return kp == 8 ? 0 : kp == 16 ? 1 : kp == 32 ? 2 : 3; }
+int round_kp(int k) { return k <= 8 ? 8 : k <= 16 ? 16 : k <= 32 ? 32 : 64; }
+
+template <typename F>
+void with_cpl(int kp, F&& f) {
+  switch (kp) {
+    case 8: f(std::integral_constant<int, 1>()); break;
+    case 16: f(std::integral_constant<int, 2>()); break;
+    case 32: f(std::integral_constant<int, 4>()); break;
+    default: f(std::integral_constant<int, 8>()); break;
+  }
+}
+
+template <typename T, int CPL, bool kForward>
+void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sfwd, T* out) {
+  const TypedArrays<T> A = arrays_of<T>(S);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(S.bsweep_blocks[plan_index<T>()][kp_index(CPL * kBatchLanes)]);
+  cfg.blockDim = dim3(kSweepThreads);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ACG_CUDA(cudaLaunchKernelEx(&cfg, kb_sweep<T, CPL, kForward>, kForward ? S.ntasks_f : S.ntasks_b,
+                              (const SweepTask*)(kForward ? S.tasks_f.p : S.tasks_b.p), kForward ? A.fi : A.bi,
+                              kForward ? A.fc : A.bc, aux, sfwd, out, S.bsh));
+}
+
+template <typename T, int CPL>
+void enqueue_bsweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y) {
+  enqueue_bsweep<T, CPL, true>(s, S, r, (const T*)nullptr, sv);
+  enqueue_bsweep<T, CPL, false>(s, S, arrays_of<T>(S).g, sv, y);
+}
+
+template <typename T, int CPL>
+void enqueue_biteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* y, T* p, T* q, T* x3, double eps,
+                        LoopCtl ctl) {
+  constexpr int kp = CPL * kBatchLanes;
+  const TypedArrays<T> A = arrays_of<T>(S);
+  const int n = S.n;
+  kb_spmv<T, CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, p, q, S.bsh);
+  kb_pq<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, ctl);
+  kb_update<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, x3, p, q, r, sv, y, S.bst, S.bsh, S.bpartials.p, ctl);
+  enqueue_bsweeps<T, CPL>(s, S, r, sv, y);
+  kb_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, y, S.bst, S.bsh, S.bpartials.p, ctl);
+  kb_zdot<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, y, r, p, S.bst, S.bsh, S.bpartials.p, eps, 0, ctl);
+  kb_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, y, p, S.bst, S.bsh);
+}
+
+template <int CPL>
+cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S) {
+  constexpr int kp = CPL * kBatchLanes;
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  const size_t N = (size_t)n * kp;
+  cudaGraph_t top;
+  ACG_CUDA(cudaGraphCreate(&top, 0));
+  cudaGraphConditionalHandle h;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&h, top, 1u, cudaGraphCondAssignDefault));
+  LoopCtl ctl{h, 1};
+  double* x3 = S.bx3_64.p;
+  begin_into(s, top, {});
+  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bb_ext.p, (long long)n, S.bbm.p, S.bst, S.bsh,
+                                                  S.bpartials.p);
+  kb_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, x3, S.bs64.p, S.by64.p, S.bst,
+                                                       S.bsh, S.bpartials.p, ctl);
+  enqueue_bsweeps<double, CPL>(s, S, S.br64.p, S.bs64.p, S.by64.p);
+  kb_ysum<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.by64.p, S.bst, S.bsh, S.bpartials.p, ctl);
+  kb_zdot<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.by64.p, S.br64.p, S.bp64.p, S.bst, S.bsh,
+                                                     S.bpartials.p, kEps64, 1, ctl);
+  std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
+  end_into(s);
+  cudaGraph_t body;
+  cudaGraphNode_t wnode = add_while(top, leaves, h, &body);
+  begin_into(s, body, {});
+  enqueue_biteration<double, CPL>(s, S, S.br64.p, S.bs64.p, S.by64.p, S.bp64.p, S.bq64.p, x3, kEps64, ctl);
+  end_into(s);
+  begin_into(s, top, {wnode});
+  kb_take_best<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, x3, S.bxf.p, S.bst);
+  kb_true_residual<CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.bxf.p, S.bbm.p,
+                                                           nullptr, S.bst, S.bsh, S.bpartials.p);
+  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, S.bx_ext.p, (long long)n, S.bsh);
+  end_into(s);
+  (void)N;
+  cudaGraphExec_t exec;
+  ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
+  cudaGraphDestroy(top);
+  return exec;
+}
+
+template <int CPL>
+cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S) {
+  constexpr int kp = CPL * kBatchLanes;
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  const double eps32 = 1.1920928955078125e-07;
+  cudaGraph_t top;
+  ACG_CUDA(cudaGraphCreate(&top, 0));
+  cudaGraphConditionalHandle ho;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&ho, top, 1u, cudaGraphCondAssignDefault));
+  LoopCtl octl{ho, 1};
+  begin_into(s, top, {});
+  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bb_ext.p, (long long)n, S.bbm.p, S.bst, S.bsh,
+                                                  S.bpartials.p);
+  kb_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, S.bxf.p, (double*)nullptr,
+                                                       (double*)nullptr, S.bst, S.bsh, S.bpartials.p, octl);
+  std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
+  end_into(s);
+  cudaGraph_t obody;
+  cudaGraphNode_t onode = add_while(top, leaves, ho, &obody);
+  cudaGraphConditionalHandle hi;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&hi, obody, 1u, cudaGraphCondAssignDefault));
+  LoopCtl ictl{hi, 1};
+  begin_into(s, obody, {});
+  kb_outer_prep<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.br64.p, S.br32.p, S.bx3_32.p, S.bs32.p, S.by32.p,
+                                                          S.bst, S.bsh, S.bpartials.p, ictl);
+  enqueue_bsweeps<float, CPL>(s, S, S.br32.p, S.bs32.p, S.by32.p);
+  kb_ysum<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.by32.p, S.bst, S.bsh, S.bpartials.p, ictl);
+  kb_zdot<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.by32.p, S.br32.p, S.bp32.p, S.bst, S.bsh, S.bpartials.p,
+                                                    eps32, 2, ictl);
+  std::vector<cudaGraphNode_t> ol = capture_leaves(s);
+  end_into(s);
+  cudaGraph_t ibody;
+  cudaGraphNode_t inode = add_while(obody, ol, hi, &ibody);
+  begin_into(s, ibody, {});
+  enqueue_biteration<float, CPL>(s, S, S.br32.p, S.bs32.p, S.by32.p, S.bp32.p, S.bq32.p, S.bx3_32.p, eps32, ictl);
+  end_into(s);
+  begin_into(s, obody, {inode});
+  kb_outer_correct<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bx3_32.p, S.bxf.p, S.bst);
+  kb_true_residual<CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.bxf.p, S.bbm.p,
+                                                           S.br64.p, S.bst, S.bsh, S.bpartials.p);
+  kb_outer_decide<<<1, kMaxBatch, 0, s>>>(S.bst, S.bsh, kp, octl);
+  end_into(s);
+  begin_into(s, top, {onode});
+  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, S.bx_ext.p, (long long)n, S.bsh);
+  end_into(s);
+  cudaGraphExec_t exec;
+  ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
+  cudaGraphDestroy(top);
+  return exec;
+}
+
+template <typename T, int CPL>
+int batch_occupancy(int sms) {
+  int a = 0, b = 0;
+  ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kb_sweep<T, CPL, true>, kSweepThreads, 0));
+  ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kb_sweep<T, CPL, false>, kSweepThreads, 0));
+  return sms * std::max(1, std::min(a, b));
+}
+
+void ensure_batch(SolverImpl& S, int kp) {
+  if (!S.bst) {
+    ACG_CUDA(cudaMalloc(&S.bst, sizeof(PcgState) * kMaxBatch));
+    ACG_CUDA(cudaMalloc(&S.bsh, sizeof(BatchShared)));
+    ACG_CUDA(cudaMemset(S.bsh, 0, sizeof(BatchShared)));
+    ACG_CUDA(cudaMallocHost(&S.h_bst, sizeof(PcgState) * kMaxBatch));
+    S.bpartials.alloc((size_t)4 * kVecBlocks * kMaxBatch);
+    int sms = 0;
+    ACG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S.device));
+    S.bsweep_blocks[0][0] = batch_occupancy<double, 1>(sms);
+    S.bsweep_blocks[0][1] = batch_occupancy<double, 2>(sms);
+    S.bsweep_blocks[0][2] = batch_occupancy<double, 4>(sms);
+    S.bsweep_blocks[0][3] = batch_occupancy<double, 8>(sms);
+    S.bsweep_blocks[1][0] = batch_occupancy<float, 1>(sms);
+    S.bsweep_blocks[1][1] = batch_occupancy<float, 2>(sms);
+    S.bsweep_blocks[1][2] = batch_occupancy<float, 4>(sms);
+    S.bsweep_blocks[1][3] = batch_occupancy<float, 8>(sms);
+  }
+  if (kp <= S.batch_kp) return;
+  // growing the buffers invalidates every captured batch graph
+  for (auto& row : S.bexec)
+    for (auto& e : row)
+      if (e) {
+        cudaGraphExecDestroy(e);
+        e = nullptr;
+      }
+  const size_t N = (size_t)S.n * kp;
+  for (DevBuf<double>* b : {&S.bb_ext, &S.bx_ext, &S.bbm, &S.br64, &S.bxf, &S.bs64, &S.by64, &S.bp64, &S.bq64})
+    b->alloc(N);
+  S.bx3_64.alloc(3 * N);
+  for (DevBuf<float>* b : {&S.br32, &S.bs32, &S.by32, &S.bp32, &S.bq32}) b->alloc(N);
+  S.bx3_32.alloc(3 * N);
+  S.batch_kp = kp;
+}
+
+// Solve k <= 64 right-hand sides (column-major, leading dimensions ldb/ldx)
+// in one batched graph launch.
+int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t ldx, int k, cudaMemcpyKind kin,
+                cudaMemcpyKind kout, double tol, int64_t maxits, double maxtime, int stag_test, int precision,
+                acg_solve_info* info) {
+  cudaStream_t s = S.stream;
+  const int kp = round_kp(k);
+  ensure_batch(S, std::max(kp, S.batch_kp));
+  cudaGraphExec_t& ge = S.bexec[precision][kp_index(kp)];
+  if (!ge) {
+    with_cpl(kp, [&](auto cpl) {
+      constexpr int C = decltype(cpl)::value;
+      ge = precision == 0 ? build_batch_fp64_graph<C>(S) : build_batch_mixed_graph<C>(S);
+    });
+  }
+  PcgState* h = S.h_bst;
+  std::memset(h, 0, sizeof(PcgState) * kMaxBatch);
+  for (int c = 0; c < kp; ++c) {
+    h[c].tol = tol;
+    h[c].maxtime_s = maxtime;
+    h[c].maxits = maxits;
+    h[c].stag_test = stag_test;
+    h[c].tol_user = tol;
+    h[c].maxits_user = maxits;
+    h[c].min_inner_tol = 1e-5;
+    h[c].max_outer = 40;
+    h[c].inner_tol = std::min(0.25, std::max(h[c].min_inner_tol, 0.5 * tol));
+  }
+  BatchShared hb = {};
+  hb.k = k;
+  ACG_CUDA(cudaMemcpyAsync(S.bst, h, sizeof(PcgState) * kp, cudaMemcpyHostToDevice, s));
+  ACG_CUDA(cudaMemcpyAsync(S.bsh, &hb, sizeof(BatchShared), cudaMemcpyHostToDevice, s));
+  ACG_CUDA(cudaMemcpy2DAsync(S.bb_ext.p, sizeof(double) * S.n, B, sizeof(double) * ldb, sizeof(double) * S.n, k, kin,
+                             s));
+  cudaEvent_t e0, e1;
+  ACG_CUDA(cudaEventCreate(&e0));
+  ACG_CUDA(cudaEventCreate(&e1));
+  ACG_CUDA(cudaEventRecord(e0, s));
+  ACG_CUDA(cudaGraphLaunch(ge, s));
+  ACG_CUDA(cudaEventRecord(e1, s));
+  ACG_CUDA(cudaMemcpy2DAsync(X, sizeof(double) * ldx, S.bx_ext.p, sizeof(double) * S.n, sizeof(double) * S.n, k, kout,
+                             s));
+  ACG_CUDA(cudaMemcpyAsync(h, S.bst, sizeof(PcgState) * kp, cudaMemcpyDeviceToHost, s));
+  ACG_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int worst = 0;
+  for (int c = 0; c < k; ++c) {
+    if (info) {
+      info[c].iterations = precision == 0 ? h[c].itcnt : h[c].total_its;
+      info[c].refinements = precision == 0 ? 0 : h[c].outer_its;
+      info[c].relres = h[c].nr;
+      info[c].best_relres = precision == 0 ? h[c].bestnr : h[c].nr_true;
+      info[c].true_relres = h[c].nr_true;
+      info[c].solve_ms = ms;
+      info[c].status = h[c].status;
+      info[c].levels = S.nlev;
+    }
+    const int rc = status_to_rc(h[c].status);
+    if (rc < 0) return rc;
+    worst = std::max(worst, rc);
+  }
+  return worst;
+}
+
 int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, cudaMemcpyKind kout, double tol,
                  int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info) {
   cudaStream_t s = S.stream;
@@ -939,6 +1214,73 @@ int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, 
     info->levels = S.nlev;
   }
   return status_to_rc(h.status);
+}
+
+// Device time per call of the batched kernels for kp columns (see time_kernels_t).
+template <typename T, int CPL>
+void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T* y, T* p, T* q) {
+  constexpr int kp = CPL * kBatchLanes;
+  cudaStream_t s = S.stream;
+  ACG_CUDA(cudaMemsetAsync(S.bsh, 0, sizeof(BatchShared), s));
+  ACG_CUDA(cudaMemsetAsync(r, 0, sizeof(T) * (size_t)S.n * kp, s));
+  ACG_CUDA(cudaMemsetAsync(p, 0, sizeof(T) * (size_t)S.n * kp, s));
+  ACG_CUDA(cudaStreamSynchronize(s));
+  const TypedArrays<T> A = arrays_of<T>(S);
+  const size_t N = (size_t)S.n * kp;
+  auto time_graph = [&](auto&& body) -> double {
+    cudaGraph_t g;
+    ACG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < reps; ++i) body();
+    ACG_CUDA(cudaStreamEndCapture(s, &g));
+    cudaGraphExec_t ge;
+    ACG_CUDA(cudaGraphInstantiate(&ge, g, 0));
+    ACG_CUDA(cudaGraphLaunch(ge, s));
+    cudaEvent_t e0, e1;
+    ACG_CUDA(cudaEventCreate(&e0));
+    ACG_CUDA(cudaEventCreate(&e1));
+    ACG_CUDA(cudaEventRecord(e0, s));
+    ACG_CUDA(cudaGraphLaunch(ge, s));
+    ACG_CUDA(cudaEventRecord(e1, s));
+    ACG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    ACG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    return (double)ms / reps;
+  };
+  auto fill_s = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)N, sv, (T*)nullptr); };
+  auto fill_y = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)N, y, (T*)nullptr); };
+  const double t_fill = time_graph(fill_s);
+  out->spmv_ms = time_graph([&]() { kb_spmv<T, CPL><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, A.lp, A.li, A.lv, p, q, S.bsh); });
+  out->forward_ms = time_graph([&]() {
+    fill_s();
+    enqueue_bsweep<T, CPL, true>(s, S, r, (const T*)nullptr, sv);
+  }) - t_fill;
+  out->backward_ms = time_graph([&]() {
+    fill_y();
+    enqueue_bsweep<T, CPL, false>(s, S, A.g, sv, y);
+  }) - t_fill;
+  out->iteration_ms = 0.0;
+  out->launches_per_iteration = 9;
+  out->forward_launches = 1;
+  const double vb = sizeof(T), nv = S.n, F = (double)S.nnz_f;
+  out->spmv_bytes = 4.0 * (nv + 1) + (double)S.nnz_l * (4.0 + vb) + 2.0 * nv * kp * vb;
+  out->forward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_f + 3.0 * nv * kp * vb;
+  out->backward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_b + nv * vb + 3.0 * nv * kp * vb;
+  BatchShared hb;
+  ACG_CUDA(cudaMemcpy(&hb, S.bsh, sizeof(BatchShared), cudaMemcpyDeviceToHost));
+  if (hb.sweep_error) throw CudaError("a batched sweep wait gave up while timing");
+}
+
+void time_batch(SolverImpl& S, int precision, int kp, int reps, acg_kernel_times* out) {
+  ensure_batch(S, std::max(kp, S.batch_kp));
+  with_cpl(kp, [&](auto cpl) {
+    constexpr int C = decltype(cpl)::value;
+    if (precision == 0) time_batch_t<double, C>(S, reps, out, S.br64.p, S.bs64.p, S.by64.p, S.bp64.p, S.bq64.p);
+    else time_batch_t<float, C>(S, reps, out, S.br32.p, S.bs32.p, S.by32.p, S.bp32.p, S.bq32.p);
+  });
 }
 
 }  // namespace
@@ -1067,10 +1409,14 @@ int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t l
   return guarded("acg_solve", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
     int worst = ACG_OK;
-    const int64_t ld = nrhs > 1 ? ldb : h->impl.n;
-    for (int64_t c = 0; c < nrhs; ++c) {
-      int rc = acg::solve_column(h->impl, b + c * ld, x + c * ld, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol,
-                                 maxits, maxtime, stag_test, precision, info ? info + c : nullptr);
+    if (nrhs == 1)
+      return acg::solve_column(h->impl, b, x, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol, maxits, maxtime,
+                               stag_test, precision, info);
+    for (int64_t c0 = 0; c0 < nrhs; c0 += acg::kMaxBatch) {
+      const int k = (int)std::min<int64_t>(acg::kMaxBatch, nrhs - c0);
+      int rc = acg::solve_batch(h->impl, b + c0 * ldb, ldb, x + c0 * ldb, ldb, k, cudaMemcpyHostToDevice,
+                                cudaMemcpyDeviceToHost, tol, maxits, maxtime, stag_test, precision,
+                                info ? info + c0 : nullptr);
       if (rc < 0) return rc;
       worst = std::max(worst, rc);
     }
@@ -1089,6 +1435,28 @@ int acg_solve_device(acg_solver* h, const double* b_dev, double* x_dev, double t
     ACG_CUDA(cudaDeviceSynchronize());
     return acg::solve_column(h->impl, b_dev, x_dev, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice, tol, maxits,
                              maxtime, stag_test, precision, info);
+  });
+}
+
+int acg_solve_batch_device(acg_solver* h, const double* b_dev, double* x_dev, int64_t nrhs, int64_t ld, double tol,
+                           int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info) {
+  if (!h || !b_dev || !x_dev || nrhs < 1 || ld < h->impl.n || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_solve_batch_device: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_solve_batch_device", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    ACG_CUDA(cudaDeviceSynchronize());
+    int worst = ACG_OK;
+    for (int64_t c0 = 0; c0 < nrhs; c0 += acg::kMaxBatch) {
+      const int k = (int)std::min<int64_t>(acg::kMaxBatch, nrhs - c0);
+      int rc = acg::solve_batch(h->impl, b_dev + c0 * ld, ld, x_dev + c0 * ld, ld, k, cudaMemcpyDeviceToDevice,
+                                cudaMemcpyDeviceToDevice, tol, maxits, maxtime, stag_test, precision,
+                                info ? info + c0 : nullptr);
+      if (rc < 0) return rc;
+      worst = std::max(worst, rc);
+    }
+    return worst;
   });
 }
 
@@ -1164,6 +1532,18 @@ int acg_ldlsolve_noalloc(acg_solver* h, const double* r_dev, double* y_dev, int 
         return ACG_ERR_TIMEOUT;
       }
     }
+    return ACG_OK;
+  });
+}
+
+int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg_kernel_times* out) {
+  if (!h || !out || reps < 1 || nrhs < 1 || nrhs > acg::kMaxBatch || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_time_kernels_batch: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_time_kernels_batch", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    acg::time_batch(h->impl, precision, acg::round_kp(nrhs), reps, out);
     return ACG_OK;
   });
 }
