@@ -100,6 +100,8 @@ typedef struct {
   int64_t wide_levels; /* levels swept with one grid launch each (FP32 plan) */
   int64_t thin_runs;   /* runs of thin levels swept by one CTA (FP32 plan) */
   int sweep_lanes, spmv_lanes;
+  int64_t device_bytes;   /* device memory held by this solver now           */
+  int64_t batch_capacity; /* right-hand sides its batch buffers hold (0 = none) */
 } acg_stats;
 
 /* Outcome of one solve (one right-hand side). */

@@ -1396,6 +1396,18 @@ int acg_solver_stats(const acg_solver* h, acg_stats* out) {
   out->wide_levels = wide;
   out->thin_runs = thin;
   out->sweep_lanes = acg::kLightLanes;
+  size_t bytes = 0;
+  auto add = [&](const auto& b) { bytes += b.n * sizeof(*b.p); };
+  add(S.perm); add(S.lvl_off_d); add(S.l_ptr); add(S.l_idx); add(S.f_ptr); add(S.f_idx); add(S.b_ptr); add(S.b_idx);
+  add(S.l_v64); add(S.f_c64); add(S.b_c64); add(S.g64); add(S.l_v32); add(S.f_c32); add(S.b_c32); add(S.g32);
+  add(S.b_ext); add(S.x_ext); add(S.bm); add(S.r64); add(S.s64); add(S.y64); add(S.p64); add(S.q64); add(S.x3_64);
+  add(S.xf); add(S.r32); add(S.s32); add(S.y32); add(S.p32); add(S.q32); add(S.x3_32); add(S.partials);
+  add(S.tasks_f); add(S.tasks_b);
+  add(S.bb_ext); add(S.bx_ext); add(S.bbm); add(S.br64); add(S.bxf); add(S.bpartials); add(S.br32); add(S.bs32);
+  add(S.by32); add(S.bp32); add(S.bq32); add(S.bx3_32); add(S.bs64); add(S.by64); add(S.bp64); add(S.bq64);
+  add(S.bx3_64);
+  out->device_bytes = (int64_t)bytes;
+  out->batch_capacity = S.batch_kp;
   out->spmv_lanes = S.vl_spmv;
   return ACG_OK;
 }

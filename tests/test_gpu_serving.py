@@ -1,0 +1,119 @@
+"""Serving: requests on several graphs arrive while others are running, are
+merged per graph into batched launches and overlap on the device.  Each
+result must equal the same right-hand sides solved alone (FP64: x within
+1e-7 after removing the mean, iterations within 1; mixed: true relative
+residual <= tol); eviction under a tight HBM budget and rejection of a graph
+larger than the budget are checked too."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import acgpu
+from acgpu import generators as G
+from acgpu.serving import AdmissionError, SolveServer
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _graphs():
+    return {
+        "g2": G.grid2(40, weights="loguniform", seed=1),
+        "g3": G.grid3(14, weights="loguniform", seed=2),
+        "pm": G.path_plus_matchings(3000, sigma=1.0, seed=3),
+    }
+
+
+def _rel(x, y):
+    return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+
+
+def _submit_stream(server, graphs, nreq, seed):
+    rng = np.random.default_rng(seed)
+    names = sorted(graphs)
+    futs = []
+
+    def producer(tid):
+        r = np.random.default_rng(seed + 100 + tid)
+        for _ in range(nreq // 2):
+            gid = names[r.integers(len(names))]
+            n = graphs[gid].shape[0]
+            k = int(r.integers(1, 6))
+            B = r.standard_normal((n, k))
+            futs.append((gid, B, server.submit(gid, B, tol=1e-9)))
+            time.sleep(float(r.exponential(0.002)))
+
+    ths = [threading.Thread(target=producer, args=(t,)) for t in range(2)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    return futs
+
+
+def test_results_same_alone_and_in_the_mix(gpu_ok):
+    graphs = _graphs()
+    factors = {}
+    for i, (gid, a) in enumerate(sorted(graphs.items())):
+        acgpu.seed(10 + i)
+        factors[gid] = acgpu.approx_chol(a)
+    server = SolveServer(hbm_budget=8 << 30, slots=3, precision="fp64")
+    for gid, a in graphs.items():
+        server.register(gid, a, ldli=factors[gid])
+    with server:
+        futs = _submit_stream(server, graphs, 24, seed=5)
+        results = [(gid, B, f.result(timeout=300)) for gid, B, f in futs]
+    stats = server.latency_stats()
+    assert stats["requests"] == len(futs) and stats["launches"] <= len(futs)
+    alone = {gid: acgpu.DeviceLapSolver(graphs[gid], factors[gid]) for gid in graphs}
+    for gid, B, (X, infos) in results:
+        for c in range(B.shape[1]):
+            its = [0]
+            x1 = alone[gid](B[:, c], tol=1e-9, maxits=2000, pcgIts=its)
+            assert abs(infos[c].iterations - its[0]) <= 1
+            assert _rel(O.center(X[:, c]), O.center(x1)) < 1e-7
+            assert O.relres(graphs[gid], X[:, c], B[:, c] - B[:, c].mean()) < 1e-8
+    for s in alone.values():
+        s.close()
+
+
+def test_mixed_precision_serving_meets_tol(gpu_ok):
+    graphs = _graphs()
+    server = SolveServer(hbm_budget=8 << 30, slots=2, precision="mixed")
+    for i, (gid, a) in enumerate(sorted(graphs.items())):
+        server.register(gid, a, seed=20 + i)
+    with server:
+        futs = _submit_stream(server, graphs, 12, seed=9)
+        for gid, B, f in futs:
+            X, infos = f.result(timeout=300)
+            for c in range(B.shape[1]):
+                assert infos[c].status == 0
+                assert O.relres(graphs[gid], X[:, c], B[:, c] - B[:, c].mean()) <= 1e-9 * 1.01
+
+
+def test_admission_by_hbm_budget(gpu_ok):
+    graphs = _graphs()
+    one = max(SolveServer(0)._estimate_bytes(_entry(a)) for a in graphs.values())
+    server = SolveServer(hbm_budget=one + 1, slots=2, precision="fp64")
+    for i, (gid, a) in enumerate(sorted(graphs.items())):
+        server.register(gid, a, seed=30 + i)
+    with server:
+        futs = [(gid, server.submit(gid, np.random.default_rng(j).standard_normal(graphs[gid].shape[0])))
+                for j, gid in enumerate(["g2", "g3", "pm", "g2", "pm", "g3"])]
+        for gid, f in futs:
+            X, infos = f.result(timeout=300)
+            assert infos[0].status == 0
+    assert server._resident <= one + 1
+    tiny = SolveServer(hbm_budget=1024, slots=1)
+    tiny.register("g2", graphs["g2"], seed=1)
+    with tiny:
+        with pytest.raises(AdmissionError):
+            tiny.submit("g2", np.ones(graphs["g2"].shape[0])).result(timeout=60)
+
+
+def _entry(a):
+    from acgpu.serving import _GraphEntry
+    acgpu.seed(1)
+    return _GraphEntry("x", a, acgpu.approx_chol(a))
