@@ -327,6 +327,180 @@ def run_acgpu(args):
         dist.destroy_process_group()
 
 
+# ---- the other workloads of the solve phase (reported, not the headline) -------
+
+def _device_solve(dev, b, prec, tol, maxits=MAXITS):
+    x = dev(b, tol=tol, maxits=maxits, precision=prec)
+    return x, dev.last_info[0]
+
+
+def run_config1(args):
+    """grid2(200), unit weights, one zero-mean Gaussian RHS, tol 1e-6: FP64 on the
+    GPU against the CPU restatement on the same LDLinv."""
+    import acgpu
+    import oracle as O
+    from acgpu import generators as G
+    a = G.grid2(200)
+    acgpu.seed(FACTOR_SEED)
+    ldli = acgpu.approx_chol(a)
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    b = rhs(a.shape[0], 11)
+    for _ in range(3):
+        x, info = _device_solve(dev, b, "fp64", 1e-6)
+    orc = O.OracleSolver(a, ldli)
+    t = time.perf_counter()
+    xo, ito, rco, _ = orc(b, tol=1e-6, maxits=1000)
+    t_cpu = time.perf_counter() - t
+    diff = float(np.linalg.norm(O.center(x) - O.center(xo)) / np.linalg.norm(O.center(xo)))
+    print(json.dumps({"workload": "config1 grid2(200) unit weights, tol 1e-6, fp64", "n": a.shape[0],
+                      "gpu_ms": info.solve_ms, "gpu_its": info.iterations, "gpu_relres": O.relres(a, x, b),
+                      "cpu_port_ms": t_cpu * 1e3, "cpu_its": ito, "cpu_relres": O.relres(a, xo, b),
+                      "x_rel_diff_vs_cpu": diff, "levels": dev.stats()["levels"]}), flush=True)
+    dev.close()
+
+
+def run_config3(args):
+    """Path over a random permutation + 4 random perfect matchings, n = 2M,
+    lognormal(0, 2) weights; mixed precision to 1e-8; level count and LDLinv GB/s."""
+    import acgpu
+    from acgpu import generators as G
+    n = 2_000_000 if GRID_SIDE == 100 else GRID_SIDE ** 3
+    a = G.path_plus_matchings(n, k=4, sigma=2.0, seed=3)
+    acgpu.seed(FACTOR_SEED)
+    t = time.perf_counter()
+    ldli = acgpu.approx_chol(a)
+    factor_s = time.perf_counter() - t
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    b = rhs(n, 12)
+    out = {"workload": "config3 path+4 matchings n=2M lognormal(0,2)", "n": n, "avg_degree": a.nnz / n,
+           "factor_nnz": ldli.nnz, "factor_s": factor_s, "levels": dev.stats()["levels"]}
+    for prec in ("mixed", "fp64"):
+        for _ in range(2):
+            x, info = _device_solve(dev, b, prec, TOL)
+        kt = dev.time_kernels(prec, reps=3)
+        out[prec] = {"solve_ms": info.solve_ms, "its": info.iterations, "refinements": info.refinements,
+                     "true_relres": info.true_relres, "status": info.status,
+                     "forward_ms": kt["forward_ms"], "backward_ms": kt["backward_ms"],
+                     "ldlinv_forward_gbs": kt["forward_bytes"] / (kt["forward_ms"] * 1e-3) / 1e9,
+                     "ldlinv_backward_gbs": kt["backward_bytes"] / (kt["backward_ms"] * 1e-3) / 1e9}
+    print(json.dumps(out), flush=True)
+    dev.close()
+
+
+def run_config4a(args):
+    """64 right-hand sides on the 1M weighted 3D grid: FP64 batched vs mixed batched."""
+    import torch
+    import acgpu
+    from acgpu._lib import AcgSolveInfo, check, lib
+    a, ldli, factor_s = build_workload()
+    n = a.shape[0]
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    k = 64
+    B = torch.empty((k, n), dtype=torch.float64, device="cuda")
+    for c in range(k):
+        B[c] = torch.from_numpy(rhs(n, 77 + c))
+    X = torch.empty_like(B)
+    infos = (AcgSolveInfo * k)()
+    out = {"workload": "config4a 64 RHS on grid3(100) log-uniform weights, tol 1e-8", "n": n}
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        times = []
+        for rep in range(3):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            check(lib().acg_solve_batch_device(dev._h, ctypes.c_void_p(B.data_ptr()), ctypes.c_void_p(X.data_ptr()),
+                                               k, n, TOL, MAXITS, float("inf"), 5, prec, infos))
+            times.append(time.perf_counter() - t)
+        its = [infos[c].iterations for c in range(k)]
+        out[name] = {"solves_per_s": k / min(times), "batch_ms": 1e3 * min(times), "its_mean": float(np.mean(its)),
+                     "true_relres_max": max(infos[c].true_relres for c in range(k))}
+        kt = dev.time_kernels_batch(k, name, reps=3)
+        out[name]["forward_ms"] = kt["forward_ms"]
+        out[name]["ldlinv_forward_gbs"] = kt["forward_bytes"] / (kt["forward_ms"] * 1e-3) / 1e9
+    out["mixed_over_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+    print(json.dumps(out), flush=True)
+    dev.close()
+
+
+def serving_graph_pool(count, seed):
+    """Graphs for the serving stream: 2D/3D grids, path + random matchings and
+    random geometric graphs (largest component), n log-uniform in [1e3, 1e6],
+    lognormal(0, 1) weights."""
+    from acgpu import generators as G
+    rng = np.random.default_rng(seed)
+    fams = ["grid2", "grid3", "matchings", "rgg"]
+    pool = []
+    for i in range(count):
+        fam = fams[i % 4]
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+        s = int(rng.integers(1 << 30))
+        if fam == "grid2":
+            side = max(2, int(round(np.sqrt(n))))
+            a = G.grid2(side, weights="lognormal:1", seed=s)
+        elif fam == "grid3":
+            side = max(2, int(round(n ** (1 / 3))))
+            a = G.grid3(side, weights="lognormal:1", seed=s)
+        elif fam == "matchings":
+            a = G.path_plus_matchings(max(4, n - n % 2), k=4, sigma=1.0, seed=s)
+        else:
+            a = G.largest_component(G.random_geometric(n, seed=s, weights="lognormal:1"))
+        pool.append((f"{fam}-{a.shape[0]}", a))
+    return pool
+
+
+def run_serving(args):
+    """Poisson stream of solve requests over a pool of cached graphs, 1-16
+    right-hand sides each, tol 1e-8: continuous batching (mixed precision)
+    against the unbatched FP64 GPU path (one request at a time, one RHS per solve)."""
+    import acgpu
+    from acgpu.serving import SolveServer
+    pool = serving_graph_pool(args.serving_graphs, seed=2024)
+    factors = {}
+    t = time.perf_counter()
+    for i, (gid, a) in enumerate(pool):
+        acgpu.seed(1000 + i)
+        factors[gid] = acgpu.approx_chol(a)
+    factor_s = time.perf_counter() - t
+    rng = np.random.default_rng(7)
+    nreq = args.serving_requests
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serving_rate, nreq))
+    picks = rng.integers(len(pool), size=nreq)
+    ks = rng.integers(1, 17, size=nreq)
+    rhs_blocks = [np.random.default_rng(10_000 + r).standard_normal((pool[picks[r]][1].shape[0], int(ks[r])))
+                  for r in range(nreq)]
+    results = {}
+    for label, kw in (("batched_mixed", dict(precision="mixed", slots=4)),
+                      ("unbatched_fp64", dict(precision="fp64", slots=1, unbatched=True))):
+        server = SolveServer(hbm_budget=int(args.serving_hbm_gb * (1 << 30)), **kw)
+        for gid, a in pool:
+            server.register(gid, a, ldli=factors[gid])
+        with server:
+            for gid, a in pool:  # warm: upload and capture every graph once
+                server.submit(gid, np.random.default_rng(1).standard_normal(a.shape[0]), tol=TOL).result()
+            server.completed.clear()
+            server.launches = 0
+            futs = []
+            t0 = time.perf_counter()
+            for r in range(nreq):
+                delay = t0 + arrivals[r] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                futs.append(server.submit(pool[picks[r]][0], rhs_blocks[r], tol=TOL))
+            worst = 0.0
+            for f in futs:
+                X, infos = f.result()
+                worst = max(worst, max(i.true_relres for i in infos))
+            st = server.latency_stats()
+            st["true_relres_max"] = worst
+            results[label] = st
+    out = {"workload": "config5 serving: Poisson arrivals, graphs from 2D/3D grids, matchings, RGG, "
+                       "n log-uniform [1e3,1e6], lognormal(0,1) weights, 1-16 RHS, tol 1e-8",
+           "graphs": [(gid, int(a.shape[0])) for gid, a in pool], "requests": nreq,
+           "arrival_rate_per_s": args.serving_rate, "factor_s_total": factor_s, **results,
+           "speedup_solves_per_s": results["batched_mixed"]["solves_per_s"] / results["unbatched_fp64"]["solves_per_s"]}
+    print(json.dumps(out), flush=True)
+
+
+
 def run_reference(args):
     """The reference's solve on the host cores: the CPU restatement of pcg +
     LDLsolver (oracle port), one independent solve per thread."""
@@ -389,14 +563,26 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--side", type=int, default=GRID_SIDE, help="grid side (100 = the benchmark workload)")
     ap.add_argument("--rhs", type=int, default=64, help="independent right-hand sides per step (batched)")
+    ap.add_argument("--workload", default="grid3",
+                    choices=["grid3", "config1", "config3", "config4a", "serving"],
+                    help="grid3 = the headline line; the others report the remaining configurations")
+    ap.add_argument("--serving-graphs", type=int, default=16)
+    ap.add_argument("--serving-requests", type=int, default=300)
+    ap.add_argument("--serving-rate", type=float, default=40.0, help="requests per second")
+    ap.add_argument("--serving-hbm-gb", type=float, default=120.0)
     args = ap.parse_args()
     globals()["GRID_SIDE"] = args.side
     if args.warmup < 3 and args.impl == "acgpu":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
-    else:
+    elif args.workload == "grid3":
         run_acgpu(args)
+    else:
+        import torch
+        torch.cuda.init()
+        {"config1": run_config1, "config3": run_config3, "config4a": run_config4a,
+         "serving": run_serving}[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -19,7 +19,7 @@ import scipy.sparse as sp
 __all__ = [
     "from_edges", "path_graph", "grid2", "grid3", "rand_matching_edges",
     "path_plus_matchings", "random_geometric", "cycle_graph", "star_graph",
-    "complete_graph", "random_tree", "loguniform_weights",
+    "complete_graph", "random_tree", "loguniform_weights", "lognormal_weights", "largest_component",
 ]
 
 
@@ -55,6 +55,21 @@ def _grid_edges(dims):
     return n, np.concatenate(ii), np.concatenate(jj)
 
 
+def lognormal_weights(m: int, sigma: float, seed: int) -> np.ndarray:
+    return np.random.default_rng(seed).lognormal(0.0, sigma, size=m)
+
+
+def _weights(kind: str, m: int, seed: int):
+    if kind == "unit":
+        return None
+    if kind == "loguniform":
+        return loguniform_weights(m, 1e-3, 1.0, seed)
+    if kind.startswith("lognormal"):
+        sigma = float(kind.split(":")[1]) if ":" in kind else 1.0
+        return lognormal_weights(m, sigma, seed)
+    raise ValueError(f"unknown weights {kind!r}")
+
+
 def loguniform_weights(m: int, lo: float, hi: float, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     return np.exp(rng.uniform(np.log(lo), np.log(hi), size=m))
@@ -87,21 +102,21 @@ def random_tree(n: int, seed: int, weighted: bool = True) -> sp.csc_matrix:
 
 
 def grid2(n: int, m: int | None = None, weights: str = "unit", seed: int = 0) -> sp.csc_matrix:
-    """n-by-m grid (4-neighbour). ``weights``: "unit" or "loguniform" in [1e-3, 1]."""
+    """n-by-m grid (4-neighbour). ``weights``: "unit", "loguniform" in [1e-3, 1],
+    or "lognormal[:sigma]"."""
     m = n if m is None else m
     nv, i, j = _grid_edges((n, m))
-    w = None if weights == "unit" else loguniform_weights(i.shape[0], 1e-3, 1.0, seed)
-    return from_edges(nv, i, j, w)
+    return from_edges(nv, i, j, _weights(weights, i.shape[0], seed))
 
 
 def grid3(n1: int, n2: int | None = None, n3: int | None = None, weights: str = "unit",
           seed: int = 0) -> sp.csc_matrix:
-    """n1-by-n2-by-n3 grid (6-neighbour). ``weights``: "unit" or "loguniform" in [1e-3, 1]."""
+    """n1-by-n2-by-n3 grid (6-neighbour). ``weights``: "unit", "loguniform" in
+    [1e-3, 1], or "lognormal[:sigma]"."""
     n2 = n1 if n2 is None else n2
     n3 = n1 if n3 is None else n3
     nv, i, j = _grid_edges((n1, n2, n3))
-    w = None if weights == "unit" else loguniform_weights(i.shape[0], 1e-3, 1.0, seed)
-    return from_edges(nv, i, j, w)
+    return from_edges(nv, i, j, _weights(weights, i.shape[0], seed))
 
 
 def rand_matching_edges(n: int, rng: np.random.Generator):
@@ -127,15 +142,28 @@ def path_plus_matchings(n: int, k: int = 4, sigma: float = 2.0, seed: int = 0) -
     return from_edges(n, i, j, w)
 
 
-def random_geometric(n: int, mean_degree: float = 8.0, seed: int = 0) -> sp.csc_matrix:
+def largest_component(a) -> sp.csc_matrix:
+    from scipy.sparse.csgraph import connected_components
+    _, lab = connected_components(a, directed=False)
+    big = np.argmax(np.bincount(lab))
+    ind = np.where(lab == big)[0]
+    sub = sp.csc_matrix(a[ind][:, ind])
+    sub.sort_indices()
+    return sub
+
+
+def random_geometric(n: int, mean_degree: float = 8.0, seed: int = 0, weights: str = "inverse_distance") -> sp.csc_matrix:
     """Points uniform in the unit square joined within radius sqrt(d/(pi n));
-    weights 1/distance.  May be disconnected."""
+    weights 1/distance (or "lognormal[:sigma]").  May be disconnected."""
     from scipy.spatial import cKDTree
     rng = np.random.default_rng(seed)
     pts = rng.random((n, 2))
     r = np.sqrt(mean_degree / (np.pi * n))
     pairs = cKDTree(pts).query_pairs(r, output_type="ndarray")
     i, j = pairs[:, 0].astype(np.int64), pairs[:, 1].astype(np.int64)
-    dist = np.linalg.norm(pts[i] - pts[j], axis=1)
-    w = 1.0 / np.maximum(dist, 1e-12)
+    if weights == "inverse_distance":
+        dist = np.linalg.norm(pts[i] - pts[j], axis=1)
+        w = 1.0 / np.maximum(dist, 1e-12)
+    else:
+        w = _weights(weights, i.shape[0], seed + 1)
     return from_edges(n, i, j, w)

@@ -68,7 +68,8 @@ class SolveServer:
     """
 
     def __init__(self, hbm_budget: int, slots: int = 4, precision: str = "mixed", max_batch: int = 64,
-                 maxits: int = 2000):
+                 maxits: int = 2000, unbatched: bool = False):
+        self.unbatched = bool(unbatched)  # baseline: one request per launch, one right-hand side per solve
         self.hbm_budget = int(hbm_budget)
         self.slots = int(slots)
         self.precision = precision
@@ -195,6 +196,8 @@ class SolveServer:
                 r = best.queue.popleft()
                 reqs.append(r)
                 cols += r.B.shape[1]
+                if self.unbatched:
+                    break
             best.busy = True
             return best, reqs
         return None, None
@@ -222,8 +225,15 @@ class SolveServer:
         B = np.concatenate([r.B for r in reqs], axis=1)
         tol = min(r.tol for r in reqs)
         try:
-            X = e.solver(B, tol=tol, maxits=self.maxits, precision=self.precision)
-            infos = list(e.solver.last_info)
+            if self.unbatched:
+                cols, infos = [], []
+                for c in range(B.shape[1]):
+                    cols.append(e.solver(B[:, c], tol=tol, maxits=self.maxits, precision=self.precision))
+                    infos += list(e.solver.last_info)
+                X = np.stack(cols, axis=1)
+            else:
+                X = e.solver(B, tol=tol, maxits=self.maxits, precision=self.precision)
+                infos = list(e.solver.last_info)
         except Exception as exc:  # noqa: BLE001 - forwarded to every waiting caller
             for r in reqs:
                 r.future.set_exception(exc)
