@@ -88,7 +88,9 @@ typedef struct {
                           narrower levels whose values fit in shared memory run in
                           one CTA with block barriers (default 2048)              */
   int reserved[5];     /* [0]: resident sweep blocks per SM (0 = 1); [1]: poll mode + 1
-                          (1 tight+sleep, 2 tight only, 3 backoff); others 0      */
+                          (1 tight+sleep, 2 tight only, 3 backoff); [2]: 2 = sweep
+                          the final narrow levels in one CTA (experimental);
+                          others 0                                                */
 } acg_options;
 
 /* Shape of an uploaded solver. */
@@ -102,6 +104,8 @@ typedef struct {
   int sweep_lanes, spmv_lanes;
   int64_t device_bytes;   /* device memory held by this solver now           */
   int64_t batch_capacity; /* right-hand sides its batch buffers hold (0 = none) */
+  int64_t tail_levels;    /* final levels swept by one CTA from shared memory    */
+  int64_t tail_vertices;  /* vertices of those levels                           */
 } acg_stats;
 
 /* Outcome of one solve (one right-hand side). */

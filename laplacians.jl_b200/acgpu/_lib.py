@@ -36,7 +36,8 @@ class AcgStats(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("nnz_lap", ctypes.c_int64), ("nnz_factor", ctypes.c_int64),
                 ("levels", ctypes.c_int64), ("wide_levels", ctypes.c_int64), ("thin_runs", ctypes.c_int64),
                 ("sweep_lanes", ctypes.c_int), ("spmv_lanes", ctypes.c_int), ("device_bytes", ctypes.c_int64),
-                ("batch_capacity", ctypes.c_int64)]
+                ("batch_capacity", ctypes.c_int64), ("tail_levels", ctypes.c_int64),
+                ("tail_vertices", ctypes.c_int64)]
 
 
 class AcgSolveInfo(ctypes.Structure):

@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <climits>
+
 namespace acg {
 
 constexpr int kMaxPartialBlocks = 2048;
@@ -509,6 +511,86 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const Sweep
     e0 = e1;
     r1 = r2;
   }
+}
+
+// ---- the narrow tail of the DAG in one CTA -----------------------------------
+//
+// The last NL levels (vertices [V0, V0+NV)) have at most 32 tasks each.  One
+// 1024-thread CTA walks them level by level (forward: upwards, backward:
+// downwards) with a block barrier between levels; the tail's values live in
+// shared memory (and are written through to global memory), so a level costs
+// a shared-memory gather and a barrier instead of a cross-SM hop.  Warp w runs
+// task w of each level.  Task records are loaded two levels ahead and
+// entries one level ahead.  lvl_tasks[i] = {first task, task count} of tail
+// level i in the sweep's task table.
+constexpr int kTailThreads = 1024;
+constexpr int kTailWarps = kTailThreads / 32;
+
+template <typename T, bool kForward>
+__global__ void __launch_bounds__(kTailThreads, 1) k_tail(int NL, int V0, int NV, const int2* __restrict__ lvl_tasks,
+                                                         int ntasks, const SweepTask* __restrict__ tasks,
+                                                         const int* __restrict__ idx, const T* __restrict__ coef,
+                                                         const T* __restrict__ aux, const T* __restrict__ sfwd,
+                                                         T* out, const PcgState* st) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sv = reinterpret_cast<T*>(smem_raw);
+  int2* lt = reinterpret_cast<int2*>(sv + NV + (NV & 1));
+  if (st && st->done) return;
+  for (int i = threadIdx.x; i < NL; i += blockDim.x) lt[i] = lvl_tasks[i];
+  if (!kForward)
+    for (int i = threadIdx.x; i < NV; i += blockDim.x) sv[i] = __ldg(&sfwd[V0 + i]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  auto task_of = [&](int step) -> int {
+    if (step >= NL) return INT_MAX;
+    const int2 r = lt[kForward ? step : NL - 1 - step];
+    return w < r.y ? r.x + w : INT_MAX;
+  };
+  SweepTask r1 = load_task(tasks, task_of(1), ntasks);
+  SweepEntries<T> e0;
+  {
+    const SweepTask r0 = load_task(tasks, task_of(0), ntasks);
+    load_entries<T, kForward>(e0, r0, lane, idx, coef, aux, sfwd);
+  }
+  for (int step = 0; step < NL; ++step) {
+    const SweepTask r2 = load_task(tasks, task_of(step + 2), ntasks);
+    SweepEntries<T> e1;
+    load_entries<T, kForward>(e1, r1, lane, idx, coef, aux, sfwd);
+    const int2 cur = lt[kForward ? step : NL - 1 - step];
+    // the first task of this warp came through the pipeline; further tasks of
+    // a level (more than 32 of them is excluded by the host) never occur
+    if (w < cur.y) {
+      const int gw = e0.gw;
+      T acc = T(0);
+      T xv[kEntryUnroll];
+#pragma unroll
+      for (int j = 0; j < kEntryUnroll; ++j) {
+        const int id = e0.id[j];
+        xv[j] = id < 0 ? T(0) : (id >= V0 ? sv[id - V0] : out[id]);
+      }
+#pragma unroll
+      for (int j = 0; j < kEntryUnroll; ++j) acc += e0.c[j] * xv[j];
+      for (int k = e0.k0 + kEntryUnroll * gw; k < e0.k1; k += gw) {
+        const int id = __ldg(&idx[k]);
+        acc += __ldg(&coef[k]) * (id >= V0 ? sv[id - V0] : out[id]);
+      }
+      acc = group_sum_w(acc, gw);
+      if (e0.active && (lane & (gw - 1)) == 0) {
+        const T res = kForward ? e0.a + acc : e0.a * e0.own + acc;
+        sv[e0.v - V0] = res;
+        out[e0.v] = res;
+      }
+    }
+    __syncthreads();
+    e0 = e1;
+    r1 = r2;
+  }
+}
+
+template <typename T>
+constexpr size_t tail_smem_bytes(int nv, int nl) {
+  return (size_t)(nv + (nv & 1)) * sizeof(T) + (size_t)nl * sizeof(int2);
 }
 
 template <typename T>

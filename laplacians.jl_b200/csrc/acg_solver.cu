@@ -74,6 +74,11 @@ struct SweepStep {
   size_t smem;  // thin runs: dynamic shared memory bytes
 };
 
+// Graph capture and device (de)allocation are serialised across threads: an
+// allocation or free on one thread while another thread captures a stream can
+// invalidate that capture.  Graph launches do not take this lock.
+std::recursive_mutex g_device_mu;
+
 struct SolverImpl {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -87,6 +92,11 @@ struct SolverImpl {
   std::vector<int> heavy;          // per level: vertices with forward in-degree > 32
   std::vector<SweepStep> plan[2];  // [0] FP64 values, [1] FP32 values
   int sweep_mode = 0;              // 0 sync-free cooperative sweep, 1 one launch per level
+  // narrow tail of the DAG run by one CTA (k_tail): levels [nlev - tail_nl, nlev)
+  int tail_nl = 0, tail_v0 = 0, tail_nv = 0;
+  int tail_tf0 = 0;                // forward: sync-free tasks [0, tail_tf0), the tail after
+  int tail_tb0 = 0;                // backward: the tail first, then sync-free tasks [tail_tb0, ntasks_b)
+  DevBuf<int2> tail_lvl_f, tail_lvl_b;
   int ntasks_f = 0, ntasks_b = 0;
   int sweep_blocks[2] = {0, 0};    // co-resident grid of k_sweep per value type
   int poll_mode = 0;
@@ -212,9 +222,11 @@ void enqueue_step(cudaStream_t s, const SolverImpl& S, const SweepStep& st_, con
   }
 }
 
-// One sync-free sweep as a cooperative launch (all blocks co-resident).
+// One sync-free sweep over tasks [t0, t1) as a cooperative launch (all blocks co-resident).
 template <typename T, bool kForward>
-void enqueue_syncfree(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sfwd, T* out, PcgState* st) {
+void enqueue_syncfree(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sfwd, T* out, PcgState* st,
+                      int t0, int t1) {
+  if (t1 <= t0) return;
   const TypedArrays<T> A = arrays_of<T>(S);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(S.sweep_blocks[plan_index<T>()]);
@@ -225,17 +237,31 @@ void enqueue_syncfree(cudaStream_t s, const SolverImpl& S, const T* aux, const T
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  const int ntasks = kForward ? S.ntasks_f : S.ntasks_b;
-  const SweepTask* tasks = kForward ? S.tasks_f.p : S.tasks_b.p;
-  ACG_CUDA(cudaLaunchKernelEx(&cfg, k_sweep<T, kForward>, ntasks, tasks, kForward ? A.fi : A.bi,
+  const SweepTask* tasks = (kForward ? S.tasks_f.p : S.tasks_b.p) + t0;
+  ACG_CUDA(cudaLaunchKernelEx(&cfg, k_sweep<T, kForward>, t1 - t0, tasks, kForward ? A.fi : A.bi,
                               kForward ? A.fc : A.bc, aux, sfwd, out, st, S.poll_mode));
+}
+
+// The narrow tail of the DAG in one CTA.
+template <typename T, bool kForward>
+void enqueue_tail(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sfwd, T* out, const PcgState* st) {
+  const TypedArrays<T> A = arrays_of<T>(S);
+  const size_t smem = tail_smem_bytes<T>(S.tail_nv, S.tail_nl);
+  k_tail<T, kForward><<<1, kTailThreads, smem, s>>>(
+      S.tail_nl, S.tail_v0, S.tail_nv, kForward ? S.tail_lvl_f.p : S.tail_lvl_b.p, kForward ? S.ntasks_f : S.ntasks_b,
+      kForward ? S.tasks_f.p : S.tasks_b.p, kForward ? A.fi : A.bi, kForward ? A.fc : A.bc, aux, sfwd, out, st);
 }
 
 // Forward sweep: s = forward values of r (s must be pending in sync-free mode).
 template <typename T>
 void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, PcgState* st) {
   if (S.sweep_mode == 0) {
-    enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st);
+    if (S.tail_nl > 0) {
+      enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.tail_tf0);
+      enqueue_tail<T, true>(s, S, r, (const T*)nullptr, sv, st);
+    } else {
+      enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.ntasks_f);
+    }
     return;
   }
   for (const SweepStep& step : S.plan[plan_index<T>()]) enqueue_step<T, true>(s, S, step, r, (const T*)nullptr, sv, st);
@@ -245,7 +271,12 @@ template <typename T>
 void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, PcgState* st) {
   const T* g = arrays_of<T>(S).g;
   if (S.sweep_mode == 0) {
-    enqueue_syncfree<T, false>(s, S, g, sv, y, st);
+    if (S.tail_nl > 0) {
+      enqueue_tail<T, false>(s, S, g, sv, y, st);
+      enqueue_syncfree<T, false>(s, S, g, sv, y, st, S.tail_tb0, S.ntasks_b);
+    } else {
+      enqueue_syncfree<T, false>(s, S, g, sv, y, st, 0, S.ntasks_b);
+    }
     return;
   }
   const auto& plan = S.plan[plan_index<T>()];
@@ -652,8 +683,50 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     std::vector<int> fdeg(n);
     for (int v = 0; v < n; ++v) fdeg[v] = fptr[v + 1] - fptr[v];
     std::vector<SweepTask> tf, tb;
-    for (int l = 0; l < nlev; ++l) emit_level(tf, S.lvl_off[l], S.lvl_off[l + 1], fdeg, fptr, 32);
-    for (int l = nlev - 1; l >= 0; --l) emit_level(tb, S.lvl_off[l], S.lvl_off[l + 1], outdeg, bptr, 32);
+    std::vector<int2> lf(nlev), lb(nlev);  // {first task, count} per level
+    for (int l = 0; l < nlev; ++l) {
+      const int t0 = (int)tf.size();
+      emit_level(tf, S.lvl_off[l], S.lvl_off[l + 1], fdeg, fptr, 32);
+      lf[l] = make_int2(t0, (int)tf.size() - t0);
+    }
+    for (int l = nlev - 1; l >= 0; --l) {
+      const int t0 = (int)tb.size();
+      emit_level(tb, S.lvl_off[l], S.lvl_off[l + 1], outdeg, bptr, 32);
+      lb[l] = make_int2(t0, (int)tb.size() - t0);
+    }
+    // the tail: the longest run of final levels with at most 32 tasks in both
+    // tables whose values fit in shared memory (FP64 sizes, so both precisions fit)
+    {
+      int optin = 0;
+      ACG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, S.device));
+      const size_t cap = optin > 8192 ? (size_t)optin - 4096 : 0;
+      int lt = nlev, nv = 0;
+      while (lt > 0) {
+        const int l = lt - 1;
+        const int w = S.lvl_off[l + 1] - S.lvl_off[l];
+        if (lf[l].y > kTailWarps || lb[l].y > kTailWarps) break;
+        if (tail_smem_bytes<double>(nv + w, nlev - l) > cap) break;
+        nv += w;
+        lt = l;
+      }
+      if (nlev - lt >= 8 && opts && opts->reserved[2] == 2) {
+        S.tail_nl = nlev - lt;
+        S.tail_v0 = S.lvl_off[lt];
+        S.tail_nv = n - S.tail_v0;
+        S.tail_tf0 = lf[lt].x;
+        S.tail_tb0 = lb[lt].x + lb[lt].y;
+        std::vector<int2> tlf(lf.begin() + lt, lf.end()), tlb(lb.begin() + lt, lb.end());
+        S.tail_lvl_f.upload(tlf, S.stream);
+        S.tail_lvl_b.upload(tlb, S.stream);
+        const int tb_bytes = (int)tail_smem_bytes<double>(S.tail_nv, S.tail_nl);
+        ACG_CUDA(cudaFuncSetAttribute(k_tail<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tb_bytes));
+        ACG_CUDA(cudaFuncSetAttribute(k_tail<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tb_bytes));
+        ACG_CUDA(cudaFuncSetAttribute(k_tail<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tb_bytes));
+        ACG_CUDA(cudaFuncSetAttribute(k_tail<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tb_bytes));
+      } else {
+        S.tail_nl = 0;
+      }
+    }
     S.ntasks_f = (int)tf.size();
     S.ntasks_b = (int)tb.size();
     S.tasks_f.upload(tf, S.stream);
@@ -1112,6 +1185,7 @@ int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t 
                 acg_solve_info* info) {
   cudaStream_t s = S.stream;
   const int kp = round_kp(k);
+  std::unique_lock<std::recursive_mutex> glk(g_device_mu);
   ensure_batch(S, std::max(kp, S.batch_kp));
   cudaGraphExec_t& ge = S.bexec[precision][kp_index(kp)];
   if (!ge) {
@@ -1120,6 +1194,7 @@ int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t 
       ge = precision == 0 ? build_batch_fp64_graph<C>(S) : build_batch_mixed_graph<C>(S);
     });
   }
+  glk.unlock();
   PcgState* h = S.h_bst;
   std::memset(h, 0, sizeof(PcgState) * kMaxBatch);
   for (int c = 0; c < kp; ++c) {
@@ -1175,7 +1250,10 @@ int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t 
 int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, cudaMemcpyKind kout, double tol,
                  int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info) {
   cudaStream_t s = S.stream;
-  if (!S.exec[precision]) S.exec[precision] = precision == 0 ? build_fp64_graph(S) : build_mixed_graph(S);
+  if (!S.exec[precision]) {
+    std::lock_guard<std::recursive_mutex> glk(g_device_mu);
+    S.exec[precision] = precision == 0 ? build_fp64_graph(S) : build_mixed_graph(S);
+  }
   PcgState& h = *S.h_st;
   std::memset(&h, 0, sizeof(PcgState));
   h.tol = tol;
@@ -1358,6 +1436,7 @@ int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, cons
   int rc = check_device();
   if (rc != ACG_OK) return rc;
   return guarded("acg_create", [&]() {
+    std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
     auto* h = new acg_solver();
     try {
       ACG_CUDA(cudaGetDevice(&h->impl.device));
@@ -1377,6 +1456,7 @@ int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, cons
 
 void acg_destroy(acg_solver* h) {
   if (!h) return;
+  std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
   cudaStreamSynchronize(h->impl.stream);
   delete h;
 }
@@ -1408,6 +1488,8 @@ int acg_solver_stats(const acg_solver* h, acg_stats* out) {
   add(S.bx3_64);
   out->device_bytes = (int64_t)bytes;
   out->batch_capacity = S.batch_kp;
+  out->tail_levels = S.tail_nl;
+  out->tail_vertices = S.tail_nv;
   out->spmv_lanes = S.vl_spmv;
   return ACG_OK;
 }
@@ -1555,6 +1637,7 @@ int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg
   }
   return guarded("acg_time_kernels_batch", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
+    std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
     acg::time_batch(h->impl, precision, acg::round_kp(nrhs), reps, out);
     return ACG_OK;
   });
@@ -1567,6 +1650,7 @@ int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* o
   }
   return guarded("acg_time_kernels", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
+    std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
     acg::SolverImpl& S = h->impl;
     acg::time_kernels(S, precision, reps, out);
     return ACG_OK;
