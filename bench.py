@@ -163,13 +163,21 @@ def dist_setup(gpus):
 
 
 def max_over_ranks(x, world):
+    """Max of a host float over the ranks (timings are reported as the slowest rank)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_rhs_seed(rank, step, column):
+    """Seed of one right-hand side: distinct for every rank, step and column
+    (replicas solve disjoint work, so whole-job throughput adds up)."""
+    return 1_000_000 * rank + 1000 * step + column
 
 
 def barrier(world):
@@ -198,7 +206,7 @@ def run_acgpu(args):
     B = torch.empty((nsteps, k, n), dtype=torch.float64, device="cuda")
     for i in range(nsteps):
         for c in range(k):
-            B[i, c] = torch.from_numpy(rhs(n, 1_000_000 * rank + 1000 * i + c))
+            B[i, c] = torch.from_numpy(rhs(n, rank_rhs_seed(rank, i, c)))
     X = torch.empty((k, n), dtype=torch.float64, device="cuda")
     infos = (AcgSolveInfo * k)()
 
@@ -421,6 +429,57 @@ def run_config4a(args):
     dev.close()
 
 
+def run_config4b(args):
+    """256 graphs in one launch: half 2D grids with side uniform in [32, 256],
+    half random geometric graphs (n uniform in [1e3, 1e5], mean degree 8,
+    weights 1/distance, largest component); one right-hand side each; FP64 to
+    tol 1e-8.  Against the same graphs solved one after another."""
+    import acgpu
+    from acgpu import generators as G
+    rng = np.random.default_rng(44)
+    graphs = []
+    for i in range(args.group_graphs):
+        s = int(rng.integers(1 << 30))
+        if i % 2 == 0:
+            graphs.append(G.grid2(int(rng.integers(32, 257)), weights="loguniform", seed=s))
+        else:
+            graphs.append(G.largest_component(G.random_geometric(int(rng.integers(1000, 100001)), seed=s)))
+    t = time.perf_counter()
+    factors = []
+    for i, a in enumerate(graphs):
+        acgpu.seed(500 + i)
+        factors.append(acgpu.approx_chol(a))
+    factor_s = time.perf_counter() - t
+    t = time.perf_counter()
+    gs = acgpu.GroupSolver(graphs, factors)
+    upload_s = time.perf_counter() - t
+    bs = [rhs(a.shape[0], 900 + i) for i, a in enumerate(graphs)]
+    times = []
+    for rep in range(3):
+        t = time.perf_counter()
+        xs = gs(bs, tol=TOL, maxits=MAXITS)
+        times.append(time.perf_counter() - t)
+    infos = gs.last_info
+    st = gs.stats()
+    seq = []
+    for a, f, b in zip(graphs, factors, bs):
+        dev = acgpu.DeviceLapSolver(a, f)
+        dev(b, tol=TOL, maxits=MAXITS)
+        dev(b, tol=TOL, maxits=MAXITS)
+        seq.append(dev.last_info[0].solve_ms)
+        dev.close()
+    out = {"workload": f"config4b {len(graphs)} graphs in one launch (2D grids side U[32,256], RGG n U[1e3,1e5]), "
+                       "1 RHS each, tol 1e-8, fp64",
+           "n_total": int(sum(a.shape[0] for a in graphs)), "levels_max": st["levels"], "factor_s": factor_s,
+           "upload_s": upload_s, "group_ms": 1e3 * min(times), "group_solves_per_s": len(graphs) / min(times),
+           "its_max": max(i.iterations for i in infos), "true_relres_max": max(i.true_relres for i in infos),
+           "all_converged": all(i.status == 0 for i in infos),
+           "sequential_ms": float(sum(seq)), "sequential_solves_per_s": 1e3 * len(graphs) / float(sum(seq)),
+           "speedup": float(sum(seq)) / (1e3 * min(times))}
+    print(json.dumps(out), flush=True)
+    gs.close()
+
+
 def serving_graph_pool(count, seed):
     """Graphs for the serving stream: 2D/3D grids, path + random matchings and
     random geometric graphs (largest component), n log-uniform in [1e3, 1e6],
@@ -564,9 +623,10 @@ def main():
     ap.add_argument("--side", type=int, default=GRID_SIDE, help="grid side (100 = the benchmark workload)")
     ap.add_argument("--rhs", type=int, default=64, help="independent right-hand sides per step (batched)")
     ap.add_argument("--workload", default="grid3",
-                    choices=["grid3", "config1", "config3", "config4a", "serving"],
+                    choices=["grid3", "config1", "config3", "config4a", "config4b", "serving"],
                     help="grid3 = the headline line; the others report the remaining configurations")
     ap.add_argument("--serving-graphs", type=int, default=16)
+    ap.add_argument("--group-graphs", type=int, default=256)
     ap.add_argument("--serving-requests", type=int, default=300)
     ap.add_argument("--serving-rate", type=float, default=40.0, help="requests per second")
     ap.add_argument("--serving-hbm-gb", type=float, default=120.0)
@@ -581,7 +641,7 @@ def main():
     else:
         import torch
         torch.cuda.init()
-        {"config1": run_config1, "config3": run_config3, "config4a": run_config4a,
+        {"config1": run_config1, "config3": run_config3, "config4a": run_config4a, "config4b": run_config4b,
          "serving": run_serving}[args.workload](args)
 
 

@@ -174,6 +174,23 @@ int acg_solve_device(acg_solver* h, const double* b_dev, double* x_dev, double t
  * optional.  The reference solves one vector per call (src/pcg.jl:256). */
 int acg_solve_batch_device(acg_solver* h, const double* b_dev, double* x_dev, int64_t nrhs, int64_t ld, double tol,
                            int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info);
+/* ---- many graphs in one launch ------------------------------------------- */
+/* The block-diagonal union of ngraphs graphs: graph g owns vertices
+ * [offsets[g], offsets[g+1]) (contiguous blocks of the union adjacency a_*),
+ * and the factor is the union of the graphs' LDLinv factors with vertex ids
+ * shifted to the union (ncol = n - ngraphs eliminated columns: one root per
+ * graph).  Every graph keeps its own PCG (FP64, its own scalars and stop
+ * rules, src/pcg.jl:256-445), as blockSolver solves components
+ * (src/solverInterface.jl:152-188), but all graphs share every launch. */
+int acg_create_group(int64_t ngraphs, const int64_t* offsets, int64_t n, const int64_t* a_colptr,
+                     const int64_t* a_rowval, const double* a_nzval, const int64_t* ldli_col, int64_t ncol,
+                     const int64_t* ldli_colptr, const int64_t* ldli_rowval, const double* ldli_fval,
+                     const double* ldli_d, int64_t ldli_nnz, int index_base, const acg_options* opts,
+                     acg_solver** out);
+/* One right-hand side per graph (b: n values of the union, host); info[ngraphs]. */
+int acg_solve_group(acg_solver* h, const double* b, double* x, double tol, int64_t maxits, double maxtime,
+                    int stag_test, acg_solve_info* info);
+
 /* y = LDLsolver(ldli, r) (src/approxChol.jl:1347-1366) on the device; host arrays. */
 int acg_ldlsolve(acg_solver* h, const double* r, double* y, int precision);
 /* y = lap(a) * x on the device (FP64 or FP32 values); host arrays. */

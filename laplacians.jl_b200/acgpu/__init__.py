@@ -6,11 +6,12 @@ Public interface (mirrors the reference's names and keyword semantics):
 The solves run in libacgpu.so (CUDA, sm_100a); see include/acgpu.h.
 """
 from . import generators
-from .solvers import (ApproxCholParams, DeviceLapSolver, LDLinv, approx_chol, approxchol_lap, approxchol_lap1,
+from .solvers import (ApproxCholParams, DeviceLapSolver, GroupSolver, LDLinv, approx_chol, approxchol_lap, approxchol_lap1,
                       components, lap, null_solver, rng_state, seed, set_rng_state, vec_to_comps)
 from .solvers import _init as _solvers_init
 
 _solvers_init()
 
-__all__ = ["approxchol_lap", "approxchol_lap1", "ApproxCholParams", "LDLinv", "DeviceLapSolver", "approx_chol",
+__all__ = ["approxchol_lap", "approxchol_lap1", "ApproxCholParams", "LDLinv", "DeviceLapSolver", "GroupSolver",
+           "approx_chol",
            "lap", "seed", "rng_state", "set_rng_state", "components", "vec_to_comps", "null_solver", "generators"]

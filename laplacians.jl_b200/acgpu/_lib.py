@@ -66,6 +66,11 @@ SIGNATURES = [
     ("acg_device_check", ctypes.c_int, []),
     ("acg_create", ctypes.c_int, [ctypes.c_int64, i64p, i64p, f64p, i64p, i64p, i64p, f64p, f64p, ctypes.c_int64,
                                   ctypes.c_int, ctypes.POINTER(AcgOptions), ctypes.POINTER(ctypes.c_void_p)]),
+    ("acg_create_group", ctypes.c_int, [ctypes.c_int64, i64p, ctypes.c_int64, i64p, i64p, f64p, i64p, ctypes.c_int64,
+                                        i64p, i64p, f64p, f64p, ctypes.c_int64, ctypes.c_int,
+                                        ctypes.POINTER(AcgOptions), ctypes.POINTER(ctypes.c_void_p)]),
+    ("acg_solve_group", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
+                                       ctypes.c_int, ctypes.POINTER(AcgSolveInfo)]),
     ("acg_destroy", None, [ctypes.c_void_p]),
     ("acg_solver_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AcgStats)]),
     ("acg_solve", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_int64, ctypes.c_int64, ctypes.c_double,

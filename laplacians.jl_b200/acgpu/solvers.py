@@ -32,7 +32,7 @@ from ._lib import AcgOptions, AcgSolveInfo, AcgStats, check, lib
 
 __all__ = [
     "ApproxCholParams", "LDLinv", "approxchol_lap", "approxchol_lap1", "lap", "seed", "rng_state",
-    "set_rng_state", "approx_chol", "components", "vec_to_comps", "DeviceLapSolver", "null_solver",
+    "set_rng_state", "approx_chol", "components", "vec_to_comps", "DeviceLapSolver", "GroupSolver", "null_solver",
 ]
 
 _PRECISIONS = {"fp64": 0, "mixed": 1}
@@ -247,6 +247,78 @@ class DeviceLapSolver:
         y = np.empty_like(x)
         check(lib().acg_lap_mul(self._h, x, y, _PRECISIONS[precision]))
         return y
+
+
+class GroupSolver:
+    """Many graphs solved in the same launches: the block-diagonal union of the
+    graphs with the union of their factors, each graph its own PCG system
+    (blockSolver's per-component solves, src/solverInterface.jl:152-188, all at
+    once).  Every graph must be connected and have at least 2 vertices."""
+
+    def __init__(self, graphs, factors=None, *, tol=1e-6, maxits=1000, maxtime=math.inf, stag_test=5):
+        graphs = [_csc(a) for a in graphs]
+        if factors is None:
+            factors = [approx_chol(a) for a in graphs]
+        sizes = [a.shape[0] for a in graphs]
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        self.n = int(self.offsets[-1])
+        self.defaults = dict(tol=tol, maxits=maxits, maxtime=maxtime)
+        self.stag_test = stag_test
+        a = _csc(sp.block_diag(graphs, format="csc"))
+        # union factor: columns of every graph in turn, vertex ids shifted (1-based)
+        cols, ptrs, rows, fvals, ds = [], [], [], [], []
+        base_entry = 0
+        for f, off in zip(factors, self.offsets[:-1]):
+            cols.append(f.col + off)
+            ptrs.append(f.colptr[:-1] + base_entry)
+            rows.append(f.rowval + off)
+            fvals.append(f.fval)
+            ds.append(f.d)
+            base_entry += f.nnz
+        col = np.concatenate(cols).astype(np.int64)
+        colptr = np.concatenate(ptrs + [np.array([base_entry + 1])]).astype(np.int64)
+        rowval = np.concatenate(rows).astype(np.int64)
+        fval = np.concatenate(fvals)
+        d = np.concatenate(ds)
+        self.factor = LDLinv(col, colptr, rowval, fval, d)
+        opts = AcgOptions()
+        h = ctypes.c_void_p()
+        check(lib().acg_create_group(len(graphs), self.offsets, self.n, a.indptr.astype(np.int64),
+                                     a.indices.astype(np.int64), np.ascontiguousarray(a.data), col, col.shape[0],
+                                     colptr, rowval, fval, d, fval.shape[0], 1, ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+        self.ngraphs = len(graphs)
+        self.last_info = []
+
+    def __call__(self, bs, tol=None, maxits=None, maxtime=None):
+        """bs: one right-hand side per graph (list), or the union vector; returns
+        the same shape."""
+        d = self.defaults
+        tol = d["tol"] if tol is None else tol
+        maxits = d["maxits"] if maxits is None else maxits
+        maxtime = d["maxtime"] if maxtime is None else maxtime
+        as_list = isinstance(bs, (list, tuple))
+        b = np.ascontiguousarray(np.concatenate(bs) if as_list else bs, dtype=np.float64)
+        x = np.empty_like(b)
+        infos = (AcgSolveInfo * self.ngraphs)()
+        check(lib().acg_solve_group(self._h, b, x, float(tol), _maxits_int(maxits), float(maxtime), int(self.stag_test),
+                                    infos))
+        self.last_info = list(infos)
+        if as_list:
+            return [x[self.offsets[g]:self.offsets[g + 1]] for g in range(self.ngraphs)]
+        return x
+
+    def stats(self) -> dict:
+        s = AcgStats()
+        check(lib().acg_solver_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in AcgStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().acg_destroy(self._h)
+            self._h = None
+
+    __del__ = close
 
 
 def null_solver(b, **kw):

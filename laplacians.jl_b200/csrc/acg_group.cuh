@@ -1,0 +1,289 @@
+// Many graphs in one launch: the block-diagonal union of G graphs, each its
+// own PCG system with one right-hand side.
+//
+// Vertices are numbered graph by graph (graph g = internal range
+// [seg_off[g], seg_off[g+1])), so every vector of a graph is contiguous; the
+// sweeps run the union's task table (level-major across the graphs) in one
+// sync-free launch.  The vector kernels run one block per chunk of a graph
+// (SegChunk); the last block of a graph to finish sums that graph's block
+// partials in block order (deterministic) and runs the scalar PCG step on the
+// graph's PcgState.  A graph that stops is counted; when all have stopped the
+// loop condition is cleared.  This is the reference's blockSolver
+// (src/solverInterface.jl:152-188) with every component solved at once.
+#pragma once
+#include "acg_pcg.cuh"
+
+namespace acg {
+
+constexpr int kChunk = 2048;  // vector elements per block in the group kernels
+
+struct SegChunk {
+  int seg, start, end, pad;
+};
+
+struct GroupShared {
+  int stopped;         // graphs whose PCG has stopped
+  int nseg;
+  unsigned int pad[2];
+};
+
+struct GroupArgs {
+  const SegChunk* chunks;
+  const int* seg_first;   // first chunk of each graph
+  const int* seg_nchunk;  // chunks of each graph
+  unsigned int* seg_cnt;  // [8][nseg] tickets of the per-graph reductions
+  double* partials;       // [nchunks][4]
+  PcgState* st;           // per graph
+  PcgState* gst;          // group flags: done (all stopped), sweep_error
+  GroupShared* gsh;
+  int nseg;
+};
+
+// Block reduction of NV values; the last block of the chunk's graph gets the
+// graph totals in tot (thread 0) and returns true.
+template <int NV>
+__device__ __forceinline__ bool seg_reduce(double (&v)[NV], const SegChunk& c, const GroupArgs& g, int slot,
+                                           double (&tot)[NV]) {
+  __shared__ double smem[32 * NV];
+  __shared__ bool am_last;
+  block_reduce<NV>(v, smem);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) g.partials[(size_t)blockIdx.x * 4 + q] = v[q];
+    __threadfence();
+    unsigned int* cnt = &g.seg_cnt[(size_t)slot * g.nseg + c.seg];
+    am_last = atomicAdd(cnt, 1u) == (unsigned int)g.seg_nchunk[c.seg] - 1u;
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int b0 = g.seg_first[c.seg], nb = g.seg_nchunk[c.seg];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (int b = 0; b < nb; ++b) s += __ldcg(&g.partials[(size_t)(b0 + b) * 4 + q]);
+      tot[q] = s;
+    }
+    g.seg_cnt[(size_t)slot * g.nseg + c.seg] = 0u;
+  }
+  return true;
+}
+
+// A graph stopped: count it; the last one ends the loop.
+__device__ __forceinline__ void seg_stopped(const GroupArgs& g, const LoopCtl& ctl) {
+  if (atomicAdd(&g.gsh->stopped, 1) + 1 == g.nseg) {
+    g.gst->done = 1;
+    clear_loop(ctl);
+  }
+}
+
+template <typename T, int VL>
+__global__ void __launch_bounds__(kVecThreads) kg_spmv(int n, const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                       const T* __restrict__ val, const T* __restrict__ p,
+                                                       T* __restrict__ q, const PcgState* gst) {
+  if (gst->done) return;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = gt & (VL - 1);
+  const int groups = gridDim.x * blockDim.x / VL;
+  for (int base = (gt & ~31) / VL; base < n; base += groups) {
+    const int row = base + (gt & 31) / VL;
+    const bool active = row < n;
+    T s = row_dot<T, VL>(ptr, idx, val, p, row, active, lane);
+    if (active && lane == 0) q[row] = s;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_pq(const T* __restrict__ p, const T* __restrict__ q, GroupArgs g,
+                                                     double eps, LoopCtl ctl) {
+  if (g.gst->done) return;
+  const SegChunk c = g.chunks[blockIdx.x];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
+    const double pv = (double)p[i], qv = (double)q[i];
+    acc[0] += pv * qv;
+    acc[1] += fabs(pv);
+    acc[2] += fabs(qv);
+  }
+  double tot[3];
+  if (seg_reduce<3>(acc, c, g, 0, tot) && threadIdx.x == 0) {
+    PcgState* s = &g.st[c.seg];
+    if (!s->done && pcg_scalar_pq(s, tot[0], tot[1], tot[2], eps)) seg_stopped(g, ctl);
+  }
+}
+
+// x' = x + alpha p, r -= alpha q for graphs still running; s, y pending.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_update(int n, T* x3, const T* __restrict__ p, const T* __restrict__ q,
+                                                         T* __restrict__ r, T* __restrict__ s_out, T* __restrict__ y_out,
+                                                         GroupArgs g, LoopCtl ctl) {
+  if (g.gst->done) return;
+  const SegChunk c = g.chunks[blockIdx.x];
+  const PcgState* sc = &g.st[c.seg];
+  const bool act = !sc->done;
+  const double al = sc->alpha;
+  const T* xc = x3 + (size_t)sc->xcur * n;
+  T* xn = x3 + (size_t)sc->xnext * n;
+  const T pend = pending_value<T>();
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
+    s_out[i] = pend;
+    y_out[i] = pend;
+    if (!act) continue;
+    const T xv = (T)((double)xc[i] + al * (double)p[i]);
+    const T rv = (T)((double)r[i] + (-al) * (double)q[i]);
+    xn[i] = xv;
+    r[i] = rv;
+    acc[0] += (double)rv * (double)rv;
+    acc[1] += fabs((double)xv);
+    acc[2] += fabs((double)rv);
+  }
+  double tot[3];
+  if (seg_reduce<3>(acc, c, g, 1, tot) && threadIdx.x == 0) {
+    PcgState* s = &g.st[c.seg];
+    if (!s->done && pcg_scalar_update(s, tot[0], tot[1], tot[2])) seg_stopped(g, ctl);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_ysum(const T* __restrict__ y, GroupArgs g, LoopCtl ctl) {
+  if (g.gst->done) return;
+  const SegChunk c = g.chunks[blockIdx.x];
+  double acc[1] = {0.0};
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) acc[0] += (double)y[i];
+  double tot[1];
+  if (seg_reduce<1>(acc, c, g, 2, tot) && threadIdx.x == 0) {
+    PcgState* s = &g.st[c.seg];
+    s->mean = tot[0] / (double)s->nvert;
+    if (g.gst->sweep_error && !s->done) {
+      mark_stop(s, kSweepTimeout);
+      seg_stopped(g, ctl);
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_zdot(T* __restrict__ yz, const T* __restrict__ r, T* __restrict__ p,
+                                                       GroupArgs g, double eps, int init, LoopCtl ctl) {
+  if (g.gst->done) return;
+  const SegChunk c = g.chunks[blockIdx.x];
+  const double mu = g.st[c.seg].mean;
+  double acc[2] = {0.0, 0.0};
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
+    const T z = (T)((double)yz[i] - mu);
+    yz[i] = z;
+    if (init) p[i] = z;
+    acc[0] += (double)z * (double)r[i];
+    acc[1] += fabs((double)z);
+  }
+  double tot[2];
+  if (seg_reduce<2>(acc, c, g, 3, tot) && threadIdx.x == 0) {
+    PcgState* s = &g.st[c.seg];
+    if (!s->done && pcg_scalar_zdot(s, tot[0], tot[1], eps, init)) seg_stopped(g, ctl);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_pupdate(const T* __restrict__ z, T* __restrict__ p, GroupArgs g) {
+  if (g.gst->done) return;
+  const SegChunk c = g.chunks[blockIdx.x];
+  const PcgState* s = &g.st[c.seg];
+  if (s->done) return;
+  const double beta = s->beta;
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) p[i] = (T)((double)z[i] + beta * (double)p[i]);
+}
+
+// b_int = b_ext[perm]; per-graph sums -> means.  Block 0 also clears the group flags.
+__global__ void __launch_bounds__(kVecThreads) kg_gather_in(const int* __restrict__ perm, const double* __restrict__ bext,
+                                                            double* __restrict__ bint, GroupArgs g) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    g.gsh->stopped = 0;
+    g.gst->done = 0;
+    g.gst->sweep_error = 0;
+  }
+  const SegChunk c = g.chunks[blockIdx.x];
+  double acc[1] = {0.0};
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
+    const double v = bext[perm[i]];
+    bint[i] = v;
+    acc[0] += v;
+  }
+  double tot[1];
+  if (seg_reduce<1>(acc, c, g, 4, tot) && threadIdx.x == 0) g.st[c.seg].mean = tot[0] / (double)g.st[c.seg].nvert;
+}
+
+// bm = b - mean; r = bm; x0 = 0; s, y pending; per-graph |b|, state reset.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_center(double* __restrict__ bm, T* __restrict__ r, T* __restrict__ x0,
+                                                         T* __restrict__ s_out, T* __restrict__ y_out, GroupArgs g,
+                                                         LoopCtl ctl) {
+  const SegChunk c = g.chunks[blockIdx.x];
+  const double mu = g.st[c.seg].mean;
+  const T pend = pending_value<T>();
+  double acc[2] = {0.0, 0.0};
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
+    const double v = bm[i] - mu;
+    bm[i] = v;
+    r[i] = (T)v;
+    x0[i] = T(0);
+    s_out[i] = pend;
+    y_out[i] = pend;
+    acc[0] += v * v;
+    acc[1] += fabs(v);
+  }
+  double tot[2];
+  if (seg_reduce<2>(acc, c, g, 5, tot) && threadIdx.x == 0) {
+    PcgState* s = &g.st[c.seg];
+    s->nb = sqrt(tot[0]);
+    s->nb64 = s->nb;
+    s->sum_abs_r = tot[1];
+    s->sum_abs_x = 0.0;
+    s->bestnr = 1.0;
+    s->nr = 1.0;
+    s->nr_true = 1.0;
+    s->itcnt = 0;
+    s->stag_count = 0;
+    s->status = kMaxits;
+    s->done = 0;
+    s->xcur = 0;
+    s->xbest = 0;
+    s->xnext = 1;
+    if (s->nb == 0.0) {
+      s->nr_true = 0.0;
+      s->nr = 0.0;
+      mark_stop(s, kConverged);
+      seg_stopped(g, ctl);
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_take_best(int n, const T* __restrict__ x3, double* __restrict__ xf,
+                                                            GroupArgs g) {
+  const SegChunk c = g.chunks[blockIdx.x];
+  const T* xb = x3 + (size_t)g.st[c.seg].xbest * n;
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) xf[i] = (double)xb[i];
+}
+
+// per graph: |bm - L xf| / |bm| (FP64)
+__global__ void __launch_bounds__(kVecThreads) kg_true_residual(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                                const double* __restrict__ val,
+                                                                const double* __restrict__ xf,
+                                                                const double* __restrict__ bm, GroupArgs g) {
+  const SegChunk c = g.chunks[blockIdx.x];
+  double acc[1] = {0.0};
+  for (int row = c.start + threadIdx.x; row < c.end; row += blockDim.x) {
+    double s = 0.0;
+    for (int k = __ldg(&ptr[row]); k < __ldg(&ptr[row + 1]); ++k) s += __ldg(&val[k]) * xf[__ldg(&idx[k])];
+    const double t = bm[row] - s;
+    acc[0] += t * t;
+  }
+  double tot[1];
+  if (seg_reduce<1>(acc, c, g, 6, tot) && threadIdx.x == 0) {
+    PcgState* s = &g.st[c.seg];
+    s->nr_true = s->nb64 > 0.0 ? sqrt(tot[0]) / s->nb64 : 0.0;
+  }
+}
+
+}  // namespace acg

@@ -60,6 +60,7 @@ struct PcgState {
   int outer_its, outer_done;
   int max_outer;
   int sweep_error;             // a bounded wait of a sync-free sweep gave up
+  long long nvert;             // vertices of this system (graphs of a group)
   unsigned int counter[16];    // last-block tickets of the reducing kernels
 };
 

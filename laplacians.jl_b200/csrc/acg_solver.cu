@@ -16,6 +16,7 @@
 #include "../../include/acgpu.h"
 #include "acg_internal.h"
 #include "acg_batch.cuh"
+#include "acg_group.cuh"
 
 namespace acg {
 
@@ -89,6 +90,8 @@ struct SolverImpl {
   int thin_max_width = 2048;
   size_t smem_optin = 0;
   std::vector<int> lvl_off;        // host copy
+  int nseg = 1;                    // graphs in this solver (a group holds several)
+  std::vector<int> seg_off;        // graph g = internal vertices [seg_off[g], seg_off[g+1])
   std::vector<int> heavy;          // per level: vertices with forward in-degree > 32
   std::vector<SweepStep> plan[2];  // [0] FP64 values, [1] FP32 values
   int sweep_mode = 0;              // 0 sync-free cooperative sweep, 1 one launch per level
@@ -118,6 +121,18 @@ struct SolverImpl {
   std::mutex mu;
   unsigned char* noalloc_scratch = nullptr;  // device address of the fixed scratch array
 
+  // groups: several graphs in one solver (nseg > 1), one right-hand side each
+  int nchunks = 0;
+  DevBuf<SegChunk> chunks;
+  DevBuf<int> seg_first, seg_nchunk;
+  DevBuf<unsigned int> seg_cnt;
+  DevBuf<double> gpartials;
+  PcgState* gstates = nullptr;  // per graph (device)
+  PcgState* gflags = nullptr;   // group flags (device)
+  GroupShared* gsh = nullptr;
+  PcgState* h_gstates = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+
   // batched solves: kp right-hand sides per launch (vertex-major n x kp blocks)
   int batch_kp = 0;  // capacity of the batch buffers
   DevBuf<double> bb_ext, bx_ext, bbm, br64, bxf, bpartials;
@@ -137,6 +152,11 @@ struct SolverImpl {
         if (e) cudaGraphExecDestroy(e);
     if (bst) cudaFree(bst);
     if (bsh) cudaFree(bsh);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (gstates) cudaFree(gstates);
+    if (gflags) cudaFree(gflags);
+    if (gsh) cudaFree(gsh);
+    if (h_gstates) cudaFreeHost(h_gstates);
     if (h_bst) cudaFreeHost(h_bst);
     if (st) cudaFree(st);
     if (h_st) cudaFreeHost(h_st);
@@ -462,13 +482,35 @@ std::vector<float> to_f32(const std::vector<T>& v) {
   return o;
 }
 
+// Builds the device solver for one graph, or for the block-diagonal union of
+// several graphs (seg_off: G+1 vertex offsets of contiguous diagonal blocks,
+// null for one graph).  The factor has ncol eliminated columns; the vertices
+// it never eliminates (one per connected block) are the roots, with d = 0.
 void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int64_t* a_rowval, const double* a_nzval,
-                  const int64_t* col, const int64_t* colptr, const int64_t* rowval, const double* fval,
-                  const double* d, int64_t F, int base, const acg_options* opts) {
+                  const int64_t* col, int64_t ncol64, const int64_t* colptr, const int64_t* rowval,
+                  const double* fval, const double* d, int64_t F, int base, const acg_options* opts,
+                  int64_t nseg = 1, const int64_t* seg_off = nullptr) {
   if (n64 < 2 || n64 >= (int64_t)INT32_MAX) throw InputError("n must be in [2, 2^31-1)");
   if (base != 0 && base != 1) throw InputError("index_base must be 0 or 1");
   const int n = (int)n64;
   S.n = n;
+  if (nseg < 1 || nseg > n) throw InputError("graph count out of range");
+  if (ncol64 < 1 || ncol64 > n - 1) throw InputError("factor column count out of range");
+  const int ncol = (int)ncol64;
+  // ---- segments (graphs of a group)
+  std::vector<int> seg_of(n, 0);
+  S.seg_off.assign(2, 0);
+  S.seg_off[1] = n;
+  if (seg_off) {
+    if (seg_off[0] != 0 || seg_off[nseg] != n64) throw InputError("graph offsets must start at 0 and end at n");
+    S.seg_off.assign(nseg + 1, 0);
+    for (int64_t g = 0; g < nseg; ++g) {
+      if (seg_off[g + 1] - seg_off[g] < 2) throw InputError("every graph of a group needs at least 2 vertices");
+      S.seg_off[g + 1] = (int)seg_off[g + 1];
+      for (int64_t v = seg_off[g]; v < seg_off[g + 1]; ++v) seg_of[v] = (int)g;
+    }
+  }
+  S.nseg = (int)nseg;
   // ---- adjacency
   const int64_t abase = a_colptr[0];
   if (abase != 0 && abase != 1) throw InputError("adjacency colptr[0] must be 0 or 1");
@@ -477,30 +519,33 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   for (int c = 0; c < n; ++c)
     if (a_colptr[c + 1] < a_colptr[c]) throw InputError("adjacency colptr not monotone");
   // ---- factor validation
-  if (F < n - 1 || F >= (int64_t)INT32_MAX) throw InputError("factor size F out of range");
+  if (F < ncol || F >= (int64_t)INT32_MAX) throw InputError("factor size F out of range");
   std::vector<int> step(n, -1);
-  for (int ii = 0; ii < n - 1; ++ii) {
+  for (int ii = 0; ii < ncol; ++ii) {
     int64_t u = col[ii] - base;
     if (u < 0 || u >= n) throw InputError("ldli.col entry out of range");
     if (step[u] != -1) throw InputError("ldli.col repeats a vertex");
     step[u] = ii;
   }
-  int root = -1;
+  std::vector<int> roots;
   for (int v = 0; v < n; ++v)
-    if (step[v] == -1) root = v;
-  step[root] = n - 1;
+    if (step[v] == -1) {
+      step[v] = ncol + (int)roots.size();
+      roots.push_back(v);
+    }
   if (colptr[0] - base != 0) throw InputError("ldli.colptr[1] must point at the first entry");
-  for (int ii = 0; ii < n - 1; ++ii)
+  for (int ii = 0; ii < ncol; ++ii)
     if (colptr[ii + 1] <= colptr[ii]) throw InputError("ldli column " + std::to_string(ii + 1) + " is empty");
-  if (colptr[n - 1] - base != F) throw InputError("ldli.colptr[n] must equal F+1 (1-based)");
+  if (colptr[ncol] - base != F) throw InputError("ldli.colptr[end] must equal F+1 (1-based)");
   // ---- levels
   std::vector<int> lev(n, 0);
-  for (int ii = 0; ii < n - 1; ++ii) {
+  for (int ii = 0; ii < ncol; ++ii) {
     const int u = (int)(col[ii] - base);
     for (int64_t e = colptr[ii] - base; e < colptr[ii + 1] - base; ++e) {
       const int64_t j = rowval[e] - base;
       if (j < 0 || j >= n) throw InputError("ldli.rowval entry out of range");
       if (step[j] <= ii) throw InputError("ldli.rowval names a vertex eliminated earlier (not an elimination order)");
+      if (seg_of[j] != seg_of[u]) throw InputError("a factor column links two different graphs of the group");
       const double f = fval[e];
       if (!(f >= 0.0 && f <= 1.0)) throw InputError("ldli.fval entries must lie in [0, 1]");
       if (lev[j] < lev[u] + 1) lev[j] = lev[u] + 1;
@@ -511,33 +556,38 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   int nlev = 0;
   for (int v = 0; v < n; ++v) nlev = std::max(nlev, lev[v] + 1);
   S.nlev = nlev;
-  S.lvl_off.assign(nlev + 1, 0);
-  for (int v = 0; v < n; ++v) S.lvl_off[lev[v] + 1]++;
-  for (int l = 0; l < nlev; ++l) S.lvl_off[l + 1] += S.lvl_off[l];
-  // Internal order: by level; inside a level by decreasing forward in-degree
-  // (then elimination step), so the level's heavy vertices come first.
+  // Internal order: by graph, then level; inside a level by decreasing
+  // forward in-degree (then elimination step), so heavy vertices come first.
   std::vector<int> indeg(n, 0);
   for (int64_t e = 0; e < F; ++e) indeg[rowval[e] - base]++;
   std::vector<int> perm(n), e2i(n);
-  {
-    std::vector<int> pos(S.lvl_off.begin(), S.lvl_off.end() - 1);
-    for (int t = 0; t < n; ++t) {
-      const int v = t < n - 1 ? (int)(col[t] - base) : root;
-      perm[pos[lev[v]]++] = v;
-    }
-    S.heavy.assign(nlev, 0);
-    for (int l = 0; l < nlev; ++l) {
-      std::stable_sort(perm.begin() + S.lvl_off[l], perm.begin() + S.lvl_off[l + 1],
-                       [&](int x, int y) { return indeg[x] > indeg[y]; });
-      for (int i = S.lvl_off[l]; i < S.lvl_off[l + 1]; ++i)
-        if (indeg[perm[i]] > 32) S.heavy[l]++;
-    }
-    for (int i = 0; i < n; ++i) e2i[perm[i]] = i;
+  for (int v = 0; v < n; ++v) perm[v] = v;
+  std::sort(perm.begin(), perm.end(), [&](int x, int y) {
+    if (seg_of[x] != seg_of[y]) return seg_of[x] < seg_of[y];
+    if (lev[x] != lev[y]) return lev[x] < lev[y];
+    if (indeg[x] != indeg[y]) return indeg[x] > indeg[y];
+    return step[x] < step[y];
+  });
+  for (int i = 0; i < n; ++i) e2i[perm[i]] = i;
+  // level runs: runs[l] = list of {first, last+1} internal ranges of level l (one per graph)
+  std::vector<std::vector<std::pair<int, int>>> runs(nlev);
+  for (int i = 0; i < n;) {
+    int j = i;
+    while (j < n && seg_of[perm[j]] == seg_of[perm[i]] && lev[perm[j]] == lev[perm[i]]) ++j;
+    runs[lev[perm[i]]].emplace_back(i, j);
+    i = j;
   }
+  // global level offsets (meaningful for one graph: its levels are contiguous)
+  S.lvl_off.assign(nlev + 1, 0);
+  for (int v = 0; v < n; ++v) S.lvl_off[lev[v] + 1]++;
+  for (int l = 0; l < nlev; ++l) S.lvl_off[l + 1] += S.lvl_off[l];
+  S.heavy.assign(nlev, 0);
+  for (int v = 0; v < n; ++v)
+    if (indeg[v] > 32) S.heavy[lev[v]]++;
   // ---- folded coefficients
   std::vector<double> coef(F);
   std::vector<double> g(n, 1.0);
-  for (int ii = 0; ii < n - 1; ++ii) {
+  for (int ii = 0; ii < ncol; ++ii) {
     const int u = (int)(col[ii] - base);
     const int64_t j0 = colptr[ii] - base, j1 = colptr[ii + 1] - base - 1;
     double prod = 1.0;
@@ -555,7 +605,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   for (int v = 0; v < n; ++v) fptr[v + 1] += fptr[v];
   {
     std::vector<int> pos(fptr.begin(), fptr.end() - 1);
-    for (int ii = 0; ii < n - 1; ++ii) {
+    for (int ii = 0; ii < ncol; ++ii) {
       const int us = e2i[col[ii] - base];
       for (int64_t e = colptr[ii] - base; e < colptr[ii + 1] - base; ++e) {
         const int t = e2i[rowval[e] - base];
@@ -572,7 +622,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     const int u = perm[v];
     gi[v] = g[u];
     bptr[v + 1] = bptr[v];
-    if (u == root) continue;
+    if (step[u] >= ncol) continue;  // a root: no column
     const int ii = step[u];
     for (int64_t e = colptr[ii] - base; e < colptr[ii + 1] - base; ++e) {
       bidx[bptr[v + 1]] = e2i[rowval[e] - base];
@@ -686,12 +736,12 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     std::vector<int2> lf(nlev), lb(nlev);  // {first task, count} per level
     for (int l = 0; l < nlev; ++l) {
       const int t0 = (int)tf.size();
-      emit_level(tf, S.lvl_off[l], S.lvl_off[l + 1], fdeg, fptr, 32);
+      for (const auto& r : runs[l]) emit_level(tf, r.first, r.second, fdeg, fptr, 32);
       lf[l] = make_int2(t0, (int)tf.size() - t0);
     }
     for (int l = nlev - 1; l >= 0; --l) {
       const int t0 = (int)tb.size();
-      emit_level(tb, S.lvl_off[l], S.lvl_off[l + 1], outdeg, bptr, 32);
+      for (const auto& r : runs[l]) emit_level(tb, r.first, r.second, outdeg, bptr, 32);
       lb[l] = make_int2(t0, (int)tb.size() - t0);
     }
     // the tail: the longest run of final levels with at most 32 tasks in both
@@ -709,7 +759,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
         nv += w;
         lt = l;
       }
-      if (nlev - lt >= 8 && opts && opts->reserved[2] == 2) {
+      if (nlev - lt >= 8 && nseg == 1 && opts && opts->reserved[2] == 2) {
         S.tail_nl = nlev - lt;
         S.tail_v0 = S.lvl_off[lt];
         S.tail_nv = n - S.tail_v0;
@@ -743,7 +793,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     const int cap = (opts && opts->reserved[0] > 0) ? opts->reserved[0] : 1;
     S.sweep_blocks[0] = sms * std::max(1, std::min(cap, std::min(occ[0], occ[1])));
     S.sweep_blocks[1] = sms * std::max(1, std::min(cap, std::min(occ[2], occ[3])));
-    S.sweep_mode = (opts && opts->sweep_lanes == 1) ? 1 : 0;
+    S.sweep_mode = (opts && opts->sweep_lanes == 1 && nseg == 1) ? 1 : 0;
     if (opts && opts->reserved[1] > 0) S.poll_mode = opts->reserved[1] - 1;
   }
   ACG_CUDA(cudaFuncSetAttribute(k_thin<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
@@ -777,6 +827,30 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   ACG_CUDA(cudaMemsetAsync(S.st, 0, sizeof(PcgState), s));
   ACG_CUDA(cudaMallocHost(&S.h_st, sizeof(PcgState)));
   std::memset(S.h_st, 0, sizeof(PcgState));
+  if (S.nseg > 1) {
+    // chunks of at most kChunk vertices, each inside one graph
+    std::vector<SegChunk> ch;
+    std::vector<int> first(S.nseg), cnt(S.nseg);
+    for (int g = 0; g < S.nseg; ++g) {
+      first[g] = (int)ch.size();
+      for (int a = S.seg_off[g]; a < S.seg_off[g + 1]; a += kChunk)
+        ch.push_back({g, a, std::min(a + kChunk, S.seg_off[g + 1]), 0});
+      cnt[g] = (int)ch.size() - first[g];
+    }
+    S.nchunks = (int)ch.size();
+    S.chunks.upload(ch, s);
+    S.seg_first.upload(first, s);
+    S.seg_nchunk.upload(cnt, s);
+    S.seg_cnt.alloc((size_t)8 * S.nseg);
+    ACG_CUDA(cudaMemsetAsync(S.seg_cnt.p, 0, sizeof(unsigned int) * 8 * S.nseg, s));
+    S.gpartials.alloc((size_t)4 * S.nchunks);
+    ACG_CUDA(cudaMalloc(&S.gstates, sizeof(PcgState) * S.nseg));
+    ACG_CUDA(cudaMalloc(&S.gflags, sizeof(PcgState)));
+    ACG_CUDA(cudaMalloc(&S.gsh, sizeof(GroupShared)));
+    ACG_CUDA(cudaMemsetAsync(S.gflags, 0, sizeof(PcgState), s));
+    ACG_CUDA(cudaMemsetAsync(S.gsh, 0, sizeof(GroupShared), s));
+    ACG_CUDA(cudaMallocHost(&S.h_gstates, sizeof(PcgState) * S.nseg));
+  }
   ACG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -1247,6 +1321,109 @@ int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t 
   return worst;
 }
 
+// ============================================================================
+// Groups: many graphs in one launch (FP64 PCG per graph)
+// ============================================================================
+
+GroupArgs group_args(const SolverImpl& S) {
+  return GroupArgs{S.chunks.p, S.seg_first.p, S.seg_nchunk.p, S.seg_cnt.p, S.gpartials.p, S.gstates, S.gflags,
+                   S.gsh, S.nseg};
+}
+
+cudaGraphExec_t build_group_graph(SolverImpl& S) {
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  const int nb = S.nchunks;
+  const GroupArgs g = group_args(S);
+  cudaGraph_t top;
+  ACG_CUDA(cudaGraphCreate(&top, 0));
+  cudaGraphConditionalHandle h;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&h, top, 1u, cudaGraphCondAssignDefault));
+  LoopCtl ctl{h, 1};
+  const TypedArrays<double> A = arrays_of<double>(S);
+  begin_into(s, top, {});
+  // tickets of graphs that stopped while blocks of the same launch were still
+  // to start are left incomplete by those blocks: clear them every solve
+  ACG_CUDA(cudaMemsetAsync(S.seg_cnt.p, 0, sizeof(unsigned int) * 8 * S.nseg, s));
+  kg_gather_in<<<nb, kVecThreads, 0, s>>>(S.perm.p, S.b_ext.p, S.bm.p, g);
+  kg_center<double><<<nb, kVecThreads, 0, s>>>(S.bm.p, S.r64.p, S.x3_64.p, S.s64.p, S.y64.p, g, ctl);
+  enqueue_sweeps<double>(s, S, S.r64.p, S.s64.p, S.y64.p, S.gflags);
+  kg_ysum<double><<<nb, kVecThreads, 0, s>>>(S.y64.p, g, ctl);
+  kg_zdot<double><<<nb, kVecThreads, 0, s>>>(S.y64.p, S.r64.p, S.p64.p, g, kEps64, 1, ctl);
+  std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
+  end_into(s);
+  cudaGraph_t body;
+  cudaGraphNode_t wnode = add_while(top, leaves, h, &body);
+  begin_into(s, body, {});
+  kg_spmv<double, 8><<<kVecBlocks, kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, S.p64.p, S.q64.p, S.gflags);
+  kg_pq<double><<<nb, kVecThreads, 0, s>>>(S.p64.p, S.q64.p, g, kEps64, ctl);
+  kg_update<double><<<nb, kVecThreads, 0, s>>>(n, S.x3_64.p, S.p64.p, S.q64.p, S.r64.p, S.s64.p, S.y64.p, g, ctl);
+  enqueue_sweeps<double>(s, S, S.r64.p, S.s64.p, S.y64.p, S.gflags);
+  kg_ysum<double><<<nb, kVecThreads, 0, s>>>(S.y64.p, g, ctl);
+  kg_zdot<double><<<nb, kVecThreads, 0, s>>>(S.y64.p, S.r64.p, S.p64.p, g, kEps64, 0, ctl);
+  kg_pupdate<double><<<nb, kVecThreads, 0, s>>>(S.y64.p, S.p64.p, g);
+  end_into(s);
+  begin_into(s, top, {wnode});
+  kg_take_best<double><<<nb, kVecThreads, 0, s>>>(n, S.x3_64.p, S.xf.p, g);
+  kg_true_residual<<<nb, kVecThreads, 0, s>>>(S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.xf.p, S.bm.p, g);
+  k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
+  end_into(s);
+  cudaGraphExec_t exec;
+  ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
+  cudaGraphDestroy(top);
+  return exec;
+}
+
+int solve_group(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, cudaMemcpyKind kout, double tol,
+                int64_t maxits, double maxtime, int stag_test, acg_solve_info* info) {
+  cudaStream_t s = S.stream;
+  if (!S.gexec) {
+    std::lock_guard<std::recursive_mutex> glk(g_device_mu);
+    S.gexec = build_group_graph(S);
+  }
+  PcgState* h = S.h_gstates;
+  std::memset(h, 0, sizeof(PcgState) * S.nseg);
+  for (int g = 0; g < S.nseg; ++g) {
+    h[g].tol = tol;
+    h[g].maxtime_s = maxtime;
+    h[g].maxits = maxits;
+    h[g].stag_test = stag_test;
+    h[g].nvert = S.seg_off[g + 1] - S.seg_off[g];
+  }
+  ACG_CUDA(cudaMemcpyAsync(S.gstates, h, sizeof(PcgState) * S.nseg, cudaMemcpyHostToDevice, s));
+  ACG_CUDA(cudaMemcpyAsync(S.b_ext.p, b, sizeof(double) * S.n, kin, s));
+  cudaEvent_t e0, e1;
+  ACG_CUDA(cudaEventCreate(&e0));
+  ACG_CUDA(cudaEventCreate(&e1));
+  ACG_CUDA(cudaEventRecord(e0, s));
+  ACG_CUDA(cudaGraphLaunch(S.gexec, s));
+  ACG_CUDA(cudaEventRecord(e1, s));
+  ACG_CUDA(cudaMemcpyAsync(x, S.x_ext.p, sizeof(double) * S.n, kout, s));
+  ACG_CUDA(cudaMemcpyAsync(h, S.gstates, sizeof(PcgState) * S.nseg, cudaMemcpyDeviceToHost, s));
+  ACG_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int worst = 0;
+  for (int g = 0; g < S.nseg; ++g) {
+    if (info) {
+      info[g].iterations = h[g].itcnt;
+      info[g].refinements = 0;
+      info[g].relres = h[g].nr;
+      info[g].best_relres = h[g].bestnr;
+      info[g].true_relres = h[g].nr_true;
+      info[g].solve_ms = ms;
+      info[g].status = h[g].status;
+      info[g].levels = S.nlev;
+    }
+    const int rc = status_to_rc(h[g].status);
+    if (rc < 0) return rc;
+    worst = std::max(worst, rc);
+  }
+  return worst;
+}
+
 int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, cudaMemcpyKind kout, double tol,
                  int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info) {
   cudaStream_t s = S.stream;
@@ -1441,7 +1618,7 @@ int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, cons
     try {
       ACG_CUDA(cudaGetDevice(&h->impl.device));
       ACG_CUDA(cudaStreamCreateWithFlags(&h->impl.stream, cudaStreamNonBlocking));
-      acg::build_solver(h->impl, n, a_colptr, a_rowval, a_nzval, ldli_col, ldli_colptr, ldli_rowval, ldli_fval,
+      acg::build_solver(h->impl, n, a_colptr, a_rowval, a_nzval, ldli_col, n - 1, ldli_colptr, ldli_rowval, ldli_fval,
                         ldli_d, ldli_nnz, index_base, opts);
       // set-up of the allocation-free entry point, with this device current
       h->impl.noalloc_scratch = acg::noalloc_scratch_for_current_device(h->impl.device);
@@ -1496,8 +1673,9 @@ int acg_solver_stats(const acg_solver* h, acg_stats* out) {
 
 int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol, int64_t maxits,
               double maxtime, int stag_test, int precision, acg_solve_info* info) {
-  if (!h || !b || !x || nrhs < 0 || (nrhs > 1 && ldb < h->impl.n) || (precision != 0 && precision != 1)) {
-    acg::set_last_error("acg_solve: bad arguments");
+  if (!h || !b || !x || nrhs < 0 || (nrhs > 1 && ldb < h->impl.n) || (precision != 0 && precision != 1) ||
+      h->impl.nseg > 1) {
+    acg::set_last_error("acg_solve: bad arguments (a group solver takes acg_solve_group)");
     return ACG_ERR_INVALID;
   }
   return guarded("acg_solve", [&]() {
@@ -1515,6 +1693,49 @@ int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t l
       worst = std::max(worst, rc);
     }
     return worst;
+  });
+}
+
+int acg_create_group(int64_t ngraphs, const int64_t* offsets, int64_t n, const int64_t* a_colptr,
+                     const int64_t* a_rowval, const double* a_nzval, const int64_t* ldli_col, int64_t ncol,
+                     const int64_t* ldli_colptr, const int64_t* ldli_rowval, const double* ldli_fval,
+                     const double* ldli_d, int64_t ldli_nnz, int index_base, const acg_options* opts,
+                     acg_solver** out) {
+  if (!out || !offsets || !a_colptr || !a_rowval || !a_nzval || !ldli_col || !ldli_colptr || !ldli_rowval ||
+      !ldli_fval || !ldli_d || ngraphs < 1 || ncol != n - ngraphs) {
+    acg::set_last_error("acg_create_group: bad arguments (the union factor must have n - ngraphs columns)");
+    return ACG_ERR_INVALID;
+  }
+  *out = nullptr;
+  int rc = check_device();
+  if (rc != ACG_OK) return rc;
+  return guarded("acg_create_group", [&]() {
+    std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
+    auto* h = new acg_solver();
+    try {
+      ACG_CUDA(cudaGetDevice(&h->impl.device));
+      ACG_CUDA(cudaStreamCreateWithFlags(&h->impl.stream, cudaStreamNonBlocking));
+      acg::build_solver(h->impl, n, a_colptr, a_rowval, a_nzval, ldli_col, ncol, ldli_colptr, ldli_rowval, ldli_fval,
+                        ldli_d, ldli_nnz, index_base, opts, ngraphs, offsets);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return ACG_OK;
+  });
+}
+
+int acg_solve_group(acg_solver* h, const double* b, double* x, double tol, int64_t maxits, double maxtime,
+                    int stag_test, acg_solve_info* info) {
+  if (!h || !b || !x || h->impl.nseg < 2) {
+    acg::set_last_error("acg_solve_group: bad arguments (needs a solver made by acg_create_group)");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_solve_group", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    return acg::solve_group(h->impl, b, x, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol, maxits, maxtime,
+                            stag_test, info);
   });
 }
 

@@ -1,0 +1,56 @@
+"""approxchol_lap on a disconnected graph follows lapWrapComponents
+(src/solverInterface.jl:212-275): singletons get zero, components with fewer
+than 50 vertices a direct solve, larger ones the GPU solver; x agrees with the
+exact solution per component, and pcgIts is the largest count over components."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import acgpu
+from acgpu import generators as G
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _union(parts, isolated):
+    blocks = list(parts) + [sp.csc_matrix((1, 1))] * isolated
+    a = sp.block_diag(blocks, format="csc")
+    a.sort_indices()
+    return a
+
+
+def test_components_match_exact(gpu_ok):
+    parts = [G.grid2(12, weights="loguniform", seed=1), G.cycle_graph(20, np.linspace(0.5, 2, 20)),
+             G.path_plus_matchings(300, seed=2), G.star_graph(7)]
+    a = _union(parts, 5)
+    n = a.shape[0]
+    rng = np.random.default_rng(0)
+    b = rng.standard_normal(n)
+    # make b orthogonal to every component's constant vector (the solvable part)
+    co = acgpu.components(a)
+    for c in np.unique(co):
+        m = co == c
+        b[m] -= b[m].mean()
+    acgpu.seed(3)
+    its = [0]
+    f = acgpu.approxchol_lap(a, tol=1e-10, pcgIts=its)
+    x = f(b)
+    start = 0
+    for p in parts:
+        k = p.shape[0]
+        xe = O.exact_solve(p, b[start:start + k])
+        xs = x[start:start + k]
+        assert np.linalg.norm((xs - xs.mean()) - xe) <= 1e-7 * max(np.linalg.norm(xe), 1e-30)
+        start += k
+    assert np.all(x[start:] == 0)  # singletons
+    assert its[0] >= 1
+    la = acgpu.lap(a)
+    assert np.linalg.norm(la @ x - b) / np.linalg.norm(b) < 1e-8
+
+
+def test_negative_weight_error(gpu_ok):
+    a = G.grid2(6).tolil()
+    a[0, 1] = a[1, 0] = -2.0
+    with pytest.raises(ValueError):
+        acgpu.approxchol_lap(a.tocsc())
