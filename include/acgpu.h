@@ -87,10 +87,17 @@ typedef struct {
   int wide_level_min;  /* levels at least this wide get a grid launch each; runs of
                           narrower levels whose values fit in shared memory run in
                           one CTA with block barriers (default 2048)              */
-  int reserved[5];     /* [0]: resident sweep blocks per SM (0 = 1); [1]: poll mode + 1
-                          (1 tight+sleep, 2 tight only, 3 backoff); [2]: 2 = sweep
-                          the final narrow levels in one CTA (experimental);
-                          others 0                                                */
+  int sweep_blocks_per_sm;   /* resident blocks per SM of the single-vector sweeps (0 = 1) */
+  int poll_mode;             /* waits on a pending value: 0 = automatic, 1 tight+sleep,
+                                2 tight only, 3 backoff                               */
+  int tail;                  /* 2 = sweep the final narrow levels in one CTA from shared
+                                memory (experimental); 0 = off                         */
+  int batch_bwd_heavy;       /* batched sweeps: vertices with more entries than this get a
+                                whole warp (0 = 8); backward and forward tables       */
+  int batch_fwd_heavy;
+  int batch_blocks_per_sm;   /* resident blocks per SM of the batched sweeps (0 = the
+                                occupancy limit)                                       */
+  int reserved[2];           /* 0 */
 } acg_options;
 
 /* Shape of an uploaded solver. */

@@ -29,7 +29,9 @@ u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
 
 class AcgOptions(ctypes.Structure):
     _fields_ = [("sweep_lanes", ctypes.c_int), ("spmv_lanes", ctypes.c_int), ("wide_level_min", ctypes.c_int),
-                ("reserved", ctypes.c_int * 5)]
+                ("sweep_blocks_per_sm", ctypes.c_int), ("poll_mode", ctypes.c_int), ("tail", ctypes.c_int),
+                ("batch_bwd_heavy", ctypes.c_int), ("batch_fwd_heavy", ctypes.c_int),
+                ("batch_blocks_per_sm", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
 
 
 class AcgStats(ctypes.Structure):

@@ -148,7 +148,8 @@ __global__ void __launch_bounds__(kSweepThreads) kb_sweep(int ntasks, const Swee
                                                           T* out, BatchShared* bs) {
   if (bs->all_done) return;
   constexpr int kp = CPL * kBatchLanes;
-  constexpr int EB = (CPL * sizeof(T) >= 32) ? 2 : (CPL * sizeof(T) >= 16 ? 4 : 8);
+  // rows loaded per batch: a whole slot of 8 entries where registers allow
+  constexpr int EB = (CPL * sizeof(T) <= 32) ? 8 : 4;
   const int lane = threadIdx.x & 31;
   const int gl = lane & 7;
   const int W = (int)((gridDim.x * blockDim.x) >> 5);

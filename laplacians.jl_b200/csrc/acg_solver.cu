@@ -142,6 +142,9 @@ struct SolverImpl {
   BatchShared* bsh = nullptr;
   PcgState* h_bst = nullptr;
   int bsweep_blocks[2][4] = {};          // [precision][log2(kp/8)]
+  int batch_bps = 0;                     // batched sweep blocks per SM (0 = occupancy limit)
+  int ntasks_bb = 0, ntasks_fb = 0;      // task tables of the batched sweeps
+  DevBuf<SweepTask> tasks_bb, tasks_fb;
   cudaGraphExec_t bexec[2][4] = {};
 
   ~SolverImpl() {
@@ -630,6 +633,29 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
       bptr[v + 1]++;
     }
   }
+  // Entries of a vertex in the order their values become ready: the sweeps
+  // walk a long row in rounds, and the input finished last (forward: the
+  // highest internal index; backward: the lowest) belongs in the last round
+  // so the earlier rounds overlap the wait for it.
+  {
+    std::vector<std::pair<int, double>> tmp;
+    auto order = [&](std::vector<int>& ptr, std::vector<int>& ix, std::vector<double>& cv, bool descending) {
+      for (int v = 0; v < n; ++v) {
+        tmp.clear();
+        for (int k = ptr[v]; k < ptr[v + 1]; ++k) tmp.emplace_back(ix[k], cv[k]);
+        if (descending)
+          std::stable_sort(tmp.begin(), tmp.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        else
+          std::stable_sort(tmp.begin(), tmp.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+        for (int k = ptr[v]; k < ptr[v + 1]; ++k) {
+          ix[k] = tmp[k - ptr[v]].first;
+          cv[k] = tmp[k - ptr[v]].second;
+        }
+      }
+    };
+    order(fptr, fidx, fc, false);
+    order(bptr, bidx, bc, true);
+  }
   // Laplacian rows in internal order; diagonal = a*ones summed in column order
   std::vector<int> lptr(n + 1, 0), lidx(m + n);
   std::vector<double> lv(m + n);
@@ -759,7 +785,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
         nv += w;
         lt = l;
       }
-      if (nlev - lt >= 8 && nseg == 1 && opts && opts->reserved[2] == 2) {
+      if (nlev - lt >= 8 && nseg == 1 && opts && opts->tail == 2) {
         S.tail_nl = nlev - lt;
         S.tail_v0 = S.lvl_off[lt];
         S.tail_nv = n - S.tail_v0;
@@ -777,6 +803,21 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
         S.tail_nl = 0;
       }
     }
+    // task tables of the batched sweeps: a vertex with more than bheavy
+    // (backward) or fheavy (forward) entries gets a whole warp
+    {
+      const int bheavy = (opts && opts->batch_bwd_heavy > 0) ? opts->batch_bwd_heavy : 8;
+      const int fheavy = (opts && opts->batch_fwd_heavy > 0) ? opts->batch_fwd_heavy : 8;
+      std::vector<SweepTask> tbb, tfb;
+      for (int l = nlev - 1; l >= 0; --l)
+        for (const auto& r : runs[l]) emit_level(tbb, r.first, r.second, outdeg, bptr, bheavy);
+      for (int l = 0; l < nlev; ++l)
+        for (const auto& r : runs[l]) emit_level(tfb, r.first, r.second, fdeg, fptr, fheavy);
+      S.ntasks_bb = (int)tbb.size();
+      S.tasks_bb.upload(tbb, S.stream);
+      S.ntasks_fb = (int)tfb.size();
+      S.tasks_fb.upload(tfb, S.stream);
+    }
     S.ntasks_f = (int)tf.size();
     S.ntasks_b = (int)tb.size();
     S.tasks_f.upload(tf, S.stream);
@@ -790,11 +831,12 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_sweep<float, false>, kSweepThreads, 0));
     // One resident block (8 warps) per SM by default: more warps mostly add
     // polling traffic on the L2 without shortening the dependency chains.
-    const int cap = (opts && opts->reserved[0] > 0) ? opts->reserved[0] : 1;
+    const int cap = (opts && opts->sweep_blocks_per_sm > 0) ? opts->sweep_blocks_per_sm : 1;
     S.sweep_blocks[0] = sms * std::max(1, std::min(cap, std::min(occ[0], occ[1])));
     S.sweep_blocks[1] = sms * std::max(1, std::min(cap, std::min(occ[2], occ[3])));
     S.sweep_mode = (opts && opts->sweep_lanes == 1 && nseg == 1) ? 1 : 0;
-    if (opts && opts->reserved[1] > 0) S.poll_mode = opts->reserved[1] - 1;
+    if (opts && opts->poll_mode > 0) S.poll_mode = opts->poll_mode - 1;
+    S.batch_bps = (opts && opts->batch_blocks_per_sm > 0) ? opts->batch_blocks_per_sm : 0;
   }
   ACG_CUDA(cudaFuncSetAttribute(k_thin<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
   ACG_CUDA(cudaFuncSetAttribute(k_thin<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
@@ -1090,8 +1132,8 @@ void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, const T* 
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  ACG_CUDA(cudaLaunchKernelEx(&cfg, kb_sweep<T, CPL, kForward>, kForward ? S.ntasks_f : S.ntasks_b,
-                              (const SweepTask*)(kForward ? S.tasks_f.p : S.tasks_b.p), kForward ? A.fi : A.bi,
+  ACG_CUDA(cudaLaunchKernelEx(&cfg, kb_sweep<T, CPL, kForward>, kForward ? S.ntasks_fb : S.ntasks_bb,
+                              (const SweepTask*)(kForward ? S.tasks_fb.p : S.tasks_bb.p), kForward ? A.fi : A.bi,
                               kForward ? A.fc : A.bc, aux, sfwd, out, S.bsh));
 }
 
@@ -1210,11 +1252,13 @@ cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S) {
 }
 
 template <typename T, int CPL>
-int batch_occupancy(int sms) {
+int batch_occupancy(int sms, int cap) {
   int a = 0, b = 0;
   ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kb_sweep<T, CPL, true>, kSweepThreads, 0));
   ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kb_sweep<T, CPL, false>, kSweepThreads, 0));
-  return sms * std::max(1, std::min(a, b));
+  int m = std::min(a, b);
+  if (cap > 0) m = std::min(m, cap);
+  return sms * std::max(1, m);
 }
 
 void ensure_batch(SolverImpl& S, int kp) {
@@ -1226,14 +1270,14 @@ void ensure_batch(SolverImpl& S, int kp) {
     S.bpartials.alloc((size_t)4 * kVecBlocks * kMaxBatch);
     int sms = 0;
     ACG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S.device));
-    S.bsweep_blocks[0][0] = batch_occupancy<double, 1>(sms);
-    S.bsweep_blocks[0][1] = batch_occupancy<double, 2>(sms);
-    S.bsweep_blocks[0][2] = batch_occupancy<double, 4>(sms);
-    S.bsweep_blocks[0][3] = batch_occupancy<double, 8>(sms);
-    S.bsweep_blocks[1][0] = batch_occupancy<float, 1>(sms);
-    S.bsweep_blocks[1][1] = batch_occupancy<float, 2>(sms);
-    S.bsweep_blocks[1][2] = batch_occupancy<float, 4>(sms);
-    S.bsweep_blocks[1][3] = batch_occupancy<float, 8>(sms);
+    S.bsweep_blocks[0][0] = batch_occupancy<double, 1>(sms, S.batch_bps);
+    S.bsweep_blocks[0][1] = batch_occupancy<double, 2>(sms, S.batch_bps);
+    S.bsweep_blocks[0][2] = batch_occupancy<double, 4>(sms, S.batch_bps);
+    S.bsweep_blocks[0][3] = batch_occupancy<double, 8>(sms, S.batch_bps);
+    S.bsweep_blocks[1][0] = batch_occupancy<float, 1>(sms, S.batch_bps);
+    S.bsweep_blocks[1][1] = batch_occupancy<float, 2>(sms, S.batch_bps);
+    S.bsweep_blocks[1][2] = batch_occupancy<float, 4>(sms, S.batch_bps);
+    S.bsweep_blocks[1][3] = batch_occupancy<float, 8>(sms, S.batch_bps);
   }
   if (kp <= S.batch_kp) return;
   // growing the buffers invalidates every captured batch graph
