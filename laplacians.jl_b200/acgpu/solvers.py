@@ -182,6 +182,7 @@ class DeviceLapSolver:
                                np.ascontiguousarray(a.data), ldli.col, ldli.colptr, ldli.rowval, ldli.fval, ldli.d,
                                ldli.nnz, 1, ctypes.byref(opts), ctypes.byref(h)))
         self._h = h
+        self._lib = lib()
         self.last_info: list[AcgSolveInfo] = []
 
     def stats(self) -> dict:
@@ -191,7 +192,9 @@ class DeviceLapSolver:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().acg_destroy(self._h)
+            # the library handle taken at creation: module globals may be gone
+            # when this runs from __del__ at interpreter exit
+            self._lib.acg_destroy(self._h)
             self._h = None
 
     __del__ = close
@@ -287,6 +290,7 @@ class GroupSolver:
                                      a.indices.astype(np.int64), np.ascontiguousarray(a.data), col, col.shape[0],
                                      colptr, rowval, fval, d, fval.shape[0], 1, ctypes.byref(opts), ctypes.byref(h)))
         self._h = h
+        self._lib = lib()
         self.ngraphs = len(graphs)
         self.last_info = []
 
@@ -315,7 +319,9 @@ class GroupSolver:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().acg_destroy(self._h)
+            # the library handle taken at creation: module globals may be gone
+            # when this runs from __del__ at interpreter exit
+            self._lib.acg_destroy(self._h)
             self._h = None
 
     __del__ = close

@@ -1566,8 +1566,8 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
   out->forward_launches = 1;
   const double vb = sizeof(T), nv = S.n, F = (double)S.nnz_f;
   out->spmv_bytes = 4.0 * (nv + 1) + (double)S.nnz_l * (4.0 + vb) + 2.0 * nv * kp * vb;
-  out->forward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_f + 3.0 * nv * kp * vb;
-  out->backward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_b + nv * vb + 3.0 * nv * kp * vb;
+  out->forward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_fb + 3.0 * nv * kp * vb;
+  out->backward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_bb + nv * vb + 3.0 * nv * kp * vb;
   BatchShared hb;
   ACG_CUDA(cudaMemcpy(&hb, S.bsh, sizeof(BatchShared), cudaMemcpyDeviceToHost));
   if (hb.sweep_error) throw CudaError("a batched sweep wait gave up while timing");
