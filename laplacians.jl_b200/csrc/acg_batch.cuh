@@ -225,6 +225,11 @@ __global__ void __launch_bounds__(kSweepThreads) kb_sweep(int ntasks, const Swee
           for (int q = 0; q < CPL; ++q) acc[q] += cs[u] * vals[u].v[q];
         }
       }
+      // Reconverge explicitly after the (divergent, sleeping) waits: without
+      // it the next shuffle waits for the lanes that skipped the wait far
+      // longer than the wait itself (measured: 2.9 us instead of 0.9 us per
+      // dependency hop at 64 columns).
+      __syncwarp();
     }
     if (gw == 32) {  // combine the four groups of a heavy task
 #pragma unroll

@@ -507,6 +507,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const Sweep
     }
     for (int k = e0.k0 + kEntryUnroll * gw; k < e0.k1; k += gw)
       acc += __ldg(&coef[k]) * wait_value(&out[__ldg(&idx[k])], st, poll_mode);
+    __syncwarp();  // reconverge after the divergent waits before the shuffles
     acc = group_sum_w(acc, gw);
     if (e0.active && (lane & (gw - 1)) == 0) st_relaxed(&out[e0.v], kForward ? e0.a + acc : e0.a * e0.own + acc);
     e0 = e1;
