@@ -97,7 +97,12 @@ typedef struct {
   int batch_fwd_heavy;
   int batch_blocks_per_sm;   /* resident blocks per SM of the batched sweeps (0 = the
                                 occupancy limit)                                       */
-  int reserved[2];           /* 0 */
+  int sweep_heavy;           /* single-vector sweeps: vertices with more entries than this
+                                get a whole warp (0 = 16)                              */
+  int dense_tail;            /* largest number of final-level vertices whose substitution
+                                is replaced by a dense triangular product (0 = 4096,
+                                -1 = none; at most 8192 and n/4)                       */
+  int reserved[1];           /* 0 */
 } acg_options;
 
 /* Shape of an uploaded solver. */
@@ -113,6 +118,8 @@ typedef struct {
   int64_t batch_capacity; /* right-hand sides its batch buffers hold (0 = none) */
   int64_t tail_levels;    /* final levels swept by one CTA from shared memory    */
   int64_t tail_vertices;  /* vertices of those levels                           */
+  int64_t dense_levels;   /* final levels replaced by the dense triangular block */
+  int64_t dense_vertices; /* K: vertices of that block (0 = none)                */
 } acg_stats;
 
 /* Outcome of one solve (one right-hand side). */

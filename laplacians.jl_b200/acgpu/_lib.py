@@ -31,7 +31,8 @@ class AcgOptions(ctypes.Structure):
     _fields_ = [("sweep_lanes", ctypes.c_int), ("spmv_lanes", ctypes.c_int), ("wide_level_min", ctypes.c_int),
                 ("sweep_blocks_per_sm", ctypes.c_int), ("poll_mode", ctypes.c_int), ("tail", ctypes.c_int),
                 ("batch_bwd_heavy", ctypes.c_int), ("batch_fwd_heavy", ctypes.c_int),
-                ("batch_blocks_per_sm", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
+                ("batch_blocks_per_sm", ctypes.c_int), ("sweep_heavy", ctypes.c_int),
+                ("dense_tail", ctypes.c_int), ("reserved", ctypes.c_int * 1)]
 
 
 class AcgStats(ctypes.Structure):
@@ -39,7 +40,8 @@ class AcgStats(ctypes.Structure):
                 ("levels", ctypes.c_int64), ("wide_levels", ctypes.c_int64), ("thin_runs", ctypes.c_int64),
                 ("sweep_lanes", ctypes.c_int), ("spmv_lanes", ctypes.c_int), ("device_bytes", ctypes.c_int64),
                 ("batch_capacity", ctypes.c_int64), ("tail_levels", ctypes.c_int64),
-                ("tail_vertices", ctypes.c_int64)]
+                ("tail_vertices", ctypes.c_int64), ("dense_levels", ctypes.c_int64),
+                ("dense_vertices", ctypes.c_int64)]
 
 
 class AcgSolveInfo(ctypes.Structure):

@@ -11,11 +11,13 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/acgpu.h"
 #include "acg_internal.h"
 #include "acg_batch.cuh"
+#include "acg_dense.cuh"
 #include "acg_group.cuh"
 
 namespace acg {
@@ -143,6 +145,12 @@ struct SolverImpl {
   PcgState* h_bst = nullptr;
   int bsweep_blocks[2][4] = {};          // [precision][log2(kp/8)]
   int batch_bps = 0;                     // batched sweep blocks per SM (0 = occupancy limit)
+  // dense tail: vertices [dt_v0, n) (levels >= dt_L0) handled by s_T = M w_T,
+  // y_T = M^T (g_T s_T) with M = (I - C_TT)^{-1} (K x K, row-major); K = 0: none
+  int dt_K = 0, dt_v0 = 0, dt_L0 = 0;
+  DevBuf<double> dt_M64, dt_part;        // dt_part: partial tiles (chunks x K x columns, as T)
+  DevBuf<float> dt_M32;
+  size_t dt_part_cols = 0;               // columns dt_part holds
   int ntasks_bb = 0, ntasks_fb = 0;      // task tables of the batched sweeps
   DevBuf<SweepTask> tasks_bb, tasks_fb;
   cudaGraphExec_t bexec[2][4] = {};
@@ -181,18 +189,18 @@ int choose_vl(double avg) {
 template <typename T>
 struct TypedArrays {
   const int *fp, *fi, *bp, *bi, *lp, *li;
-  const T *fc, *bc, *g, *lv;
+  const T *fc, *bc, *g, *lv, *dm;
 };
 
 template <typename T>
 TypedArrays<T> arrays_of(const SolverImpl& S);
 template <>
 TypedArrays<double> arrays_of<double>(const SolverImpl& S) {
-  return {S.f_ptr.p, S.f_idx.p, S.b_ptr.p, S.b_idx.p, S.l_ptr.p, S.l_idx.p, S.f_c64.p, S.b_c64.p, S.g64.p, S.l_v64.p};
+  return {S.f_ptr.p, S.f_idx.p, S.b_ptr.p, S.b_idx.p, S.l_ptr.p, S.l_idx.p, S.f_c64.p, S.b_c64.p, S.g64.p, S.l_v64.p, S.dt_M64.p};
 }
 template <>
 TypedArrays<float> arrays_of<float>(const SolverImpl& S) {
-  return {S.f_ptr.p, S.f_idx.p, S.b_ptr.p, S.b_idx.p, S.l_ptr.p, S.l_idx.p, S.f_c32.p, S.b_c32.p, S.g32.p, S.l_v32.p};
+  return {S.f_ptr.p, S.f_idx.p, S.b_ptr.p, S.b_idx.p, S.l_ptr.p, S.l_idx.p, S.f_c32.p, S.b_c32.p, S.g32.p, S.l_v32.p, S.dt_M32.p};
 }
 
 #define ACG_VL_SWITCH(vl, FN, ...)                   \
@@ -275,9 +283,34 @@ void enqueue_tail(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sf
       kForward ? S.tasks_f.p : S.tasks_b.p, kForward ? A.fi : A.bi, kForward ? A.fc : A.bc, aux, sfwd, out, st);
 }
 
+// The dense tail step of a sweep on kp-column vectors (kp = 1, or 8 * CPL):
+// forward s_T = M w_T in place in sv; backward y_T = M^T (g_T s_T).  part
+// holds the partial tiles; done (device) ends the step early when set.
+template <typename T, int CPL>
+void enqueue_dense(cudaStream_t s, const SolverImpl& S, bool fwd, T* sv, T* y, T* part, const int* done) {
+  constexpr int kp = CPL == 0 ? 1 : 8 * CPL;
+  const int K = S.dt_K;
+  const TypedArrays<T> A = arrays_of<T>(S);
+  const size_t off = (size_t)S.dt_v0 * kp;
+  const dim3 grid(dense_row_tiles(K), dense_chunks(K));
+  const T* g = A.g + S.dt_v0;
+  if constexpr (CPL == 0) {
+    if (fwd) kd1_partial<T, true><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done);
+    else kd1_partial<T, false><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done);
+  } else {
+    if (fwd) kd_partial<T, CPL, true><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done);
+    else kd_partial<T, CPL, false><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done);
+  }
+  ACG_CUDA(cudaGetLastError());
+  const int rb = (int)std::min<long long>(kVecBlocks, ((long long)K * kp + kVecThreads - 1) / kVecThreads);
+  if (fwd) kd_reduce<T, true><<<rb, kVecThreads, 0, s>>>(K, kp, part, sv + off, done);
+  else kd_reduce<T, false><<<rb, kVecThreads, 0, s>>>(K, kp, part, y + off, done);
+}
+
 // Forward sweep: s = forward values of r (s must be pending in sync-free mode).
+// part: partial tiles of the dense tail (null: the solver's own buffer).
 template <typename T>
-void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, PcgState* st) {
+void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, PcgState* st, T* part = nullptr) {
   if (S.sweep_mode == 0) {
     if (S.tail_nl > 0) {
       enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.tail_tf0);
@@ -285,15 +318,20 @@ void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, Pcg
     } else {
       enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.ntasks_f);
     }
+    if (S.dt_K)
+      enqueue_dense<T, 0>(s, S, true, sv, (T*)nullptr, part ? part : reinterpret_cast<T*>(S.dt_part.p), &st->done);
     return;
   }
   for (const SweepStep& step : S.plan[plan_index<T>()]) enqueue_step<T, true>(s, S, step, r, (const T*)nullptr, sv, st);
 }
 // Backward sweep: y from the forward values s (y pending in sync-free mode).
 template <typename T>
-void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, PcgState* st) {
+void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, PcgState* st, T* part = nullptr) {
   const T* g = arrays_of<T>(S).g;
   if (S.sweep_mode == 0) {
+    if (S.dt_K)
+      enqueue_dense<T, 0>(s, S, false, const_cast<T*>(sv), y, part ? part : reinterpret_cast<T*>(S.dt_part.p),
+                          &st->done);
     if (S.tail_nl > 0) {
       enqueue_tail<T, false>(s, S, g, sv, y, st);
       enqueue_syncfree<T, false>(s, S, g, sv, y, st, S.tail_tb0, S.ntasks_b);
@@ -307,9 +345,9 @@ void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, Pc
 }
 // y = LDLinv sweeps of r (without the final mean removal); sv is scratch.
 template <typename T>
-void enqueue_sweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y, PcgState* st) {
-  enqueue_forward<T>(s, S, r, sv, st);
-  enqueue_backward<T>(s, S, sv, y, st);
+void enqueue_sweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y, PcgState* st, T* part = nullptr) {
+  enqueue_forward<T>(s, S, r, sv, st, part);
+  enqueue_backward<T>(s, S, sv, y, st, part);
 }
 
 template <typename T, int VL>
@@ -656,6 +694,70 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     order(fptr, fidx, fc, false);
     order(bptr, bidx, bc, true);
   }
+  // ---- dense tail: the final levels as one dense triangular block (one
+  // graph, sync-free sweeps; the per-level engine and the one-CTA tail keep
+  // the full entry lists)
+  S.dt_K = 0;
+  if (nseg == 1 && !(opts && (opts->sweep_lanes == 1 || opts->tail == 2 || opts->dense_tail < 0))) {
+    int kmax = (opts && opts->dense_tail > 0) ? opts->dense_tail : kDenseDefaultK;
+    kmax = std::min(std::min(kmax, kDenseMaxK), n / 4);
+    int L0 = nlev;
+    while (L0 > 0 && n - S.lvl_off[L0 - 1] <= kmax) --L0;
+    if (nlev - L0 >= kDenseMinLevels && n - S.lvl_off[L0] > 0) {
+      S.dt_L0 = L0;
+      S.dt_v0 = S.lvl_off[L0];
+      S.dt_K = n - S.dt_v0;
+    }
+  }
+  std::vector<double> dense_m;
+  if (S.dt_K) {
+    const int K = S.dt_K, v0 = S.dt_v0;
+    // M = (I - C_TT)^{-1}, row by row: M[i,:] = e_i + sum over tail inputs u of
+    // i of coef * M[u,:] (inputs precede i in internal order).  Threads own
+    // interleaved blocks of 64 columns and walk all rows, so no thread waits
+    // for another and each entry is summed in one fixed order.
+    dense_m.assign((size_t)K * K, 0.0);
+    const int nthreads = std::max(1, std::min(32, (int)std::thread::hardware_concurrency()));
+    auto work = [&](int tid) {
+      for (int i = 0; i < K; ++i) {
+        double* row = &dense_m[(size_t)i * K];
+        for (int cb = tid * 64; cb <= i; cb += nthreads * 64) {
+          const int ce = std::min(cb + 64, i + 1);
+          if (i >= cb && i < ce) row[i] = 1.0;
+          for (int k = fptr[v0 + i]; k < fptr[v0 + i + 1]; ++k) {
+            const int u = fidx[k] - v0;
+            if (u < 0) continue;
+            const double c = fc[k];
+            const double* mu = &dense_m[(size_t)u * K];
+            const int e2 = std::min(ce, u + 1);
+            for (int j = cb; j < e2; ++j) row[j] += c * mu[j];
+          }
+        }
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto& t : pool) t.join();
+    // the sweep keeps only the head inputs of tail vertices (a prefix: entries
+    // are in increasing internal order)
+    std::vector<int> nptr(n + 1, 0);
+    int w = 0;
+    for (int v = 0; v < n; ++v) {
+      const int k0 = fptr[v], k1 = fptr[v + 1];
+      nptr[v] = w;
+      for (int k = k0; k < k1; ++k) {
+        if (v >= v0 && fidx[k] >= v0) break;
+        fidx[w] = fidx[k];
+        fc[w] = fc[k];
+        ++w;
+      }
+    }
+    nptr[n] = w;
+    fptr.swap(nptr);
+    fidx.resize(w);
+    fc.resize(w);
+  }
   // Laplacian rows in internal order; diagonal = a*ones summed in column order
   std::vector<int> lptr(n + 1, 0), lidx(m + n);
   std::vector<double> lv(m + n);
@@ -726,8 +828,9 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     }
   }
   // ---- sync-free task tables: tasks in level order (backward: reverse level
-  // order); a vertex with more than 32 entries is a task of its own on a
-  // whole warp, other vertices go four to a task within one level.
+  // order); a vertex with more than sweep_heavy entries (default 16) is a
+  // task of its own on a whole warp, other vertices go four to a task within
+  // one level.
   {
     std::vector<int> outdeg(n, 0);
     for (int v = 0; v < n; ++v) outdeg[v] = bptr[v + 1] - bptr[v];
@@ -758,16 +861,19 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     };
     std::vector<int> fdeg(n);
     for (int v = 0; v < n; ++v) fdeg[v] = fptr[v + 1] - fptr[v];
+    const int sheavy = (opts && opts->sweep_heavy > 0) ? opts->sweep_heavy : 16;
     std::vector<SweepTask> tf, tb;
     std::vector<int2> lf(nlev), lb(nlev);  // {first task, count} per level
     for (int l = 0; l < nlev; ++l) {
       const int t0 = (int)tf.size();
-      for (const auto& r : runs[l]) emit_level(tf, r.first, r.second, fdeg, fptr, 32);
+      for (const auto& r : runs[l]) emit_level(tf, r.first, r.second, fdeg, fptr, sheavy);
       lf[l] = make_int2(t0, (int)tf.size() - t0);
     }
-    for (int l = nlev - 1; l >= 0; --l) {
+    const int blev = S.dt_K ? S.dt_L0 : nlev;  // levels the backward sweep walks
+    for (int l = nlev - 1; l >= blev; --l) lb[l] = make_int2((int)tb.size(), 0);
+    for (int l = blev - 1; l >= 0; --l) {
       const int t0 = (int)tb.size();
-      for (const auto& r : runs[l]) emit_level(tb, r.first, r.second, outdeg, bptr, 32);
+      for (const auto& r : runs[l]) emit_level(tb, r.first, r.second, outdeg, bptr, sheavy);
       lb[l] = make_int2(t0, (int)tb.size() - t0);
     }
     // the tail: the longest run of final levels with at most 32 tasks in both
@@ -809,7 +915,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
       const int bheavy = (opts && opts->batch_bwd_heavy > 0) ? opts->batch_bwd_heavy : 8;
       const int fheavy = (opts && opts->batch_fwd_heavy > 0) ? opts->batch_fwd_heavy : 8;
       std::vector<SweepTask> tbb, tfb;
-      for (int l = nlev - 1; l >= 0; --l)
+      for (int l = blev - 1; l >= 0; --l)
         for (const auto& r : runs[l]) emit_level(tbb, r.first, r.second, outdeg, bptr, bheavy);
       for (int l = 0; l < nlev; ++l)
         for (const auto& r : runs[l]) emit_level(tfb, r.first, r.second, fdeg, fptr, fheavy);
@@ -860,6 +966,13 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   S.b_c32.upload(to_f32(bc), s);
   S.g64.upload(gi, s);
   S.g32.upload(to_f32(gi), s);
+  if (S.dt_K) {
+    S.dt_M64.upload(dense_m, s);
+    S.dt_M32.upload(to_f32(dense_m), s);
+    // partial tiles for up to kMaxBatch columns, so no later growth moves them
+    S.dt_part_cols = kMaxBatch;
+    S.dt_part.alloc((size_t)dense_chunks(S.dt_K) * S.dt_K * kMaxBatch);
+  }
   for (DevBuf<double>* b : {&S.b_ext, &S.x_ext, &S.bm, &S.r64, &S.s64, &S.y64, &S.p64, &S.q64, &S.xf}) b->alloc(n);
   S.x3_64.alloc((size_t)3 * n);
   for (DevBuf<float>* b : {&S.r32, &S.s32, &S.y32, &S.p32, &S.q32}) b->alloc(n);
@@ -952,13 +1065,18 @@ void ldlsolve_impl(SolverImpl& S, T* rbuf, T* sbuf, T* ybuf) {
 // graph (the allocator may not be called then), or a serving loop whose device
 // memory comes from a pool that must not grow after start-up.  For them
 // acg_ldlsolve_noalloc keeps every piece of its scratch (the input in solver
-// order, the forward and backward sweep vectors, the reduction partials and
-// the scalar state) in the one fixed array below, which the library reserves
-// on every GPU it is loaded on, for as long as the process lives.
+// order, the forward and backward sweep vectors, the reduction partials, the
+// dense tail's partial tiles and the scalar state) in the one fixed array
+// below, which the library reserves on every GPU it is loaded on, for as long
+// as the process lives.
 constexpr int kNoAllocMaxN = ACG_NOALLOC_MAX_N;
 constexpr size_t kNoAllocVec = (size_t)kNoAllocMaxN * sizeof(double);
 constexpr size_t kNoAllocPartials = (size_t)4 * kMaxPartialBlocks * sizeof(double);
-constexpr size_t kNoAllocBytes = 4 * kNoAllocVec + kNoAllocPartials + ((sizeof(PcgState) + 255) / 256) * 256;
+// a dense tail has at most min(kDenseMaxK, n / 4) vertices
+constexpr int kNoAllocDenseK = kDenseMaxK < kNoAllocMaxN / 4 ? kDenseMaxK : kNoAllocMaxN / 4;
+constexpr size_t kNoAllocDense = (size_t)dense_chunks(kNoAllocDenseK) * kNoAllocDenseK * sizeof(double);
+constexpr size_t kNoAllocState = 4 * kNoAllocVec + kNoAllocPartials + kNoAllocDense;
+constexpr size_t kNoAllocBytes = kNoAllocState + ((sizeof(PcgState) + 255) / 256) * 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -987,14 +1105,15 @@ void ldlsolve_noalloc_impl(const SolverImpl& S, cudaStream_t s, const double* r_
   T* sv = reinterpret_cast<T*>(base + 2 * kNoAllocVec);
   T* yv = reinterpret_cast<T*>(base + 3 * kNoAllocVec);
   double* partials = reinterpret_cast<double*>(base + 4 * kNoAllocVec);
-  PcgState* st = reinterpret_cast<PcgState*>(base + 4 * kNoAllocVec + kNoAllocPartials);
+  T* dense_part = reinterpret_cast<T*>(base + 4 * kNoAllocVec + kNoAllocPartials);
+  PcgState* st = reinterpret_cast<PcgState*>(base + kNoAllocState);
   LoopCtl none{0, 0};
   // the state (done flag, sweep error flag, reduction tickets) must start at zero
   ACG_CUDA(cudaMemsetAsync(st, 0, sizeof(PcgState), s));
   k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, r_ext, r64, st, partials);
   k_cast_from64<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, r64, rT);
   k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, sv, yv);
-  enqueue_sweeps<T>(s, S, rT, sv, yv, st);
+  enqueue_sweeps<T>(s, S, rT, sv, yv, st, dense_part);
   k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, yv, st, partials, none);
   k_minus_mean<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, yv, st, r64);
   k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, r64, y_ext);
@@ -1002,7 +1121,7 @@ void ldlsolve_noalloc_impl(const SolverImpl& S, cudaStream_t s, const double* r_
 
 int noalloc_sweep_error(unsigned char* base) {
   PcgState hs;
-  ACG_CUDA(cudaMemcpy(&hs, base + 4 * kNoAllocVec + kNoAllocPartials, sizeof(PcgState), cudaMemcpyDeviceToHost));
+  ACG_CUDA(cudaMemcpy(&hs, base + kNoAllocState, sizeof(PcgState), cudaMemcpyDeviceToHost));
   return hs.sweep_error;
 }
 
@@ -1137,10 +1256,21 @@ void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, const T* 
                               kForward ? A.fc : A.bc, aux, sfwd, out, S.bsh));
 }
 
+// Batched forward (s from r) and backward (y from s) sweeps, dense tail included.
+template <typename T, int CPL>
+void enqueue_bforward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv) {
+  enqueue_bsweep<T, CPL, true>(s, S, r, (const T*)nullptr, sv);
+  if (S.dt_K) enqueue_dense<T, CPL>(s, S, true, sv, (T*)nullptr, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
+}
+template <typename T, int CPL>
+void enqueue_bbackward(cudaStream_t s, const SolverImpl& S, T* sv, T* y) {
+  if (S.dt_K) enqueue_dense<T, CPL>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
+  enqueue_bsweep<T, CPL, false>(s, S, arrays_of<T>(S).g, sv, y);
+}
 template <typename T, int CPL>
 void enqueue_bsweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y) {
-  enqueue_bsweep<T, CPL, true>(s, S, r, (const T*)nullptr, sv);
-  enqueue_bsweep<T, CPL, false>(s, S, arrays_of<T>(S).g, sv, y);
+  enqueue_bforward<T, CPL>(s, S, r, sv);
+  enqueue_bbackward<T, CPL>(s, S, sv, y);
 }
 
 template <typename T, int CPL>
@@ -1555,11 +1685,11 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
   out->spmv_ms = time_graph([&]() { kb_spmv<T, CPL><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, A.lp, A.li, A.lv, p, q, S.bsh); });
   out->forward_ms = time_graph([&]() {
     fill_s();
-    enqueue_bsweep<T, CPL, true>(s, S, r, (const T*)nullptr, sv);
+    enqueue_bforward<T, CPL>(s, S, r, sv);
   }) - t_fill;
   out->backward_ms = time_graph([&]() {
     fill_y();
-    enqueue_bsweep<T, CPL, false>(s, S, A.g, sv, y);
+    enqueue_bbackward<T, CPL>(s, S, sv, y);
   }) - t_fill;
   out->iteration_ms = 0.0;
   out->launches_per_iteration = 9;
@@ -1711,6 +1841,8 @@ int acg_solver_stats(const acg_solver* h, acg_stats* out) {
   out->batch_capacity = S.batch_kp;
   out->tail_levels = S.tail_nl;
   out->tail_vertices = S.tail_nv;
+  out->dense_levels = S.dt_K ? S.nlev - S.dt_L0 : 0;
+  out->dense_vertices = S.dt_K;
   out->spmv_lanes = S.vl_spmv;
   return ACG_OK;
 }

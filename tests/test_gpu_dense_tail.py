@@ -1,0 +1,89 @@
+"""The dense tail: the final levels of the LDLinv DAG applied as one dense
+triangular product instead of level-by-level substitution.
+
+It is the same linear operator as src/approxChol.jl:1347-1408 up to rounding,
+so the FP64 LDLsolver must agree with the oracle to 1e-12 relative (the
+tolerance of the sweep parity tests), with the same solver built without a
+dense tail to 1e-12, and FP32 to 1e-4.  Tail sizes that do not fill the
+32-row and 256-index tiles of the dense kernels are covered, as are the
+batched (several right-hand sides) path and full PCG solves.
+"""
+import numpy as np
+import pytest
+
+import acgpu
+from acgpu import generators as G
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(x, y):
+    return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+
+
+GRAPHS = [
+    ("grid3_20_logw", lambda: G.grid3(20, weights="loguniform", seed=31)),
+    ("grid2_90", lambda: G.grid2(90)),
+    ("pm_12000", lambda: G.path_plus_matchings(12000, seed=32)),
+]
+
+
+@pytest.fixture(scope="module", params=GRAPHS, ids=[g[0] for g in GRAPHS])
+def graph(gpu_ok, request):
+    a = request.param[1]()
+    acgpu.seed(3)
+    ldli = acgpu.approx_chol(a)
+    plain = acgpu.DeviceLapSolver(a, ldli, options=dict(dense_tail=-1))
+    yield a, ldli, plain
+    plain.close()
+
+
+@pytest.mark.parametrize("kmax", [0, 1000, 777, 33])
+def test_ldlsolve_with_dense_tail(graph, kmax):
+    a, ldli, plain = graph
+    n = a.shape[0]
+    dev = acgpu.DeviceLapSolver(a, ldli, options=dict(dense_tail=kmax))
+    st = dev.stats()
+    assert plain.stats()["dense_vertices"] == 0
+    limit = min(kmax if kmax > 0 else 4096, n // 4)
+    assert 0 <= st["dense_vertices"] <= limit
+    if kmax in (0, 1000):
+        assert st["dense_vertices"] > 0 and st["dense_levels"] >= 8
+    rng = np.random.default_rng(kmax)
+    r = rng.standard_normal(n)
+    r -= r.mean()
+    y_ref = O.ldlsolve(ldli, r)
+    y = dev.ldlsolve(r)
+    assert _rel(y, y_ref) < 1e-12
+    assert _rel(y, plain.ldlsolve(r)) < 1e-12
+    assert _rel(dev.ldlsolve(r, "mixed"), y_ref) < 1e-4
+    # twice in a row: the dense step keeps no state between calls
+    assert np.array_equal(dev.ldlsolve(r), y)
+    dev.close()
+
+
+def test_solves_with_dense_tail(graph):
+    a, ldli, plain = graph
+    n = a.shape[0]
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    assert dev.stats()["dense_vertices"] > 0
+    orc = O.OracleSolver(a, ldli)
+    b = np.random.default_rng(5).standard_normal(n)
+    its = [0]
+    x = dev(b, tol=1e-9, maxits=500, pcgIts=its)
+    xo, ito, _, _ = orc(b, tol=1e-9, maxits=500)
+    assert abs(its[0] - ito) <= 1
+    assert _rel(O.center(x), O.center(xo)) < 1e-7
+    xm = dev(b, tol=1e-8, maxits=2000, precision="mixed")
+    assert O.relres(a, xm, b - b.mean()) <= 1e-8 * 1.01
+    # batched columns through the dense tail agree with the solver without one
+    B = np.random.default_rng(6).standard_normal((n, 12))
+    X = dev(B, tol=1e-9, maxits=500)
+    Xp = plain(B, tol=1e-9, maxits=500)
+    for c in range(12):
+        assert _rel(O.center(X[:, c]), O.center(Xp[:, c])) < 1e-7
+    Xm = dev(B, tol=1e-8, maxits=2000, precision="mixed")
+    for c in range(12):
+        assert O.relres(a, Xm[:, c], B[:, c] - B[:, c].mean()) <= 1e-8 * 1.01
+    dev.close()
