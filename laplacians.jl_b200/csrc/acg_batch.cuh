@@ -13,6 +13,10 @@
 namespace acg {
 
 constexpr int kMaxBatch = 64;
+// launch shape of the per-iteration batched vector kernels: 2 blocks of 512
+// threads per SM, each thread keeping four elements' loads in flight
+constexpr int kBVecThreads = 512;
+constexpr int kBVecBlocks = 148 * 2;
 constexpr int kBatchLanes = 8;  // lanes per vertex in the batched sweeps and mat-vec
 
 struct BatchShared {
@@ -288,7 +292,7 @@ __global__ void __launch_bounds__(kVecThreads) kb_spmv(int n, const int* __restr
 template <int NV>
 __device__ __forceinline__ bool batch_reduce(double (&v)[NV], int kp, double* partials, unsigned int* counter,
                                              double (&out)[NV]) {
-  __shared__ double sm[NV][kVecThreads];
+  __shared__ double sm[NV][kBVecThreads];
   __shared__ bool am_last;
 #pragma unroll
   for (int q = 0; q < NV; ++q) sm[q][threadIdx.x] = v[q];
@@ -310,11 +314,35 @@ __device__ __forceinline__ bool batch_reduce(double (&v)[NV], int kp, double* pa
   __syncthreads();
   if (!am_last) return false;
   __threadfence();
+  // The last block: thread t sums, in block order, the partials of column
+  // t % kp from a fixed contiguous range of blocks (part t / kp of `per`);
+  // then the parts are added in order.  The shape depends only on the launch.
+  {
+    const int c = threadIdx.x % kp, part = threadIdx.x / kp;
+    const int G = gridDim.x;
+    const int b0 = (int)((long long)G * part / per), b1 = (int)((long long)G * (part + 1) / per);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      const double* pq = partials + (size_t)q * G * kp + c;
+      double s = 0.0;
+      int b = b0;
+      for (; b + 8 <= b1; b += 8) {
+        double l[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) l[u] = __ldcg(pq + (size_t)(b + u) * kp);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s += l[u];
+      }
+      for (; b < b1; ++b) s += __ldcg(pq + (size_t)b * kp);
+      sm[q][threadIdx.x] = s;
+    }
+  }
+  __syncthreads();
   if ((int)threadIdx.x < kp) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       double s = 0.0;
-      for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(&partials[((size_t)q * gridDim.x + b) * kp + threadIdx.x]);
+      for (int j = 0; j < per; ++j) s += sm[q][threadIdx.x + j * kp];
       out[q] = s;
     }
   }
@@ -335,15 +363,37 @@ __device__ __forceinline__ void batch_check_all(PcgState* st, BatchShared* bs, i
   }
 }
 
+// The per-iteration kernels below walk their n*kp elements with a grid
+// stride that is a multiple of kp (each thread keeps one column) and four
+// strides per step, all loads issued before any arithmetic; per-thread sums
+// still run in element order.
+constexpr int kBU = 4;
+
 // pq, |p|_1, |q|_1 per column -> alpha, stagnation tests 1 and 2
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) kb_pq(int n, int kp, const T* __restrict__ p, const T* __restrict__ q,
-                                                     PcgState* st, BatchShared* bs, double* partials, double eps,
-                                                     LoopCtl ctl) {
+__global__ void __launch_bounds__(kBVecThreads) kb_pq(int n, int kp, const T* __restrict__ p, const T* __restrict__ q,
+                                                      PcgState* st, BatchShared* bs, double* partials, double eps,
+                                                      LoopCtl ctl) {
   if (bs->all_done) return;
   const size_t N = (size_t)n * kp;
+  const size_t S = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[3] = {0.0, 0.0, 0.0};
-  for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+  for (; i + (kBU - 1) * S < N; i += kBU * S) {
+    T pv[kBU], qv[kBU];
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      pv[u] = p[i + u * S];
+      qv[u] = q[i + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      acc[0] += (double)pv[u] * (double)qv[u];
+      acc[1] += fabs((double)pv[u]);
+      acc[2] += fabs((double)qv[u]);
+    }
+  }
+  for (; i < N; i += S) {
     const double pv = (double)p[i], qv = (double)q[i];
     acc[0] += pv * qv;
     acc[1] += fabs(pv);
@@ -359,13 +409,13 @@ __global__ void __launch_bounds__(kVecThreads) kb_pq(int n, int kp, const T* __r
 
 // x' = x + alpha p, r -= alpha q (active columns); s, y pending; |r|^2, |x'|_1, |r|_1
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) kb_update(int n, int kp, T* x3, const T* __restrict__ p,
-                                                         const T* __restrict__ q, T* __restrict__ r, T* __restrict__ s_out,
-                                                         T* __restrict__ y_out, PcgState* st, BatchShared* bs,
-                                                         double* partials, LoopCtl ctl) {
+__global__ void __launch_bounds__(kBVecThreads) kb_update(int n, int kp, T* x3, const T* __restrict__ p,
+                                                          const T* __restrict__ q, T* __restrict__ r,
+                                                          T* __restrict__ s_out, T* __restrict__ y_out, PcgState* st,
+                                                          BatchShared* bs, double* partials, LoopCtl ctl) {
   if (bs->all_done) return;
   const size_t N = (size_t)n * kp;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t S = (size_t)gridDim.x * blockDim.x;
   const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = (int)(i0 % kp);
   const bool act = !st[c].done;
@@ -374,7 +424,34 @@ __global__ void __launch_bounds__(kVecThreads) kb_update(int n, int kp, T* x3, c
   T* xn = x3 + (size_t)st[c].xnext * N;
   const T pend = pending_value<T>();
   double acc[3] = {0.0, 0.0, 0.0};
-  for (size_t i = i0; i < N; i += stride) {
+  size_t i = i0;
+  for (; i + (kBU - 1) * S < N; i += kBU * S) {
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      s_out[i + u * S] = pend;
+      y_out[i + u * S] = pend;
+    }
+    if (!act) continue;
+    T xv[kBU], pv[kBU], qv[kBU], rv[kBU];
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      xv[u] = xc[i + u * S];
+      pv[u] = p[i + u * S];
+      qv[u] = q[i + u * S];
+      rv[u] = r[i + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      const T xw = (T)((double)xv[u] + al * (double)pv[u]);
+      const T rw = (T)((double)rv[u] + (-al) * (double)qv[u]);
+      xn[i + u * S] = xw;
+      r[i + u * S] = rw;
+      acc[0] += (double)rw * (double)rw;
+      acc[1] += fabs((double)xw);
+      acc[2] += fabs((double)rw);
+    }
+  }
+  for (; i < N; i += S) {
     s_out[i] = pend;
     y_out[i] = pend;
     if (!act) continue;
@@ -395,13 +472,21 @@ __global__ void __launch_bounds__(kVecThreads) kb_update(int n, int kp, T* x3, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) kb_ysum(int n, int kp, const T* __restrict__ y, PcgState* st,
-                                                       BatchShared* bs, double* partials, LoopCtl ctl) {
+__global__ void __launch_bounds__(kBVecThreads) kb_ysum(int n, int kp, const T* __restrict__ y, PcgState* st,
+                                                        BatchShared* bs, double* partials, LoopCtl ctl) {
   if (bs->all_done) return;
   const size_t N = (size_t)n * kp;
+  const size_t S = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0.0};
-  for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
-    acc[0] += (double)y[i];
+  for (; i + (kBU - 1) * S < N; i += kBU * S) {
+    T yv[kBU];
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) yv[u] = y[i + u * S];
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) acc[0] += (double)yv[u];
+  }
+  for (; i < N; i += S) acc[0] += (double)y[i];
   double tot[1];
   if (batch_reduce<1>(acc, kp, partials, &bs->counter[2], tot)) {
     const int c = threadIdx.x;
@@ -415,16 +500,34 @@ __global__ void __launch_bounds__(kVecThreads) kb_ysum(int n, int kp, const T* _
 
 // z = y - mean (in place); rho = z.r, |z|_1; the iteration's remaining scalar steps
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) kb_zdot(int n, int kp, T* __restrict__ yz, const T* __restrict__ r,
-                                                       T* __restrict__ p, PcgState* st, BatchShared* bs,
-                                                       double* partials, double eps, int init, LoopCtl ctl) {
+__global__ void __launch_bounds__(kBVecThreads) kb_zdot(int n, int kp, T* __restrict__ yz, const T* __restrict__ r,
+                                                        T* __restrict__ p, PcgState* st, BatchShared* bs,
+                                                        double* partials, double eps, int init, LoopCtl ctl) {
   if (bs->all_done) return;
   const size_t N = (size_t)n * kp;
+  const size_t S = (size_t)gridDim.x * blockDim.x;
   const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = (int)(i0 % kp);
   const double mu = st[c].mean;
   double acc[2] = {0.0, 0.0};
-  for (size_t i = i0; i < N; i += (size_t)gridDim.x * blockDim.x) {
+  size_t i = i0;
+  for (; i + (kBU - 1) * S < N; i += kBU * S) {
+    T yv[kBU], rv[kBU];
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      yv[u] = yz[i + u * S];
+      rv[u] = r[i + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      const T z = (T)((double)yv[u] - mu);
+      yz[i + u * S] = z;
+      if (init) p[i + u * S] = z;
+      acc[0] += (double)z * (double)rv[u];
+      acc[1] += fabs((double)z);
+    }
+  }
+  for (; i < N; i += S) {
     const T z = (T)((double)yz[i] - mu);
     yz[i] = z;
     if (init) p[i] = z;
@@ -440,15 +543,27 @@ __global__ void __launch_bounds__(kVecThreads) kb_zdot(int n, int kp, T* __restr
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) kb_pupdate(int n, int kp, const T* __restrict__ z, T* __restrict__ p,
-                                                          const PcgState* st, const BatchShared* bs) {
+__global__ void __launch_bounds__(kBVecThreads) kb_pupdate(int n, int kp, const T* __restrict__ z, T* __restrict__ p,
+                                                           const PcgState* st, const BatchShared* bs) {
   if (bs->all_done) return;
   const size_t N = (size_t)n * kp;
+  const size_t S = (size_t)gridDim.x * blockDim.x;
   const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = (int)(i0 % kp);
   if (st[c].done) return;
   const double beta = st[c].beta;
-  for (size_t i = i0; i < N; i += (size_t)gridDim.x * blockDim.x) p[i] = (T)((double)z[i] + beta * (double)p[i]);
+  size_t i = i0;
+  for (; i + (kBU - 1) * S < N; i += kBU * S) {
+    T zv[kBU], pv[kBU];
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      zv[u] = z[i + u * S];
+      pv[u] = p[i + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) p[i + u * S] = (T)((double)zv[u] + beta * (double)pv[u]);
+  }
+  for (; i < N; i += S) p[i] = (T)((double)z[i] + beta * (double)p[i]);
 }
 
 // ---- set-up and wrap-up ------------------------------------------------------

@@ -1280,12 +1280,12 @@ void enqueue_biteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* y, 
   const TypedArrays<T> A = arrays_of<T>(S);
   const int n = S.n;
   kb_spmv<T, CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, p, q, S.bsh);
-  kb_pq<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, ctl);
-  kb_update<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, x3, p, q, r, sv, y, S.bst, S.bsh, S.bpartials.p, ctl);
+  kb_pq<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, ctl);
+  kb_update<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, x3, p, q, r, sv, y, S.bst, S.bsh, S.bpartials.p, ctl);
   enqueue_bsweeps<T, CPL>(s, S, r, sv, y);
-  kb_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, y, S.bst, S.bsh, S.bpartials.p, ctl);
-  kb_zdot<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, y, r, p, S.bst, S.bsh, S.bpartials.p, eps, 0, ctl);
-  kb_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, y, p, S.bst, S.bsh);
+  kb_ysum<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, y, S.bst, S.bsh, S.bpartials.p, ctl);
+  kb_zdot<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, y, r, p, S.bst, S.bsh, S.bpartials.p, eps, 0, ctl);
+  kb_pupdate<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, y, p, S.bst, S.bsh);
 }
 
 template <int CPL>
@@ -1306,8 +1306,8 @@ cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S) {
   kb_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, x3, S.bs64.p, S.by64.p, S.bst,
                                                        S.bsh, S.bpartials.p, ctl);
   enqueue_bsweeps<double, CPL>(s, S, S.br64.p, S.bs64.p, S.by64.p);
-  kb_ysum<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.by64.p, S.bst, S.bsh, S.bpartials.p, ctl);
-  kb_zdot<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.by64.p, S.br64.p, S.bp64.p, S.bst, S.bsh,
+  kb_ysum<double><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, S.by64.p, S.bst, S.bsh, S.bpartials.p, ctl);
+  kb_zdot<double><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, S.by64.p, S.br64.p, S.bp64.p, S.bst, S.bsh,
                                                      S.bpartials.p, kEps64, 1, ctl);
   std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
   end_into(s);
@@ -1356,8 +1356,8 @@ cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S) {
   kb_outer_prep<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.br64.p, S.br32.p, S.bx3_32.p, S.bs32.p, S.by32.p,
                                                           S.bst, S.bsh, S.bpartials.p, ictl);
   enqueue_bsweeps<float, CPL>(s, S, S.br32.p, S.bs32.p, S.by32.p);
-  kb_ysum<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.by32.p, S.bst, S.bsh, S.bpartials.p, ictl);
-  kb_zdot<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.by32.p, S.br32.p, S.bp32.p, S.bst, S.bsh, S.bpartials.p,
+  kb_ysum<float><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, S.by32.p, S.bst, S.bsh, S.bpartials.p, ictl);
+  kb_zdot<float><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, S.by32.p, S.br32.p, S.bp32.p, S.bst, S.bsh, S.bpartials.p,
                                                     eps32, 2, ictl);
   std::vector<cudaGraphNode_t> ol = capture_leaves(s);
   end_into(s);
