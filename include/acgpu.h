@@ -145,6 +145,11 @@ typedef struct {
   /* algorithmic bytes per call: every structure entry, task record and vector
      element the kernel must touch once (re-reads not counted) */
   double spmv_bytes, forward_bytes, backward_bytes;
+  /* the sweep kernel alone, without the dense tail products (equal to
+     forward_ms / backward_ms when the solver has no dense tail) */
+  double forward_sweep_ms, backward_sweep_ms;
+  double dense_ms;          /* both dense tail products (forward + backward) */
+  double forward_sweep_bytes, backward_sweep_bytes, dense_bytes;
 } acg_kernel_times;
 
 /* 0 if the current CUDA device is usable (sm_100), else an error code. */

@@ -54,7 +54,10 @@ class AcgKernelTimes(ctypes.Structure):
     _fields_ = [("spmv_ms", ctypes.c_double), ("forward_ms", ctypes.c_double), ("backward_ms", ctypes.c_double),
                 ("iteration_ms", ctypes.c_double), ("launches_per_iteration", ctypes.c_int),
                 ("forward_launches", ctypes.c_int), ("spmv_bytes", ctypes.c_double),
-                ("forward_bytes", ctypes.c_double), ("backward_bytes", ctypes.c_double)]
+                ("forward_bytes", ctypes.c_double), ("backward_bytes", ctypes.c_double),
+                ("forward_sweep_ms", ctypes.c_double), ("backward_sweep_ms", ctypes.c_double),
+                ("dense_ms", ctypes.c_double), ("forward_sweep_bytes", ctypes.c_double),
+                ("backward_sweep_bytes", ctypes.c_double), ("dense_bytes", ctypes.c_double)]
 
 
 # (name, restype, argtypes) for every entry point of include/acgpu.h

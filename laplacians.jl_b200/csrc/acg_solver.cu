@@ -87,6 +87,7 @@ struct SolverImpl {
   cudaStream_t stream = nullptr;
   int n = 0;
   int64_t nnz_l = 0, nnz_f = 0;
+  int64_t nnz_fsweep = 0, nnz_bsweep = 0;  // entries the forward / backward sweeps walk
   int nlev = 0;
   int vl_spmv = 8;
   int thin_max_width = 2048;
@@ -310,7 +311,8 @@ void enqueue_dense(cudaStream_t s, const SolverImpl& S, bool fwd, T* sv, T* y, T
 // Forward sweep: s = forward values of r (s must be pending in sync-free mode).
 // part: partial tiles of the dense tail (null: the solver's own buffer).
 template <typename T>
-void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, PcgState* st, T* part = nullptr) {
+void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, PcgState* st, T* part = nullptr,
+                     bool dense = true) {
   if (S.sweep_mode == 0) {
     if (S.tail_nl > 0) {
       enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.tail_tf0);
@@ -318,7 +320,7 @@ void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, Pcg
     } else {
       enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.ntasks_f);
     }
-    if (S.dt_K)
+    if (S.dt_K && dense)
       enqueue_dense<T, 0>(s, S, true, sv, (T*)nullptr, part ? part : reinterpret_cast<T*>(S.dt_part.p), &st->done);
     return;
   }
@@ -326,10 +328,11 @@ void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, Pcg
 }
 // Backward sweep: y from the forward values s (y pending in sync-free mode).
 template <typename T>
-void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, PcgState* st, T* part = nullptr) {
+void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, PcgState* st, T* part = nullptr,
+                      bool dense = true) {
   const T* g = arrays_of<T>(S).g;
   if (S.sweep_mode == 0) {
-    if (S.dt_K)
+    if (S.dt_K && dense)
       enqueue_dense<T, 0>(s, S, false, const_cast<T*>(sv), y, part ? part : reinterpret_cast<T*>(S.dt_part.p),
                           &st->done);
     if (S.tail_nl > 0) {
@@ -926,6 +929,8 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     }
     S.ntasks_f = (int)tf.size();
     S.ntasks_b = (int)tb.size();
+    S.nnz_fsweep = fptr[n];
+    S.nnz_bsweep = bptr[S.dt_K ? S.dt_v0 : n];
     S.tasks_f.upload(tf, S.stream);
     S.tasks_b.upload(tb, S.stream);
     int sms = 0;
@@ -1193,16 +1198,40 @@ void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv,
     k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, none);
     k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, q, S.st);
   });
-  const double vb = sizeof(T), nv = S.n, F = (double)S.nnz_f;
+  out->forward_sweep_ms = time_graph([&]() {
+    fill_s();
+    enqueue_forward<T>(s, S, r, sv, S.st, (T*)nullptr, false);
+  }) - t_fill;
+  // the backward sweep alone reads the tail values the dense product wrote in
+  // the backward_ms runs above, so only the head is marked pending
+  auto fill_yh = [&]() {
+    k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.dt_K ? S.dt_v0 : S.n, y, (T*)nullptr);
+  };
+  const double t_fill_h = time_graph(fill_yh);
+  out->backward_sweep_ms = time_graph([&]() {
+    fill_yh();
+    enqueue_backward<T>(s, S, sv, y, S.st, (T*)nullptr, false);
+  }) - t_fill_h;
+  out->dense_ms = S.dt_K ? time_graph([&]() {
+    enqueue_dense<T, 0>(s, S, true, sv, (T*)nullptr, reinterpret_cast<T*>(S.dt_part.p), &S.st->done);
+    enqueue_dense<T, 0>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.st->done);
+  }) : 0.0;
+  const double vb = sizeof(T), nv = S.n;
   // mat-vec: row pointers, (index, value) per entry, x once, y (FP64) out
   out->spmv_bytes = 4.0 * (nv + 1) + (double)S.nnz_l * (4.0 + vb) + nv * vb + nv * 8.0;
   // sweeps: (index, coefficient) per entry, one 32-byte task record per task,
   // aux (r or g) in, own forward value (backward), each input value once, output
-  out->forward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_f + nv * vb * 3.0;
-  out->backward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_b + nv * vb * 4.0;
+  out->forward_sweep_bytes = (double)S.nnz_fsweep * (4.0 + vb) + 32.0 * S.ntasks_f + nv * vb * 3.0;
+  out->backward_sweep_bytes = (double)S.nnz_bsweep * (4.0 + vb) + 32.0 * S.ntasks_b + nv * vb * 4.0;
+  // dense tail: the K(K+1)/2 entries of M once per product
+  const double kk = (double)S.dt_K;
+  out->dense_bytes = 2.0 * kk * (kk + 1.0) / 2.0 * vb;
+  out->forward_bytes = out->forward_sweep_bytes + out->dense_bytes / 2.0;
+  out->backward_bytes = out->backward_sweep_bytes + out->dense_bytes / 2.0;
   const int sweep_launches = S.sweep_mode == 0 ? 1 : (int)S.plan[plan_index<T>()].size();
-  out->launches_per_iteration = 6 + 2 * sweep_launches;
-  out->forward_launches = sweep_launches;
+  const int dense_launches = S.dt_K ? 2 : 0;
+  out->launches_per_iteration = 6 + 2 * (sweep_launches + dense_launches);
+  out->forward_launches = sweep_launches + dense_launches;
   ACG_CUDA(cudaStreamSynchronize(s));
   PcgState hs;
   ACG_CUDA(cudaMemcpy(&hs, S.st, sizeof(PcgState), cudaMemcpyDeviceToHost));
@@ -1691,13 +1720,36 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
     fill_y();
     enqueue_bbackward<T, CPL>(s, S, sv, y);
   }) - t_fill;
+  out->forward_sweep_ms = time_graph([&]() {
+    fill_s();
+    enqueue_bsweep<T, CPL, true>(s, S, r, (const T*)nullptr, sv);
+  }) - t_fill;
+  // the backward sweep alone reads the tail rows the dense product wrote in
+  // the backward_ms runs above, so only the head is marked pending
+  auto fill_yh = [&]() {
+    k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)((size_t)(S.dt_K ? S.dt_v0 : S.n) * kp), y, (T*)nullptr);
+  };
+  const double t_fill_h = time_graph(fill_yh);
+  out->backward_sweep_ms = time_graph([&]() {
+    fill_yh();
+    enqueue_bsweep<T, CPL, false>(s, S, A.g, sv, y);
+  }) - t_fill_h;
+  out->dense_ms = S.dt_K ? time_graph([&]() {
+    enqueue_dense<T, CPL>(s, S, true, sv, (T*)nullptr, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
+    enqueue_dense<T, CPL>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
+  }) : 0.0;
   out->iteration_ms = 0.0;
-  out->launches_per_iteration = 9;
-  out->forward_launches = 1;
-  const double vb = sizeof(T), nv = S.n, F = (double)S.nnz_f;
+  const int dense_launches = S.dt_K ? 2 : 0;
+  out->launches_per_iteration = 8 + 2 * dense_launches;
+  out->forward_launches = 1 + dense_launches;
+  const double vb = sizeof(T), nv = S.n;
   out->spmv_bytes = 4.0 * (nv + 1) + (double)S.nnz_l * (4.0 + vb) + 2.0 * nv * kp * vb;
-  out->forward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_fb + 3.0 * nv * kp * vb;
-  out->backward_bytes = F * (4.0 + vb) + 32.0 * S.ntasks_bb + nv * vb + 3.0 * nv * kp * vb;
+  out->forward_sweep_bytes = (double)S.nnz_fsweep * (4.0 + vb) + 32.0 * S.ntasks_fb + 3.0 * nv * kp * vb;
+  out->backward_sweep_bytes = (double)S.nnz_bsweep * (4.0 + vb) + 32.0 * S.ntasks_bb + nv * vb + 3.0 * nv * kp * vb;
+  const double kk = (double)S.dt_K;
+  out->dense_bytes = 2.0 * kk * (kk + 1.0) / 2.0 * vb;
+  out->forward_bytes = out->forward_sweep_bytes + out->dense_bytes / 2.0;
+  out->backward_bytes = out->backward_sweep_bytes + out->dense_bytes / 2.0;
   BatchShared hb;
   ACG_CUDA(cudaMemcpy(&hb, S.bsh, sizeof(BatchShared), cudaMemcpyDeviceToHost));
   if (hb.sweep_error) throw CudaError("a batched sweep wait gave up while timing");

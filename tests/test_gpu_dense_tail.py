@@ -87,3 +87,24 @@ def test_solves_with_dense_tail(graph):
     for c in range(12):
         assert O.relres(a, Xm[:, c], B[:, c] - B[:, c].mean()) <= 1e-8 * 1.01
     dev.close()
+
+
+def test_kernel_timing_with_dense_tail(graph):
+    """The timing entry points run every sweep variant (with and without the
+    dense products) to completion: no wait gives up."""
+    a, ldli, plain = graph
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    for prec in ("fp64", "mixed"):
+        kt = dev.time_kernels(prec, reps=2)
+        assert kt["dense_ms"] > 0 and kt["forward_sweep_ms"] > 0 and kt["backward_sweep_ms"] > 0
+        assert kt["launches_per_iteration"] == 12 and kt["forward_launches"] == 3
+        kb = dev.time_kernels_batch(16, prec, reps=2)
+        assert kb["dense_ms"] > 0 and kb["forward_sweep_ms"] > 0 and kb["backward_sweep_ms"] > 0
+        assert kb["launches_per_iteration"] == 12
+    # the solver still solves correctly afterwards
+    b = np.random.default_rng(8).standard_normal(a.shape[0])
+    x = dev(b, tol=1e-8, maxits=2000, precision="mixed")
+    assert O.relres(a, x, b - b.mean()) <= 1e-8 * 1.01
+    kp = plain.time_kernels("fp64", reps=2)
+    assert kp["dense_ms"] == 0 and kp["launches_per_iteration"] == 8
+    dev.close()
