@@ -352,7 +352,7 @@ def _device_solve(dev, b, prec, tol, maxits=MAXITS):
     return x, dev.last_info[0]
 
 
-def run_config1(args):
+def run_grid2_200(args):
     """grid2(200), unit weights, one zero-mean Gaussian RHS, tol 1e-6: FP64 on the
     GPU against the CPU restatement on the same LDLinv."""
     import acgpu
@@ -370,14 +370,14 @@ def run_config1(args):
     xo, ito, rco, _ = orc(b, tol=1e-6, maxits=1000)
     t_cpu = time.perf_counter() - t
     diff = float(np.linalg.norm(O.center(x) - O.center(xo)) / np.linalg.norm(O.center(xo)))
-    print(json.dumps({"workload": "config1 grid2(200) unit weights, tol 1e-6, fp64", "n": a.shape[0],
+    print(json.dumps({"workload": "grid2(200) unit weights, tol 1e-6, fp64", "n": a.shape[0],
                       "gpu_ms": info.solve_ms, "gpu_its": info.iterations, "gpu_relres": O.relres(a, x, b),
                       "cpu_port_ms": t_cpu * 1e3, "cpu_its": ito, "cpu_relres": O.relres(a, xo, b),
                       "x_rel_diff_vs_cpu": diff, "levels": dev.stats()["levels"]}), flush=True)
     dev.close()
 
 
-def run_config3(args):
+def run_matchings_2m(args):
     """Path over a random permutation + 4 random perfect matchings, n = 2M,
     lognormal(0, 2) weights; mixed precision to 1e-8; level count and LDLinv GB/s."""
     import acgpu
@@ -390,7 +390,7 @@ def run_config3(args):
     factor_s = time.perf_counter() - t
     dev = acgpu.DeviceLapSolver(a, ldli)
     b = rhs(n, 12)
-    out = {"workload": "config3 path+4 matchings n=2M lognormal(0,2)", "n": n, "avg_degree": a.nnz / n,
+    out = {"workload": "path+4 matchings n=2M lognormal(0,2)", "n": n, "avg_degree": a.nnz / n,
            "factor_nnz": ldli.nnz, "factor_s": factor_s, "levels": dev.stats()["levels"]}
     for prec in ("mixed", "fp64"):
         for _ in range(2):
@@ -405,7 +405,7 @@ def run_config3(args):
     dev.close()
 
 
-def run_config4a(args):
+def run_grid3_64rhs(args):
     """64 right-hand sides on the 1M weighted 3D grid: FP64 batched vs mixed batched."""
     import torch
     import acgpu
@@ -419,7 +419,7 @@ def run_config4a(args):
         B[c] = torch.from_numpy(rhs(n, 77 + c))
     X = torch.empty_like(B)
     infos = (AcgSolveInfo * k)()
-    out = {"workload": "config4a 64 RHS on grid3(100) log-uniform weights, tol 1e-8", "n": n}
+    out = {"workload": "64 RHS on grid3(100) log-uniform weights, tol 1e-8", "n": n}
     for prec, name in ((0, "fp64"), (1, "mixed")):
         times = []
         for rep in range(3):
@@ -439,7 +439,7 @@ def run_config4a(args):
     dev.close()
 
 
-def run_config4b(args):
+def run_many_graphs(args):
     """256 graphs in one launch: half 2D grids with side uniform in [32, 256],
     half random geometric graphs (n uniform in [1e3, 1e5], mean degree 8,
     weights 1/distance, largest component); one right-hand side each; FP64 to
@@ -478,7 +478,7 @@ def run_config4b(args):
         dev(b, tol=TOL, maxits=MAXITS)
         seq.append(dev.last_info[0].solve_ms)
         dev.close()
-    out = {"workload": f"config4b {len(graphs)} graphs in one launch (2D grids side U[32,256], RGG n U[1e3,1e5]), "
+    out = {"workload": f"{len(graphs)} graphs in one launch (2D grids side U[32,256], RGG n U[1e3,1e5]), "
                        "1 RHS each, tol 1e-8, fp64",
            "n_total": int(sum(a.shape[0] for a in graphs)), "levels_max": st["levels"], "factor_s": factor_s,
            "upload_s": upload_s, "group_ms": 1e3 * min(times), "group_solves_per_s": len(graphs) / min(times),
@@ -561,7 +561,7 @@ def run_serving(args):
             st = server.latency_stats()
             st["true_relres_max"] = worst
             results[label] = st
-    out = {"workload": "config5 serving: Poisson arrivals, graphs from 2D/3D grids, matchings, RGG, "
+    out = {"workload": "serving: Poisson arrivals, graphs from 2D/3D grids, matchings, RGG, "
                        "n log-uniform [1e3,1e6], lognormal(0,1) weights, 1-16 RHS, tol 1e-8",
            "graphs": [(gid, int(a.shape[0])) for gid, a in pool], "requests": nreq,
            "arrival_rate_per_s": args.serving_rate, "factor_s_total": factor_s, **results,
@@ -633,8 +633,8 @@ def main():
     ap.add_argument("--side", type=int, default=GRID_SIDE, help="grid side (100 = the benchmark workload)")
     ap.add_argument("--rhs", type=int, default=64, help="independent right-hand sides per step (batched)")
     ap.add_argument("--workload", default="grid3",
-                    choices=["grid3", "config1", "config3", "config4a", "config4b", "serving"],
-                    help="grid3 = the headline line; the others report the remaining configurations")
+                    choices=["grid3", "grid2_200", "matchings_2m", "grid3_64rhs", "many_graphs", "serving"],
+                    help="grid3 = the headline line; the others report the remaining workloads")
     ap.add_argument("--serving-graphs", type=int, default=16)
     ap.add_argument("--group-graphs", type=int, default=256)
     ap.add_argument("--serving-requests", type=int, default=300)
@@ -651,7 +651,7 @@ def main():
     else:
         import torch
         torch.cuda.init()
-        {"config1": run_config1, "config3": run_config3, "config4a": run_config4a, "config4b": run_config4b,
+        {"grid2_200": run_grid2_200, "matchings_2m": run_matchings_2m, "grid3_64rhs": run_grid3_64rhs, "many_graphs": run_many_graphs,
          "serving": run_serving}[args.workload](args)
 
 

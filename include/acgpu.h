@@ -226,7 +226,7 @@ int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg
  * y_dev = LDLsolver(ldli, r_dev), as acg_ldlsolve computes it, for vectors
  * already in device memory, without allocating: every piece of scratch comes
  * from one fixed device array inside the library (ACG_NOALLOC_MAX_N vertices
- * at most, about 4.1 MB, reserved on each GPU that loads the library until
+ * at most, about 6.4 MB, reserved on each GPU that loads the library until
  * the process exits).  Meant for callers that must not allocate at that
  * moment, e.g. work enqueued while a stream is captured into a CUDA graph, or
  * a serving loop whose device memory is a fixed pool.  The scratch address is

@@ -53,3 +53,28 @@ def test_bad_arguments_are_errors():
     assert rc < 0
     st = np.zeros(4, np.uint64)
     assert L.acg_approxchol(1, z, z, f, st, ctypes.byref(h)) == -1
+
+
+def _header_struct_fields(tag):
+    """Field names, in order, of `typedef struct { ... } tag;` in include/acgpu.h."""
+    text = (ROOT / "include" / "acgpu.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    m = re.search(r"typedef struct\s*\{([^}]*)\}\s*" + tag + r"\s*;", text, flags=re.S)
+    assert m, tag
+    names = []
+    for decl in m.group(1).split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        decl = re.sub(r"^(const\s+)?(unsigned\s+)?[A-Za-z_0-9]+\s+", "", decl)
+        for part in decl.split(","):
+            names.append(re.sub(r"\[.*\]", "", part).strip())
+    return names
+
+
+@pytest.mark.parametrize("tag,cls", [("acg_options", "AcgOptions"), ("acg_stats", "AcgStats"),
+                                     ("acg_solve_info", "AcgSolveInfo"), ("acg_kernel_times", "AcgKernelTimes")])
+def test_binding_structs_match_header(tag, cls):
+    """The ctypes mirrors declare the header's fields in the header's order."""
+    fields = [f[0] for f in getattr(_lib, cls)._fields_]
+    assert fields == _header_struct_fields(tag)

@@ -72,7 +72,7 @@ def test_pcg_fp64_matches_oracle(gpu_ok, name, make):
     assert O.relres(a, x, b - b.mean()) < 1e-7
 
 
-def test_config1_grid2_200(gpu_ok):
+def test_grid2_200_fp64(gpu_ok):
     """grid2(200), one Gaussian RHS, tol 1e-6: GPU vs CPU on the same LDLinv."""
     a = G.grid2(200)
     ldli, dev, orc = _setup(a, seed=1)
