@@ -30,7 +30,7 @@
 
 namespace acg {
 
-constexpr int kDenseRows = 32;
+constexpr int kDenseRows = 64;
 constexpr int kDenseChunk = 256;
 constexpr int kDenseSub = 64;
 constexpr int kDenseThreads = 256;
@@ -50,6 +50,9 @@ __host__ __device__ __forceinline__ bool dense_active(bool fwd, int rt, int kc) 
 
 // part[kc][i][c] = sum over j in chunk kc (inside the triangle) of A[i][j] * src[j][c],
 // A = M (forward) or M^T (backward, src scaled by g); kp = 8 * CPL columns.
+// Register tiling: the 256 threads form RG row groups x CG column groups and
+// each computes RT rows x CT columns of the 64-row tile, so one stage of SUB
+// reduction indices costs RT + CT shared-memory loads per RT * CT FMAs.
 template <typename T, int CPL, bool kFwd>
 __global__ void __launch_bounds__(kDenseThreads) kd_partial(int K, const T* __restrict__ M, const T* __restrict__ src,
                                                             const T* __restrict__ g, T* __restrict__ part,
@@ -58,27 +61,33 @@ __global__ void __launch_bounds__(kDenseThreads) kd_partial(int K, const T* __re
   const int rt = blockIdx.x, kc = blockIdx.y;
   if (!dense_active(kFwd, rt, kc)) return;
   constexpr int kp = 8 * CPL;
-  // reduction indices per shared-memory stage: 64, or 32 for rows of more than 256 bytes
-  constexpr int SUB = (kp * sizeof(T) > 256) ? kDenseSub / 2 : kDenseSub;
-  __shared__ T At[SUB][kDenseRows + 1];  // At[j][i]: the A tile, transposed
+  constexpr int CT = kp >= 32 ? kp / 16 : 1;       // columns per thread
+  constexpr int CG = kp / CT;                      // column groups
+  constexpr int RG = kDenseThreads / CG;           // row groups
+  constexpr int RT = kDenseRows / RG;              // rows per thread
+  constexpr int SUB = 32;                          // reduction indices per stage
+  static_assert(CG * RG == kDenseThreads && RT * RG == kDenseRows, "dense tile shape");
+  __shared__ T As[kDenseRows][SUB + 1];            // A tile, row-major, padded
   __shared__ __align__(16) T Bs[SUB][kp];
   const int tid = threadIdx.x;
-  const int r = tid >> 3, cg = tid & 7;
+  const int rg = tid / CG, cg = tid % CG;
   const int i0 = rt * kDenseRows;
-  T acc[CPL];
+  T acc[RT][CT];
 #pragma unroll
-  for (int q = 0; q < CPL; ++q) acc[q] = T(0);
+  for (int a = 0; a < RT; ++a)
+#pragma unroll
+    for (int b = 0; b < CT; ++b) acc[a][b] = T(0);
   const int jend = min(K, kc * kDenseChunk + kDenseChunk);
   for (int j0 = kc * kDenseChunk; j0 < jend; j0 += SUB) {
     for (int e = tid; e < kDenseRows * SUB; e += kDenseThreads) {
       // forward reads rows of M along j, backward reads rows of M along i:
-      // both coalesced
+      // both coalesced, both conflict-free in shared memory
       const int rr = kFwd ? e / SUB : e % kDenseRows;
       const int jj = kFwd ? e % SUB : e / kDenseRows;
       const int ii = i0 + rr, j = j0 + jj;
       T a = T(0);
       if (ii < K && j < K && (kFwd ? j <= ii : j >= ii)) a = kFwd ? M[(size_t)ii * K + j] : M[(size_t)j * K + ii];
-      At[jj][rr] = a;
+      As[rr][jj] = a;
     }
     for (int e = tid; e < SUB * kp; e += kDenseThreads) {
       const int jj = e / kp, c = e % kp, j = j0 + jj;
@@ -90,18 +99,27 @@ __global__ void __launch_bounds__(kDenseThreads) kd_partial(int K, const T* __re
       Bs[jj][c] = b;
     }
     __syncthreads();
-#pragma unroll 8
+#pragma unroll 4
     for (int jj = 0; jj < SUB; ++jj) {
-      const T a = At[jj][r];
+      T a[RT], b[CT];
 #pragma unroll
-      for (int q = 0; q < CPL; ++q) acc[q] += a * Bs[jj][cg * CPL + q];
+      for (int q = 0; q < RT; ++q) a[q] = As[rg * RT + q][jj];
+#pragma unroll
+      for (int q = 0; q < CT; ++q) b[q] = Bs[jj][cg * CT + q];
+#pragma unroll
+      for (int x = 0; x < RT; ++x)
+#pragma unroll
+        for (int y = 0; y < CT; ++y) acc[x][y] += a[x] * b[y];
     }
     __syncthreads();
   }
-  const int i = i0 + r;
-  if (i < K) {
 #pragma unroll
-    for (int q = 0; q < CPL; ++q) part[((size_t)kc * K + i) * kp + cg * CPL + q] = acc[q];
+  for (int x = 0; x < RT; ++x) {
+    const int i = i0 + rg * RT + x;
+    if (i < K) {
+#pragma unroll
+      for (int y = 0; y < CT; ++y) part[((size_t)kc * K + i) * kp + cg * CT + y] = acc[x][y];
+    }
   }
 }
 
@@ -144,21 +162,24 @@ __global__ void __launch_bounds__(kDenseThreads) kd1_partial(int K, const T* __r
       if (lane == 0 && i < K) part[(size_t)kc * K + i] = acc;
     }
   } else {
-    const int i = i0 + lane;
-    T acc = T(0);
-    if (i < K) {
-      for (int jj = w * 32; jj < w * 32 + 32; ++jj) {
-        const int j = j0 + jj;
-        if (j >= i && j < K) acc += M[(size_t)j * K + i] * Bs[jj];
+    for (int h = 0; h < kDenseRows / 32; ++h) {
+      const int i = i0 + h * 32 + lane;
+      T acc = T(0);
+      if (i < K) {
+        for (int jj = w * 32; jj < w * 32 + 32; ++jj) {
+          const int j = j0 + jj;
+          if (j >= i && j < K) acc += M[(size_t)j * K + i] * Bs[jj];
+        }
       }
-    }
-    red[w][lane] = acc;
-    __syncthreads();
-    if (w == 0) {
-      T sum = T(0);
+      red[w][lane] = acc;
+      __syncthreads();
+      if (w == 0) {
+        T sum = T(0);
 #pragma unroll
-      for (int q = 0; q < kDenseThreads / 32; ++q) sum += red[q][lane];
-      if (i < K) part[(size_t)kc * K + i] = sum;
+        for (int q = 0; q < kDenseThreads / 32; ++q) sum += red[q][lane];
+        if (i < K) part[(size_t)kc * K + i] = sum;
+      }
+      __syncthreads();
     }
   }
 }
