@@ -148,8 +148,8 @@ __device__ __forceinline__ void st_row(double* p, const double (&v)[CPL]) {
 template <typename T, int CPL, bool kForward>
 __global__ void __launch_bounds__(kSweepThreads) kb_sweep(int ntasks, const SweepTask* __restrict__ tasks,
                                                           const int* __restrict__ idx, const T* __restrict__ coef,
-                                                          const T* __restrict__ aux, const T* __restrict__ sfwd,
-                                                          T* out, BatchShared* bs) {
+                                                          const T* __restrict__ aux, const T* sfwd,
+                                                          T* out, T* mark, BatchShared* bs) {
   if (bs->all_done) return;
   constexpr int kp = CPL * kBatchLanes;
   // rows loaded per batch: a whole slot of 8 entries where registers allow
@@ -247,6 +247,15 @@ __global__ void __launch_bounds__(kSweepThreads) kb_sweep(int ntasks, const Swee
 #pragma unroll
       for (int q = 0; q < CPL; ++q) res[q] = a.v[q] + acc[q];
       st_row<CPL>(out + (size_t)e0.v * kp + gl * CPL, res);
+      if (mark) {
+        // the vertex's row of the other sweep's vector is dead from here on
+        // (forward: y, read by no one until the backward rewrites it;
+        // backward: s, whose only reader was this task): mark it pending
+        // for the next sweep instead of a separate pass over the vector
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) res[q] = pending_value<T>();
+        st_row<CPL>(mark + (size_t)e0.v * kp + gl * CPL, res);
+      }
     }
     e0 = e1;
     r1 = r2;
@@ -407,11 +416,11 @@ __global__ void __launch_bounds__(kBVecThreads) kb_pq(int n, int kp, const T* __
   }
 }
 
-// x' = x + alpha p, r -= alpha q (active columns); s, y pending; |r|^2, |x'|_1, |r|_1
+// x' = x + alpha p, r -= alpha q (active columns); |r|^2, |x'|_1, |r|_1.  The
+// sweeps' vectors s and y are marked pending by the sweeps themselves.
 template <typename T>
 __global__ void __launch_bounds__(kBVecThreads) kb_update(int n, int kp, T* x3, const T* __restrict__ p,
-                                                          const T* __restrict__ q, T* __restrict__ r,
-                                                          T* __restrict__ s_out, T* __restrict__ y_out, PcgState* st,
+                                                          const T* __restrict__ q, T* __restrict__ r, PcgState* st,
                                                           BatchShared* bs, double* partials, LoopCtl ctl) {
   if (bs->all_done) return;
   const size_t N = (size_t)n * kp;
@@ -422,16 +431,10 @@ __global__ void __launch_bounds__(kBVecThreads) kb_update(int n, int kp, T* x3, 
   const double al = st[c].alpha;
   const T* xc = x3 + (size_t)st[c].xcur * N;
   T* xn = x3 + (size_t)st[c].xnext * N;
-  const T pend = pending_value<T>();
   double acc[3] = {0.0, 0.0, 0.0};
   size_t i = i0;
+  if (!act) i = N;  // a stopped column keeps its vectors
   for (; i + (kBU - 1) * S < N; i += kBU * S) {
-#pragma unroll
-    for (int u = 0; u < kBU; ++u) {
-      s_out[i + u * S] = pend;
-      y_out[i + u * S] = pend;
-    }
-    if (!act) continue;
     T xv[kBU], pv[kBU], qv[kBU], rv[kBU];
 #pragma unroll
     for (int u = 0; u < kBU; ++u) {
@@ -452,9 +455,6 @@ __global__ void __launch_bounds__(kBVecThreads) kb_update(int n, int kp, T* x3, 
     }
   }
   for (; i < N; i += S) {
-    s_out[i] = pend;
-    y_out[i] = pend;
-    if (!act) continue;
     const T xv = (T)((double)xc[i] + al * (double)p[i]);
     const T rv = (T)((double)r[i] + (-al) * (double)q[i]);
     xn[i] = xv;

@@ -1269,7 +1269,7 @@ void with_cpl(int kp, F&& f) {
 }
 
 template <typename T, int CPL, bool kForward>
-void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sfwd, T* out) {
+void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, T* sfwd, T* out, T* mark) {
   const TypedArrays<T> A = arrays_of<T>(S);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(S.bsweep_blocks[plan_index<T>()][kp_index(CPL * kBatchLanes)]);
@@ -1282,23 +1282,26 @@ void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, const T* 
   cfg.numAttrs = 1;
   ACG_CUDA(cudaLaunchKernelEx(&cfg, kb_sweep<T, CPL, kForward>, kForward ? S.ntasks_fb : S.ntasks_bb,
                               (const SweepTask*)(kForward ? S.tasks_fb.p : S.tasks_bb.p), kForward ? A.fi : A.bi,
-                              kForward ? A.fc : A.bc, aux, sfwd, out, S.bsh));
+                              kForward ? A.fc : A.bc, aux, (const T*)sfwd, out, mark, S.bsh));
 }
 
 // Batched forward (s from r) and backward (y from s) sweeps, dense tail included.
+// The forward sweep marks y pending and the backward sweep marks s pending
+// (head rows; nothing waits on the dense tail's rows), so the next iteration
+// finds both vectors ready to be swept.
 template <typename T, int CPL>
-void enqueue_bforward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv) {
-  enqueue_bsweep<T, CPL, true>(s, S, r, (const T*)nullptr, sv);
+void enqueue_bforward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y) {
+  enqueue_bsweep<T, CPL, true>(s, S, r, (T*)nullptr, sv, y);
   if (S.dt_K) enqueue_dense<T, CPL>(s, S, true, sv, (T*)nullptr, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
 }
 template <typename T, int CPL>
 void enqueue_bbackward(cudaStream_t s, const SolverImpl& S, T* sv, T* y) {
   if (S.dt_K) enqueue_dense<T, CPL>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
-  enqueue_bsweep<T, CPL, false>(s, S, arrays_of<T>(S).g, sv, y);
+  enqueue_bsweep<T, CPL, false>(s, S, arrays_of<T>(S).g, sv, y, sv);
 }
 template <typename T, int CPL>
 void enqueue_bsweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y) {
-  enqueue_bforward<T, CPL>(s, S, r, sv);
+  enqueue_bforward<T, CPL>(s, S, r, sv, y);
   enqueue_bbackward<T, CPL>(s, S, sv, y);
 }
 
@@ -1310,7 +1313,7 @@ void enqueue_biteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* y, 
   const int n = S.n;
   kb_spmv<T, CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, p, q, S.bsh);
   kb_pq<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, ctl);
-  kb_update<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, x3, p, q, r, sv, y, S.bst, S.bsh, S.bpartials.p, ctl);
+  kb_update<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, ctl);
   enqueue_bsweeps<T, CPL>(s, S, r, sv, y);
   kb_ysum<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, y, S.bst, S.bsh, S.bpartials.p, ctl);
   kb_zdot<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, y, r, p, S.bst, S.bsh, S.bpartials.p, eps, 0, ctl);
@@ -1714,16 +1717,27 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
   out->spmv_ms = time_graph([&]() { kb_spmv<T, CPL><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, A.lp, A.li, A.lv, p, q, S.bsh); });
   out->forward_ms = time_graph([&]() {
     fill_s();
-    enqueue_bforward<T, CPL>(s, S, r, sv);
+    enqueue_bforward<T, CPL>(s, S, r, sv, y);
   }) - t_fill;
+  // A backward sweep marks s pending as it consumes it, so each timed backward
+  // starts from a saved copy of the forward output (q is free after the
+  // mat-vec timing); the copy is timed apart and subtracted like the fills.
+  ACG_CUDA(cudaMemcpyAsync(q, sv, sizeof(T) * N, cudaMemcpyDeviceToDevice, s));
+  auto restore_s = [&]() { ACG_CUDA(cudaMemcpyAsync(sv, q, sizeof(T) * N, cudaMemcpyDeviceToDevice, s)); };
+  const double t_restore = time_graph(restore_s);
   out->backward_ms = time_graph([&]() {
+    restore_s();
     fill_y();
     enqueue_bbackward<T, CPL>(s, S, sv, y);
-  }) - t_fill;
+  }) - t_fill - t_restore;
   out->forward_sweep_ms = time_graph([&]() {
     fill_s();
-    enqueue_bsweep<T, CPL, true>(s, S, r, (const T*)nullptr, sv);
+    enqueue_bsweep<T, CPL, true>(s, S, r, (T*)nullptr, sv, y);
   }) - t_fill;
+  // the forward sweeps above marked all of y pending: rewrite the tail's rows
+  // once, which the backward sweep alone reads and never marks
+  if (S.dt_K)
+    enqueue_dense<T, CPL>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
   // the backward sweep alone reads the tail rows the dense product wrote in
   // the backward_ms runs above, so only the head is marked pending
   auto fill_yh = [&]() {
@@ -1731,9 +1745,11 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
   };
   const double t_fill_h = time_graph(fill_yh);
   out->backward_sweep_ms = time_graph([&]() {
+    restore_s();
     fill_yh();
-    enqueue_bsweep<T, CPL, false>(s, S, A.g, sv, y);
-  }) - t_fill_h;
+    enqueue_bsweep<T, CPL, false>(s, S, A.g, sv, y, sv);
+  }) - t_fill_h - t_restore;
+  restore_s();
   out->dense_ms = S.dt_K ? time_graph([&]() {
     enqueue_dense<T, CPL>(s, S, true, sv, (T*)nullptr, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
     enqueue_dense<T, CPL>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
