@@ -102,7 +102,9 @@ typedef struct {
   int dense_tail;            /* largest number of final-level vertices whose substitution
                                 is replaced by a dense triangular product (0 = 4096,
                                 -1 = none; at most 8192 and n/4)                       */
-  int reserved[1];           /* 0 */
+  int sweep_stride;          /* 1 = one value per vertex in the one-vector sweep vectors;
+                                0 = one 32-byte sector per vertex (faster: values that
+                                different SMs write at once never share a sector)     */
 } acg_options;
 
 /* Shape of an uploaded solver. */

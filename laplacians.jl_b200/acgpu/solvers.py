@@ -171,12 +171,11 @@ class DeviceLapSolver:
         self.defaults = dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts,
                              precision=precision)
         opts = AcgOptions()
+        known = {f[0] for f in AcgOptions._fields_}
         for k, v in (options or {}).items():
-            if k == "reserved":
-                for i, x in enumerate(v):
-                    opts.reserved[i] = int(x)
-            else:
-                setattr(opts, k, int(v))
+            if k not in known:
+                raise ValueError(f"unknown solver option {k!r}; known: {sorted(known)}")
+            setattr(opts, k, int(v))
         h = ctypes.c_void_p()
         check(lib().acg_create(self.n, a.indptr.astype(np.int64), a.indices.astype(np.int64),
                                np.ascontiguousarray(a.data), ldli.col, ldli.colptr, ldli.rowval, ldli.fval, ldli.d,

@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kDenseThreads) kd_partial(int K, const T* __re
 template <typename T, bool kFwd>
 __global__ void __launch_bounds__(kDenseThreads) kd1_partial(int K, const T* __restrict__ M, const T* __restrict__ src,
                                                              const T* __restrict__ g, T* __restrict__ part,
-                                                             const int* __restrict__ done) {
+                                                             const int* __restrict__ done, int vs) {
   if (done && *done) return;
   const int rt = blockIdx.x, kc = blockIdx.y;
   if (!dense_active(kFwd, rt, kc)) return;
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kDenseThreads) kd1_partial(int K, const T* __r
     const int j = j0 + jj;
     T b = T(0);
     if (j < K) {
-      b = src[j];
+      b = src[(size_t)j * vs];
       if (!kFwd) b *= g[j];
     }
     Bs[jj] = b;
@@ -184,10 +184,11 @@ __global__ void __launch_bounds__(kDenseThreads) kd1_partial(int K, const T* __r
   }
 }
 
-// dst[i][c] = sum of the partial tiles of row i over its chunks, in chunk order.
+// dst[i * rs + c] = sum of the partial tiles of row i over its chunks, in chunk
+// order (rs: the destination's row stride, kp for batched rows).
 template <typename T, bool kFwd>
 __global__ void __launch_bounds__(kVecThreads) kd_reduce(int K, int kp, const T* __restrict__ part, T* __restrict__ dst,
-                                                         const int* __restrict__ done) {
+                                                         const int* __restrict__ done, int rs) {
   if (done && *done) return;
   const int nch = dense_chunks(K);
   const size_t N = (size_t)K * kp;
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(kVecThreads) kd_reduce(int K, int kp, const T*
     T sum = T(0);
     for (int kc = 0; kc < nch; ++kc)
       if (dense_active(kFwd, rt, kc)) sum += part[(size_t)kc * N + e];
-    dst[e] = sum;
+    dst[(e / kp) * rs + e % kp] = sum;
   }
 }
 

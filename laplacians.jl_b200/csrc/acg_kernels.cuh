@@ -445,7 +445,7 @@ __device__ __forceinline__ SweepTask load_task(const SweepTask* __restrict__ tas
 template <typename T, bool kForward, bool kLoadAux = true>
 __device__ __forceinline__ void load_entries(SweepEntries<T>& e, const SweepTask& r, int lane,
                                              const int* __restrict__ idx, const T* __restrict__ coef,
-                                             const T* __restrict__ aux, const T* __restrict__ sfwd) {
+                                             const T* __restrict__ aux, const T* __restrict__ sfwd, int vs = 1) {
   const bool heavy = r.cnt_heavy & 1;
   const int cnt = r.cnt_heavy >> 1;
   const int sub = heavy ? 0 : (lane >> 3);
@@ -462,7 +462,7 @@ __device__ __forceinline__ void load_entries(SweepEntries<T>& e, const SweepTask
   e.k0 = k0 + gl;
   e.k1 = k1;
   e.a = (kLoadAux && e.active) ? __ldg(&aux[e.v]) : T(0);
-  e.own = (kLoadAux && !kForward && e.active) ? __ldg(&sfwd[e.v]) : T(0);
+  e.own = (kLoadAux && !kForward && e.active) ? __ldg(&sfwd[(size_t)e.v * vs]) : T(0);
 #pragma unroll
   for (int j = 0; j < kEntryUnroll; ++j) {
     const int k = e.k0 + j * gw;
@@ -478,7 +478,7 @@ template <typename T, bool kForward>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const SweepTask* __restrict__ tasks,
                                                          const int* __restrict__ idx, const T* __restrict__ coef,
                                                          const T* __restrict__ aux, const T* __restrict__ sfwd, T* out,
-                                                         PcgState* st, int poll_mode) {
+                                                         PcgState* st, int poll_mode, int vs) {
   if (st->done) return;
   const int lane = threadIdx.x & 31;
   const int W = (int)((gridDim.x * blockDim.x) >> 5);
@@ -487,29 +487,29 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const Sweep
   SweepEntries<T> e0;
   {
     const SweepTask r0 = load_task(tasks, t, ntasks);
-    load_entries<T, kForward>(e0, r0, lane, idx, coef, aux, sfwd);
+    load_entries<T, kForward>(e0, r0, lane, idx, coef, aux, sfwd, vs);
   }
   for (; t < ntasks; t += W) {
     const SweepTask r2 = load_task(tasks, t + 2 * W, ntasks);
     SweepEntries<T> e1;
-    load_entries<T, kForward>(e1, r1, lane, idx, coef, aux, sfwd);
+    load_entries<T, kForward>(e1, r1, lane, idx, coef, aux, sfwd, vs);
     const int gw = e0.gw;  // uniform across the warp: one task per warp
     T acc = T(0);
     // issue the loads of all prefetched entries before checking any of them
     T xv[kEntryUnroll];
 #pragma unroll
-    for (int j = 0; j < kEntryUnroll; ++j) xv[j] = e0.id[j] >= 0 ? ld_relaxed(&out[e0.id[j]]) : T(0);
+    for (int j = 0; j < kEntryUnroll; ++j) xv[j] = e0.id[j] >= 0 ? ld_relaxed(&out[(size_t)e0.id[j] * vs]) : T(0);
 #pragma unroll
     for (int j = 0; j < kEntryUnroll; ++j) {
       if (e0.id[j] < 0) continue;
-      if (is_pending(xv[j])) xv[j] = wait_value_slow(&out[e0.id[j]], st, poll_mode);
+      if (is_pending(xv[j])) xv[j] = wait_value_slow(&out[(size_t)e0.id[j] * vs], st, poll_mode);
       acc += e0.c[j] * xv[j];
     }
     for (int k = e0.k0 + kEntryUnroll * gw; k < e0.k1; k += gw)
-      acc += __ldg(&coef[k]) * wait_value(&out[__ldg(&idx[k])], st, poll_mode);
+      acc += __ldg(&coef[k]) * wait_value(&out[(size_t)__ldg(&idx[k]) * vs], st, poll_mode);
     __syncwarp();  // reconverge after the divergent waits before the shuffles
     acc = group_sum_w(acc, gw);
-    if (e0.active && (lane & (gw - 1)) == 0) st_relaxed(&out[e0.v], kForward ? e0.a + acc : e0.a * e0.own + acc);
+    if (e0.active && (lane & (gw - 1)) == 0) st_relaxed(&out[(size_t)e0.v * vs], kForward ? e0.a + acc : e0.a * e0.own + acc);
     e0 = e1;
     r1 = r2;
   }
@@ -596,11 +596,11 @@ constexpr size_t tail_smem_bytes(int nv, int nl) {
 }
 
 template <typename T>
-__global__ void k_fill_pending(int n, T* a, T* b) {
+__global__ void k_fill_pending(int n, T* a, T* b, int vs = 1) {
   const T pv = pending_value<T>();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    a[i] = pv;
-    if (b) b[i] = pv;
+    a[(size_t)i * vs] = pv;
+    if (b) b[(size_t)i * vs] = pv;
   }
 }
 

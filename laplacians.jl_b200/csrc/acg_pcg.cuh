@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(kVecThreads) k_spmv_pq(int n, const int* __res
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_update(int n, T* x3, const T* __restrict__ p, const T* __restrict__ q,
                                                         T* __restrict__ r, T* __restrict__ s_out, T* __restrict__ y_out,
-                                                        PcgState* st, double* partials, LoopCtl ctl) {
+                                                        PcgState* st, double* partials, LoopCtl ctl, int vs) {
   if (st->done) return;
   const T pend = pending_value<T>();
   const double al = st->alpha;
@@ -169,8 +169,8 @@ __global__ void __launch_bounds__(kVecThreads) k_update(int n, T* x3, const T* _
     const T rv = (T)((double)r[i] + (-al) * (double)q[i]);
     xn[i] = xv;
     r[i] = rv;
-    s_out[i] = pend;
-    y_out[i] = pend;
+    s_out[(size_t)i * vs] = pend;
+    y_out[(size_t)i * vs] = pend;
     acc[0] += (double)rv * (double)rv;
     acc[1] += fabs((double)xv);
     acc[2] += fabs((double)rv);
@@ -181,10 +181,10 @@ __global__ void __launch_bounds__(kVecThreads) k_update(int n, T* x3, const T* _
 
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_ysum(int n, const T* __restrict__ y, PcgState* st, double* partials,
-                                                     LoopCtl ctl) {
+                                                     LoopCtl ctl, int vs) {
   if (st->done) return;
   double acc[1] = {0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] += (double)y[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] += (double)y[(size_t)i * vs];
   if (grid_reduce<1>(acc, partials, &st->counter[2]) && threadIdx.x == 0) {
     st->mean = acc[0] / (double)n;
     if (st->sweep_error) pcg_stop(st, kSweepTimeout, ctl);
@@ -197,13 +197,14 @@ __global__ void __launch_bounds__(kVecThreads) k_ysum(int n, const T* __restrict
 // solve of the refinement loop) keeps the clock started by k_center.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_zdot(int n, T* __restrict__ yz, const T* __restrict__ r, T* __restrict__ p,
-                                                      PcgState* st, double* partials, double eps, int init, LoopCtl ctl) {
+                                                      PcgState* st, double* partials, double eps, int init, LoopCtl ctl,
+                                                      int vs) {
   if (st->done) return;
   const double mu = st->mean;
   double acc[2] = {0.0, 0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const T z = (T)((double)yz[i] - mu);
-    yz[i] = z;
+    const T z = (T)((double)yz[(size_t)i * vs] - mu);
+    yz[(size_t)i * vs] = z;
     if (init) p[i] = z;
     acc[0] += (double)z * (double)r[i];
     acc[1] += fabs((double)z);
@@ -213,11 +214,12 @@ __global__ void __launch_bounds__(kVecThreads) k_zdot(int n, T* __restrict__ yz,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_pupdate(int n, const T* __restrict__ z, T* __restrict__ p, const PcgState* st) {
+__global__ void __launch_bounds__(kVecThreads) k_pupdate(int n, const T* __restrict__ z, T* __restrict__ p, const PcgState* st,
+                                                         int vs) {
   if (st->done) return;
   const double beta = st->beta;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = (T)((double)z[i] + beta * (double)p[i]);
+    p[i] = (T)((double)z[(size_t)i * vs] + beta * (double)p[i]);
 }
 
 // ---- set-up and wrap-up kernels (FP64) ------------------------------------
@@ -238,7 +240,7 @@ __global__ void __launch_bounds__(kVecThreads) k_gather_in(int n, const int* __r
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_center(int n, double* __restrict__ bm, T* __restrict__ r, T* __restrict__ x0,
                                                         T* __restrict__ s_out, T* __restrict__ y_out, PcgState* st,
-                                                        double* partials, LoopCtl ctl) {
+                                                        double* partials, LoopCtl ctl, int vs) {
   const double mu = st->mean;
   const T pend = pending_value<T>();
   double acc[2] = {0.0, 0.0};
@@ -247,8 +249,8 @@ __global__ void __launch_bounds__(kVecThreads) k_center(int n, double* __restric
     bm[i] = v;
     r[i] = (T)v;
     x0[i] = T(0);
-    if (s_out) s_out[i] = pend;
-    if (y_out) y_out[i] = pend;
+    if (s_out) s_out[(size_t)i * vs] = pend;
+    if (y_out) y_out[(size_t)i * vs] = pend;
     acc[0] += v * v;
     acc[1] += fabs(v);
   }
@@ -326,7 +328,7 @@ __global__ void __launch_bounds__(kVecThreads) k_scatter_out(int n, const int* _
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_outer_prep(int n, const double* __restrict__ r64, T* __restrict__ rin,
                                                             T* __restrict__ x0, T* __restrict__ s_out, T* __restrict__ y_out,
-                                                            PcgState* st, double* partials, LoopCtl inner_ctl) {
+                                                            PcgState* st, double* partials, LoopCtl inner_ctl, int vs) {
   const double inv = 1.0 / st->scale;
   const T pend = pending_value<T>();
   double acc[2] = {0.0, 0.0};
@@ -334,8 +336,8 @@ __global__ void __launch_bounds__(kVecThreads) k_outer_prep(int n, const double*
     const T v = (T)(r64[i] * inv);
     rin[i] = v;
     x0[i] = T(0);
-    s_out[i] = pend;
-    y_out[i] = pend;
+    s_out[(size_t)i * vs] = pend;
+    y_out[(size_t)i * vs] = pend;
     acc[0] += (double)v * (double)v;
     acc[1] += fabs((double)v);
   }

@@ -149,6 +149,10 @@ struct SolverImpl {
   // dense tail: vertices [dt_v0, n) (levels >= dt_L0) handled by s_T = M w_T,
   // y_T = M^T (g_T s_T) with M = (I - C_TT)^{-1} (K x K, row-major); K = 0: none
   int dt_K = 0, dt_v0 = 0, dt_L0 = 0;
+  // values per vertex in the one-vector sweep vectors s and y (FP64, FP32):
+  // one 32-byte sector per vertex for the sync-free engine, so values that
+  // different SMs write at nearly the same time never share a sector
+  int vs64 = 1, vs32 = 1;
   DevBuf<double> dt_M64, dt_part;        // dt_part: partial tiles (chunks x K x columns, as T)
   DevBuf<float> dt_M32;
   size_t dt_part_cols = 0;               // columns dt_part holds
@@ -216,6 +220,10 @@ template <typename T>
 constexpr int plan_index() {
   return sizeof(T) == sizeof(double) ? 0 : 1;
 }
+template <typename T>
+int vstride(const SolverImpl& S) {
+  return sizeof(T) == sizeof(double) ? S.vs64 : S.vs32;
+}
 
 // Launch with programmatic stream serialisation (PDL): the kernel's prologue
 // (constant structure loads) overlaps the previous launch in the stream.
@@ -257,7 +265,7 @@ void enqueue_step(cudaStream_t s, const SolverImpl& S, const SweepStep& st_, con
 // One sync-free sweep over tasks [t0, t1) as a cooperative launch (all blocks co-resident).
 template <typename T, bool kForward>
 void enqueue_syncfree(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sfwd, T* out, PcgState* st,
-                      int t0, int t1) {
+                      int t0, int t1, int vs) {
   if (t1 <= t0) return;
   const TypedArrays<T> A = arrays_of<T>(S);
   cudaLaunchConfig_t cfg = {};
@@ -271,7 +279,7 @@ void enqueue_syncfree(cudaStream_t s, const SolverImpl& S, const T* aux, const T
   cfg.numAttrs = 1;
   const SweepTask* tasks = (kForward ? S.tasks_f.p : S.tasks_b.p) + t0;
   ACG_CUDA(cudaLaunchKernelEx(&cfg, k_sweep<T, kForward>, t1 - t0, tasks, kForward ? A.fi : A.bi,
-                              kForward ? A.fc : A.bc, aux, sfwd, out, st, S.poll_mode));
+                              kForward ? A.fc : A.bc, aux, sfwd, out, st, S.poll_mode, vs));
 }
 
 // The narrow tail of the DAG in one CTA.
@@ -288,40 +296,45 @@ void enqueue_tail(cudaStream_t s, const SolverImpl& S, const T* aux, const T* sf
 // forward s_T = M w_T in place in sv; backward y_T = M^T (g_T s_T).  part
 // holds the partial tiles; done (device) ends the step early when set.
 template <typename T, int CPL>
-void enqueue_dense(cudaStream_t s, const SolverImpl& S, bool fwd, T* sv, T* y, T* part, const int* done) {
+void enqueue_dense(cudaStream_t s, const SolverImpl& S, bool fwd, T* sv, T* y, T* part, const int* done,
+                   int vs = 1) {
   constexpr int kp = CPL == 0 ? 1 : 8 * CPL;
   const int K = S.dt_K;
   const TypedArrays<T> A = arrays_of<T>(S);
-  const size_t off = (size_t)S.dt_v0 * kp;
+  const int rs = CPL == 0 ? vs : kp;  // row stride of sv and y
+  const size_t off = (size_t)S.dt_v0 * rs;
   const dim3 grid(dense_row_tiles(K), dense_chunks(K));
   const T* g = A.g + S.dt_v0;
   if constexpr (CPL == 0) {
-    if (fwd) kd1_partial<T, true><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done);
-    else kd1_partial<T, false><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done);
+    if (fwd) kd1_partial<T, true><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done, vs);
+    else kd1_partial<T, false><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done, vs);
   } else {
     if (fwd) kd_partial<T, CPL, true><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done);
     else kd_partial<T, CPL, false><<<grid, kDenseThreads, 0, s>>>(K, A.dm, sv + off, g, part, done);
   }
   ACG_CUDA(cudaGetLastError());
   const int rb = (int)std::min<long long>(kVecBlocks, ((long long)K * kp + kVecThreads - 1) / kVecThreads);
-  if (fwd) kd_reduce<T, true><<<rb, kVecThreads, 0, s>>>(K, kp, part, sv + off, done);
-  else kd_reduce<T, false><<<rb, kVecThreads, 0, s>>>(K, kp, part, y + off, done);
+  if (fwd) kd_reduce<T, true><<<rb, kVecThreads, 0, s>>>(K, kp, part, sv + off, done, rs);
+  else kd_reduce<T, false><<<rb, kVecThreads, 0, s>>>(K, kp, part, y + off, done, rs);
 }
 
 // Forward sweep: s = forward values of r (s must be pending in sync-free mode).
-// part: partial tiles of the dense tail (null: the solver's own buffer).
+// part: partial tiles of the dense tail (null: the solver's own buffer); vs:
+// values per vertex in sv and y (-1: the solver's own layout, vstride<T>).
 template <typename T>
 void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, PcgState* st, T* part = nullptr,
-                     bool dense = true) {
+                     bool dense = true, int vs = -1) {
+  if (vs < 0) vs = vstride<T>(S);
   if (S.sweep_mode == 0) {
     if (S.tail_nl > 0) {
-      enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.tail_tf0);
+      enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.tail_tf0, vs);
       enqueue_tail<T, true>(s, S, r, (const T*)nullptr, sv, st);
     } else {
-      enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.ntasks_f);
+      enqueue_syncfree<T, true>(s, S, r, (const T*)nullptr, sv, st, 0, S.ntasks_f, vs);
     }
     if (S.dt_K && dense)
-      enqueue_dense<T, 0>(s, S, true, sv, (T*)nullptr, part ? part : reinterpret_cast<T*>(S.dt_part.p), &st->done);
+      enqueue_dense<T, 0>(s, S, true, sv, (T*)nullptr, part ? part : reinterpret_cast<T*>(S.dt_part.p), &st->done,
+                          vs);
     return;
   }
   for (const SweepStep& step : S.plan[plan_index<T>()]) enqueue_step<T, true>(s, S, step, r, (const T*)nullptr, sv, st);
@@ -329,17 +342,18 @@ void enqueue_forward(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, Pcg
 // Backward sweep: y from the forward values s (y pending in sync-free mode).
 template <typename T>
 void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, PcgState* st, T* part = nullptr,
-                      bool dense = true) {
+                      bool dense = true, int vs = -1) {
+  if (vs < 0) vs = vstride<T>(S);
   const T* g = arrays_of<T>(S).g;
   if (S.sweep_mode == 0) {
     if (S.dt_K && dense)
       enqueue_dense<T, 0>(s, S, false, const_cast<T*>(sv), y, part ? part : reinterpret_cast<T*>(S.dt_part.p),
-                          &st->done);
+                          &st->done, vs);
     if (S.tail_nl > 0) {
       enqueue_tail<T, false>(s, S, g, sv, y, st);
-      enqueue_syncfree<T, false>(s, S, g, sv, y, st, S.tail_tb0, S.ntasks_b);
+      enqueue_syncfree<T, false>(s, S, g, sv, y, st, S.tail_tb0, S.ntasks_b, vs);
     } else {
-      enqueue_syncfree<T, false>(s, S, g, sv, y, st, 0, S.ntasks_b);
+      enqueue_syncfree<T, false>(s, S, g, sv, y, st, 0, S.ntasks_b, vs);
     }
     return;
   }
@@ -348,9 +362,10 @@ void enqueue_backward(cudaStream_t s, const SolverImpl& S, const T* sv, T* y, Pc
 }
 // y = LDLinv sweeps of r (without the final mean removal); sv is scratch.
 template <typename T>
-void enqueue_sweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y, PcgState* st, T* part = nullptr) {
-  enqueue_forward<T>(s, S, r, sv, st, part);
-  enqueue_backward<T>(s, S, sv, y, st, part);
+void enqueue_sweeps(cudaStream_t s, const SolverImpl& S, const T* r, T* sv, T* y, PcgState* st, T* part = nullptr,
+                    int vs = -1) {
+  enqueue_forward<T>(s, S, r, sv, st, part, true, vs);
+  enqueue_backward<T>(s, S, sv, y, st, part, true, vs);
 }
 
 template <typename T, int VL>
@@ -370,11 +385,12 @@ void enqueue_pcg_iteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* 
                            LoopCtl ctl) {
   const TypedArrays<T> A = arrays_of<T>(S);
   ACG_VL_SWITCH(S.vl_spmv, spmv_pq_vl, s, S, A, p, q, S.st, eps, ctl);
-  k_update<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, x3, p, q, r, sv, y, S.st, S.partials.p, ctl);
+  const int vs = vstride<T>(S);
+  k_update<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, x3, p, q, r, sv, y, S.st, S.partials.p, ctl, vs);
   enqueue_sweeps<T>(s, S, r, sv, y, S.st);
-  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, ctl);
-  k_zdot<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, r, p, S.st, S.partials.p, eps, 0, ctl);
-  k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, p, S.st);
+  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, ctl, vs);
+  k_zdot<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, r, p, S.st, S.partials.p, eps, 0, ctl, vs);
+  k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, p, S.st, vs);
 }
 
 // ---- graph construction -----------------------------------------------------
@@ -423,10 +439,11 @@ cudaGraphExec_t build_fp64_graph(SolverImpl& S) {
   begin_into(s, top, {});
   k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
   k_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, S.r64.p, S.x3_64.p, S.s64.p, S.y64.p, S.st,
-                                                      S.partials.p, ctl);
+                                                      S.partials.p, ctl, S.vs64);
   enqueue_sweeps<double>(s, S, S.r64.p, S.s64.p, S.y64.p, S.st);
-  k_ysum<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.st, S.partials.p, ctl);
-  k_zdot<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.r64.p, S.p64.p, S.st, S.partials.p, kEps64, 1, ctl);
+  k_ysum<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.st, S.partials.p, ctl, S.vs64);
+  k_zdot<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y64.p, S.r64.p, S.p64.p, S.st, S.partials.p, kEps64, 1, ctl,
+                                                   S.vs64);
   std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
   end_into(s);
 
@@ -466,7 +483,7 @@ cudaGraphExec_t build_mixed_graph(SolverImpl& S) {
   k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
   // r64 = bm, x64 (xf) = 0
   k_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, S.r64.p, S.xf.p, (double*)nullptr,
-                                                      (double*)nullptr, S.st, S.partials.p, octl);
+                                                      (double*)nullptr, S.st, S.partials.p, octl, 1);
   std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
   end_into(s);
 
@@ -478,10 +495,11 @@ cudaGraphExec_t build_mixed_graph(SolverImpl& S) {
 
   begin_into(s, obody, {});
   k_outer_prep<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.r64.p, S.r32.p, S.x3_32.p, S.s32.p, S.y32.p, S.st,
-                                                         S.partials.p, ictl);
+                                                         S.partials.p, ictl, S.vs32);
   enqueue_sweeps<float>(s, S, S.r32.p, S.s32.p, S.y32.p, S.st);
-  k_ysum<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.st, S.partials.p, ictl);
-  k_zdot<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.r32.p, S.p32.p, S.st, S.partials.p, eps32, 2, ictl);
+  k_ysum<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.st, S.partials.p, ictl, S.vs32);
+  k_zdot<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.y32.p, S.r32.p, S.p32.p, S.st, S.partials.p, eps32, 2, ictl,
+                                                  S.vs32);
   std::vector<cudaGraphNode_t> ol = capture_leaves(s);
   end_into(s);
 
@@ -978,9 +996,16 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     S.dt_part_cols = kMaxBatch;
     S.dt_part.alloc((size_t)dense_chunks(S.dt_K) * S.dt_K * kMaxBatch);
   }
-  for (DevBuf<double>* b : {&S.b_ext, &S.x_ext, &S.bm, &S.r64, &S.s64, &S.y64, &S.p64, &S.q64, &S.xf}) b->alloc(n);
+  // one 32-byte sector per vertex in the sweep vectors of the sync-free engine
+  // on one graph (the other engines and the group solver index them densely)
+  const bool pad = S.sweep_mode == 0 && S.tail_nl == 0 && nseg == 1 && !(opts && opts->sweep_stride == 1);
+  S.vs64 = pad ? 32 / (int)sizeof(double) : 1;
+  S.vs32 = pad ? 32 / (int)sizeof(float) : 1;
+  for (DevBuf<double>* b : {&S.b_ext, &S.x_ext, &S.bm, &S.r64, &S.p64, &S.q64, &S.xf}) b->alloc(n);
+  for (DevBuf<double>* b : {&S.s64, &S.y64}) b->alloc((size_t)n * S.vs64);
   S.x3_64.alloc((size_t)3 * n);
-  for (DevBuf<float>* b : {&S.r32, &S.s32, &S.y32, &S.p32, &S.q32}) b->alloc(n);
+  for (DevBuf<float>* b : {&S.r32, &S.p32, &S.q32}) b->alloc(n);
+  for (DevBuf<float>* b : {&S.s32, &S.y32}) b->alloc((size_t)n * S.vs32);
   S.x3_32.alloc((size_t)3 * n);
   S.partials.alloc((size_t)4 * kMaxPartialBlocks);
   ACG_CUDA(cudaMalloc(&S.st, sizeof(PcgState)));
@@ -1021,9 +1046,10 @@ __global__ void k_cast_from64(int n, const double* __restrict__ a, T* __restrict
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (T)a[i];
 }
 template <typename T>
-__global__ void k_minus_mean(int n, const T* __restrict__ y, const PcgState* st, double* __restrict__ out) {
+__global__ void k_minus_mean(int n, const T* __restrict__ y, const PcgState* st, double* __restrict__ out, int vs) {
   const double mu = st->mean;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (double)y[i] - mu;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = (double)y[(size_t)i * vs] - mu;
 }
 template <typename T, int VL>
 __global__ void __launch_bounds__(kVecThreads) k_spmv_plain(int n, const int* __restrict__ ptr, const int* __restrict__ idx,
@@ -1056,10 +1082,11 @@ void ldlsolve_impl(SolverImpl& S, T* rbuf, T* sbuf, T* ybuf) {
   LoopCtl none{0, 0};
   k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.b_ext.p, S.bm.p, S.st, S.partials.p);
   k_cast_from64<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.bm.p, rbuf);
-  k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, sbuf, ybuf);
+  const int vs = vstride<T>(S);
+  k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, sbuf, ybuf, vs);
   enqueue_sweeps<T>(s, S, rbuf, sbuf, ybuf, S.st);
-  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.partials.p, none);
-  k_minus_mean<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.xf.p);
+  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.partials.p, none, vs);
+  k_minus_mean<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, ybuf, S.st, S.xf.p, vs);
   k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
 }
 
@@ -1117,10 +1144,11 @@ void ldlsolve_noalloc_impl(const SolverImpl& S, cudaStream_t s, const double* r_
   ACG_CUDA(cudaMemsetAsync(st, 0, sizeof(PcgState), s));
   k_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, r_ext, r64, st, partials);
   k_cast_from64<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, r64, rT);
-  k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, sv, yv);
-  enqueue_sweeps<T>(s, S, rT, sv, yv, st, dense_part);
-  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, yv, st, partials, none);
-  k_minus_mean<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, yv, st, r64);
+  // compact vectors (one value per vertex): the fixed array holds n values each
+  k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, sv, yv, 1);
+  enqueue_sweeps<T>(s, S, rT, sv, yv, st, dense_part, 1);
+  k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, yv, st, partials, none, 1);
+  k_minus_mean<T><<<kVecBlocks, kVecThreads, 0, s>>>(n, yv, st, r64, 1);
   k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, r64, y_ext);
 }
 
@@ -1177,8 +1205,9 @@ void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv,
     cudaGraphDestroy(g);
     return (double)ms / reps;
   };
-  auto fill_s = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, sv, (T*)nullptr); };
-  auto fill_y = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, (T*)nullptr); };
+  const int vs = vstride<T>(S);
+  auto fill_s = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, sv, (T*)nullptr, vs); };
+  auto fill_y = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, (T*)nullptr, vs); };
   const double t_fill = time_graph(fill_s);
   out->spmv_ms = time_graph([&]() { ACG_VL_SWITCH(S.vl_spmv, spmv_plain_vl, s, S, A, p, S.xf.p); });
   out->forward_ms = time_graph([&]() {
@@ -1192,11 +1221,11 @@ void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv,
   out->iteration_ms = time_graph([&]() {
     // the kernels of one PCG iteration without the stop logic taking effect
     ACG_VL_SWITCH(S.vl_spmv, spmv_plain_vl, s, S, A, p, S.xf.p);
-    k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, sv, y);
+    k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, sv, y, vs);
     enqueue_sweeps<T>(s, S, r, sv, y, S.st);
-    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, none);
-    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, none);
-    k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, q, S.st);
+    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, none, vs);
+    k_ysum<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, S.st, S.partials.p, none, vs);
+    k_pupdate<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, y, q, S.st, vs);
   });
   out->forward_sweep_ms = time_graph([&]() {
     fill_s();
@@ -1205,7 +1234,7 @@ void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv,
   // the backward sweep alone reads the tail values the dense product wrote in
   // the backward_ms runs above, so only the head is marked pending
   auto fill_yh = [&]() {
-    k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.dt_K ? S.dt_v0 : S.n, y, (T*)nullptr);
+    k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>(S.dt_K ? S.dt_v0 : S.n, y, (T*)nullptr, vs);
   };
   const double t_fill_h = time_graph(fill_yh);
   out->backward_sweep_ms = time_graph([&]() {
@@ -1213,8 +1242,8 @@ void time_kernels_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv,
     enqueue_backward<T>(s, S, sv, y, S.st, (T*)nullptr, false);
   }) - t_fill_h;
   out->dense_ms = S.dt_K ? time_graph([&]() {
-    enqueue_dense<T, 0>(s, S, true, sv, (T*)nullptr, reinterpret_cast<T*>(S.dt_part.p), &S.st->done);
-    enqueue_dense<T, 0>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.st->done);
+    enqueue_dense<T, 0>(s, S, true, sv, (T*)nullptr, reinterpret_cast<T*>(S.dt_part.p), &S.st->done, vs);
+    enqueue_dense<T, 0>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.st->done, vs);
   }) : 0.0;
   const double vb = sizeof(T), nv = S.n;
   // mat-vec: row pointers, (index, value) per entry, x once, y (FP64) out

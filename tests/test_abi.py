@@ -78,3 +78,14 @@ def test_binding_structs_match_header(tag, cls):
     """The ctypes mirrors declare the header's fields in the header's order."""
     fields = [f[0] for f in getattr(_lib, cls)._fields_]
     assert fields == _header_struct_fields(tag)
+
+
+def test_unknown_solver_option_is_rejected():
+    """A misspelled tuning knob raises instead of being silently ignored (no device needed)."""
+    import acgpu
+    from acgpu import generators as G
+    a = G.grid2(4)
+    acgpu.seed(1)
+    ldli = acgpu.approx_chol(a)
+    with pytest.raises(ValueError, match="unknown solver option"):
+        acgpu.DeviceLapSolver(a, ldli, options=dict(dense_tial=0))

@@ -150,3 +150,24 @@ def test_repeatable_bitwise(gpu_ok):
     m1 = dev(b, tol=1e-9, precision="mixed")
     m2 = dev(b, tol=1e-9, precision="mixed")
     assert np.array_equal(m1, m2)
+
+
+@pytest.mark.parametrize("name,make", GRAPHS[:5], ids=[g[0] for g in GRAPHS[:5]])
+def test_sweep_vector_layout_is_invisible(gpu_ok, name, make):
+    """One 32-byte sector per vertex in the sweep vectors (the default) and one
+    value per vertex (sweep_stride=1) run the same arithmetic in the same
+    order: LDLsolver and whole solves agree bit for bit."""
+    a = make()
+    acgpu.seed(1)
+    ldli = acgpu.approx_chol(a)
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    compact = acgpu.DeviceLapSolver(a, ldli, options=dict(sweep_stride=1))
+    rng = np.random.default_rng(3)
+    r = rng.standard_normal(a.shape[0])
+    r -= r.mean()
+    for prec in ("fp64", "mixed"):
+        assert np.array_equal(dev.ldlsolve(r, prec), compact.ldlsolve(r, prec))
+        assert np.array_equal(dev(r, tol=1e-9, maxits=300, precision=prec),
+                              compact(r, tol=1e-9, maxits=300, precision=prec))
+    dev.close()
+    compact.close()
