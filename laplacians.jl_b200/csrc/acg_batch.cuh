@@ -264,6 +264,35 @@ __global__ void __launch_bounds__(kSweepThreads) kb_sweep(int ntasks, const Swee
 
 // ---- batched mat-vec: q = L p for kp columns -------------------------------
 
+// A lane's slice of a row through the read-only path (p does not change
+// during the mat-vec), in 16-byte pieces where the slice allows.
+template <typename T, int CPL>
+__device__ __forceinline__ void ldg_row(T (&v)[CPL], const T* src) {
+  if constexpr (sizeof(T) == 4 && CPL % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < CPL / 4; ++q) {
+      const float4 x = __ldg(reinterpret_cast<const float4*>(src) + q);
+      v[4 * q] = x.x;
+      v[4 * q + 1] = x.y;
+      v[4 * q + 2] = x.z;
+      v[4 * q + 3] = x.w;
+    }
+  } else if constexpr (sizeof(T) == 8 && CPL % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < CPL / 2; ++q) {
+      const double2 x = __ldg(reinterpret_cast<const double2*>(src) + q);
+      v[2 * q] = x.x;
+      v[2 * q + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) v[q] = __ldg(src + q);
+  }
+}
+
+// One row per group of 8 lanes.  The group's lanes load up to 8 of the row's
+// entries at once, share them with shuffles inside the group, and issue every
+// gathered row before the first multiply-add; entries are summed in row order.
 template <typename T, int CPL>
 __global__ void __launch_bounds__(kVecThreads) kb_spmv(int n, const int* __restrict__ ptr, const int* __restrict__ idx,
                                                        const T* __restrict__ val, const T* __restrict__ p,
@@ -272,18 +301,40 @@ __global__ void __launch_bounds__(kVecThreads) kb_spmv(int n, const int* __restr
   constexpr int kp = CPL * kBatchLanes;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int gl = gt & 7;
+  const unsigned gmask = 0xffu << (threadIdx.x & 24);  // this group's lanes
   const int groups = gridDim.x * blockDim.x / 8;
-  for (int row = gt / 8; row < n; row += groups) {
-    const int k0 = __ldg(&ptr[row]), k1 = __ldg(&ptr[row + 1]);
+  int row = gt / 8;
+  int n0 = row < n ? __ldg(&ptr[row]) : 0, n1 = row < n ? __ldg(&ptr[row + 1]) : 0;
+  for (; row < n; row += groups) {
+    const int k0 = n0, k1 = n1;
+    // the group's next row: its extent is loaded while this row is summed
+    const int nxt = row + groups;
+    n0 = nxt < n ? __ldg(&ptr[nxt]) : 0;
+    n1 = nxt < n ? __ldg(&ptr[nxt + 1]) : 0;
     T acc[CPL];
 #pragma unroll
     for (int j = 0; j < CPL; ++j) acc[j] = T(0);
-    for (int k = k0; k < k1; ++k) {
-      const int id = __ldg(&idx[k]);
-      const T c = __ldg(&val[k]);
-      const T* pr = p + (size_t)id * kp + gl * CPL;
+    for (int kb = k0; kb < k1; kb += 8) {
+      const int k = kb + gl;
+      const int myid = k < k1 ? __ldg(&idx[k]) : -1;
+      const T myc = k < k1 ? __ldg(&val[k]) : T(0);
+      int ids[8];
+      T cs[8];
+      T v[8][CPL];
 #pragma unroll
-      for (int j = 0; j < CPL; ++j) acc[j] += c * pr[j];
+      for (int u = 0; u < 8; ++u) {
+        ids[u] = __shfl_sync(gmask, myid, u, 8);
+        cs[u] = __shfl_sync(gmask, myc, u, 8);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (ids[u] >= 0) ldg_row<T, CPL>(v[u], p + (size_t)ids[u] * kp + gl * CPL);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (ids[u] >= 0) {
+#pragma unroll
+          for (int j = 0; j < CPL; ++j) acc[j] += cs[u] * v[u][j];
+        }
     }
     T* qr = q + (size_t)row * kp + gl * CPL;
 #pragma unroll

@@ -145,6 +145,7 @@ struct SolverImpl {
   BatchShared* bsh = nullptr;
   PcgState* h_bst = nullptr;
   int bsweep_blocks[2][4] = {};          // [precision][log2(kp/8)]
+  int bspmv_blocks[2][4] = {};           // batched mat-vec grid: every resident block
   int batch_bps = 0;                     // batched sweep blocks per SM (0 = occupancy limit)
   // dense tail: vertices [dt_v0, n) (levels >= dt_L0) handled by s_T = M w_T,
   // y_T = M^T (g_T s_T) with M = (I - C_TT)^{-1} (K x K, row-major); K = 0: none
@@ -1340,7 +1341,7 @@ void enqueue_biteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* y, 
   constexpr int kp = CPL * kBatchLanes;
   const TypedArrays<T> A = arrays_of<T>(S);
   const int n = S.n;
-  kb_spmv<T, CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, p, q, S.bsh);
+  kb_spmv<T, CPL><<<S.bspmv_blocks[plan_index<T>()][kp_index(kp)], kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, p, q, S.bsh);
   kb_pq<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, ctl);
   kb_update<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, ctl);
   enqueue_bsweeps<T, CPL>(s, S, r, sv, y);
@@ -1452,6 +1453,13 @@ int batch_occupancy(int sms, int cap) {
   return sms * std::max(1, m);
 }
 
+template <typename T, int CPL>
+int spmv_occupancy(int sms) {
+  int a = 0;
+  ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kb_spmv<T, CPL>, kVecThreads, 0));
+  return sms * std::max(1, a);
+}
+
 void ensure_batch(SolverImpl& S, int kp) {
   if (!S.bst) {
     ACG_CUDA(cudaMalloc(&S.bst, sizeof(PcgState) * kMaxBatch));
@@ -1469,6 +1477,14 @@ void ensure_batch(SolverImpl& S, int kp) {
     S.bsweep_blocks[1][1] = batch_occupancy<float, 2>(sms, S.batch_bps);
     S.bsweep_blocks[1][2] = batch_occupancy<float, 4>(sms, S.batch_bps);
     S.bsweep_blocks[1][3] = batch_occupancy<float, 8>(sms, S.batch_bps);
+    S.bspmv_blocks[0][0] = spmv_occupancy<double, 1>(sms);
+    S.bspmv_blocks[0][1] = spmv_occupancy<double, 2>(sms);
+    S.bspmv_blocks[0][2] = spmv_occupancy<double, 4>(sms);
+    S.bspmv_blocks[0][3] = spmv_occupancy<double, 8>(sms);
+    S.bspmv_blocks[1][0] = spmv_occupancy<float, 1>(sms);
+    S.bspmv_blocks[1][1] = spmv_occupancy<float, 2>(sms);
+    S.bspmv_blocks[1][2] = spmv_occupancy<float, 4>(sms);
+    S.bspmv_blocks[1][3] = spmv_occupancy<float, 8>(sms);
   }
   if (kp <= S.batch_kp) return;
   // growing the buffers invalidates every captured batch graph
@@ -1743,7 +1759,10 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
   auto fill_s = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)N, sv, (T*)nullptr); };
   auto fill_y = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)N, y, (T*)nullptr); };
   const double t_fill = time_graph(fill_s);
-  out->spmv_ms = time_graph([&]() { kb_spmv<T, CPL><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, A.lp, A.li, A.lv, p, q, S.bsh); });
+  out->spmv_ms = time_graph([&]() {
+    kb_spmv<T, CPL><<<S.bspmv_blocks[plan_index<T>()][kp_index(kp)], kVecThreads, 0, s>>>(S.n, A.lp, A.li, A.lv, p, q,
+                                                                                       S.bsh);
+  });
   out->forward_ms = time_graph([&]() {
     fill_s();
     enqueue_bforward<T, CPL>(s, S, r, sv, y);
