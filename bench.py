@@ -405,6 +405,39 @@ def run_matchings_2m(args):
     dev.close()
 
 
+def run_orderings(args):
+    """The four elimination orders of approxchol_lap (:deg, :given, :wdeg,
+    :random; src/approxChol.jl:1628-1789) on grid3(50) with log-uniform weights:
+    factor size, DAG depth (what bounds the sweeps), factor and solve time."""
+    import acgpu
+    from acgpu import generators as G
+    side = 50
+    a = G.grid3(side, weights="loguniform", seed=7)
+    n = a.shape[0]
+    b = rhs(n, 13)
+    out = {"workload": f"elimination orders on grid3({side}) log-uniform weights, tol 1e-8", "n": n}
+    for order in ("deg", "wdeg", "random", "given"):
+        params = acgpu.ApproxCholParams(order=order)
+        acgpu.seed(FACTOR_SEED)
+        t = time.perf_counter()
+        ldli = acgpu.approx_chol(a, params)
+        factor_s = time.perf_counter() - t
+        dev = acgpu.DeviceLapSolver(a, ldli, params=params)
+        st = dev.stats()
+        row = {"factor_s": factor_s, "factor_nnz": ldli.nnz, "levels": st["levels"],
+               "dense_tail_levels": st["dense_levels"]}
+        # the given order's DAG is far deeper (the slowest solve, as the
+        # reference documents): one mixed solve of it is enough
+        for prec in (("mixed",) if order == "given" else ("mixed", "fp64")):
+            for _ in range(1 if order == "given" else 2):
+                x, info = _device_solve(dev, b, prec, TOL)
+            row[prec] = {"solve_ms": info.solve_ms, "its": info.iterations, "refinements": info.refinements,
+                         "true_relres": info.true_relres, "status": info.status}
+        out[order] = row
+        dev.close()
+    print(json.dumps(out), flush=True)
+
+
 def run_grid3_64rhs(args):
     """64 right-hand sides on the 1M weighted 3D grid: FP64 batched vs mixed batched."""
     import torch
@@ -633,7 +666,7 @@ def main():
     ap.add_argument("--side", type=int, default=GRID_SIDE, help="grid side (100 = the benchmark workload)")
     ap.add_argument("--rhs", type=int, default=64, help="independent right-hand sides per step (batched)")
     ap.add_argument("--workload", default="grid3",
-                    choices=["grid3", "grid2_200", "matchings_2m", "grid3_64rhs", "many_graphs", "serving"],
+                    choices=["grid3", "grid2_200", "matchings_2m", "grid3_64rhs", "many_graphs", "serving", "orderings"],
                     help="grid3 = the headline line; the others report the remaining workloads")
     ap.add_argument("--serving-graphs", type=int, default=16)
     ap.add_argument("--group-graphs", type=int, default=256)
@@ -651,7 +684,7 @@ def main():
     else:
         import torch
         torch.cuda.init()
-        {"grid2_200": run_grid2_200, "matchings_2m": run_matchings_2m, "grid3_64rhs": run_grid3_64rhs, "many_graphs": run_many_graphs,
+        {"orderings": run_orderings, "grid2_200": run_grid2_200, "matchings_2m": run_matchings_2m, "grid3_64rhs": run_grid3_64rhs, "many_graphs": run_many_graphs,
          "serving": run_serving}[args.workload](args)
 
 

@@ -68,6 +68,13 @@ typedef struct acg_factor acg_factor;
  * advances it.  On success *out owns the factor (free with acg_factor_free). */
 int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval,
                    const double* nzval, uint64_t rng_state[4], acg_factor** out);
+/* approxChol in a fixed elimination order (src/approxChol.jl:758-862 on
+ * LLMatOrd, src/approxChol.jl:203-229 and 265-294): perm (1-based, length n,
+ * perm[k] = the vertex eliminated k-th) or NULL for the given order 1..n; the
+ * factor comes back in the original vertex ids, as approxchol_lapGiven /
+ * approxchol_lapWdeg / approxchol_lapRandom build it (src/approxChol.jl:1628-1789). */
+int acg_approxchol_ordered(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                           const int64_t* perm, uint64_t rng_state[4], acg_factor** out);
 /* n and F = length(ldli.fval). */
 int acg_factor_dims(const acg_factor* f, int64_t* n, int64_t* nnz);
 /* Copy out the LDLinv arrays in the reference layout (src/approxCholTypes.jl:73-79),

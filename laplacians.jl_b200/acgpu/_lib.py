@@ -67,6 +67,8 @@ SIGNATURES = [
     ("acg_rng_rand", ctypes.c_int, [u64p, f64p, ctypes.c_int64]),
     ("acg_sha256", ctypes.c_int, [u8p, ctypes.c_int64, u8p]),
     ("acg_approxchol", ctypes.c_int, [ctypes.c_int64, i64p, i64p, f64p, u64p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("acg_approxchol_ordered", ctypes.c_int, [ctypes.c_int64, i64p, i64p, f64p, ctypes.c_void_p, u64p,
+                                               ctypes.POINTER(ctypes.c_void_p)]),
     ("acg_factor_dims", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     ("acg_factor_export", ctypes.c_int, [ctypes.c_void_p, i64p, i64p, i64p, f64p, f64p]),
     ("acg_factor_free", None, [ctypes.c_void_p]),

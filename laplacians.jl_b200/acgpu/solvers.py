@@ -103,16 +103,60 @@ def lap(a) -> sp.csc_matrix:
     return _csc(sp.diags(np.asarray(a.sum(axis=1)).ravel()) - a)
 
 
-def approx_chol(a) -> LDLinv:
-    """`approxChol(LLmatp(a))` with the :deg order, drawing from the global
-    stream (src/approxChol.jl:864-977).  Runs on the host."""
+def rand(k: int) -> np.ndarray:
+    """k draws of Julia's scalar `rand()` from the global stream (one at a time,
+    in order; Julia's bulk `rand(k)` fills arrays by another method)."""
+    out = np.empty(int(k), dtype=np.float64)
+    if k > 0:
+        check(lib().acg_rng_rand(_RNG, out, int(k)))
+    return out
+
+
+def elimination_order(a, order: str):
+    """The vertex order (1-based; None = the given order 1..n) that the
+    reference's fixed-order solvers eliminate in:
+      "given"  approxchol_lapGiven   (src/approxChol.jl:1628-1677): 1..n;
+      "wdeg"   approxchol_lapWdeg    (src/approxChol.jl:1679-1734): sortperm of
+               the weighted degrees times 1 + rand();
+      "random" approxchol_lapRandom  (src/approxChol.jl:1736-1789): a uniform
+               random permutation (Fisher-Yates on rand(); Julia's randperm
+               samples its integers differently)."""
     a = _csc(a)
     n = a.shape[0]
+    if order == "given":
+        return None
+    if order == "wdeg":
+        v = np.asarray(a.sum(axis=0), dtype=np.float64).ravel()
+        v = v * (1.0 + rand(n))
+        return (np.argsort(v, kind="stable") + 1).astype(np.int64)
+    if order == "random":
+        p = np.arange(1, n + 1, dtype=np.int64)
+        u = rand(n - 1)
+        for t, i in enumerate(range(n - 1, 0, -1)):
+            j = min(int(u[t] * (i + 1)), i)
+            p[i], p[j] = p[j], p[i]
+        return p
+    raise ValueError(f"unknown elimination order {order!r} (deg, given, wdeg, random)")
+
+
+def approx_chol(a, params: ApproxCholParams | None = None) -> LDLinv:
+    """The reference's host elimination, drawing from the global stream:
+    `approxChol(LLmatp(a))` for the default :deg order (src/approxChol.jl:864-977),
+    `approxChol(LLMatOrd(a[, p]))` for :given, :wdeg and :random
+    (src/approxChol.jl:758-862)."""
+    a = _csc(a)
+    n = a.shape[0]
+    order = (params or ApproxCholParams()).order
     L = lib()
     h = ctypes.c_void_p()
     cp = a.indptr.astype(np.int64) + 1
     rv = a.indices.astype(np.int64) + 1
-    check(L.acg_approxchol(n, cp, rv, np.ascontiguousarray(a.data), _RNG, ctypes.byref(h)))
+    if order == "deg":
+        check(L.acg_approxchol(n, cp, rv, np.ascontiguousarray(a.data), _RNG, ctypes.byref(h)))
+    else:
+        p = elimination_order(a, order)
+        pp = None if p is None else p.ctypes.data_as(ctypes.c_void_p)
+        check(L.acg_approxchol_ordered(n, cp, rv, np.ascontiguousarray(a.data), pp, _RNG, ctypes.byref(h)))
     try:
         nn = ctypes.c_int64()
         F = ctypes.c_int64()
@@ -392,18 +436,17 @@ def approxchol_lap1(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False
     """Dispatch on params.order (src/approxChol.jl:1791-1851); the :deg order is
     approxchol_lapGreedy (src/approxChol.jl:1581-1626)."""
     params = params or ApproxCholParams()
-    if params.order != "deg":
-        raise NotImplementedError(f"order {params.order!r}: only the default :deg elimination is built")
     if params.split >= 1:
         raise NotImplementedError("split/merge elimination (approxchol_lap2) is not built")
     t1 = time.time()
-    ldli = approx_chol(a)
+    ldli = approx_chol(a, params)
     s = DeviceLapSolver(a, ldli, tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts,
                         params=params, precision=precision, options=options)
     if verbose:
         a = _csc(a)
         dg = np.asarray(a.sum(axis=0)).ravel()
-        print("Using greedy degree ordering. Factorization time: ", time.time() - t1)
+        names = {"deg": "greedy degree", "given": "given", "wdeg": "wted degree", "random": "random"}
+        print(f"Using {names.get(params.order, params.order)} ordering. Factorization time: ", time.time() - t1)
         print(f"Factorization size: {2 * ldli.nnz}")
         print("Ratio of operator edges to original edges: ", 2 * ldli.nnz / a.nnz)
         print("ratio of max to min diagonal of laplacian : ", dg.max() / dg.min())
@@ -446,6 +489,69 @@ def approxchol_lap(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False,
             solvers.append(approxchol_lap1(asub, **kw))
     return _BlockSolver(comps, solvers, dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose,
                                              pcgIts=pcgIts))
+
+
+def adj_val_and_excess(sddm):
+    """`adjValAndExcess` (src/graphOps.jl:43-48): the adjacency a = diag(M) - M
+    (off-diagonal weights, no stored diagonal), the diagonal, and the row sums
+    M*1 (the diagonal's excess over the off-diagonal weights)."""
+    m = _csc(sddm)
+    dval = np.asarray(m.diagonal(), dtype=np.float64)
+    a = _csc(sp.diags(dval) - m)
+    a.setdiag(0.0)
+    a.eliminate_zeros()
+    a = _csc(a)
+    dexcess = np.asarray(m @ np.ones(m.shape[0]), dtype=np.float64)
+    return a, dval, dexcess
+
+
+def extend_matrix(a, dval, dexcess):
+    """`extendMatrix` (src/graphOps.jl:56-79): append a ground vertex joined to
+    every vertex whose excess exceeds 100*eps times its diagonal, with the
+    excess as the edge weight; `a` itself when there is no excess at all."""
+    if np.abs(dexcess).sum() == 0:
+        return a
+    pos = np.where(dexcess > 100 * np.finfo(np.float64).eps * dval)[0]
+    n = a.shape[0]
+    coo = a.tocoo()
+    i = np.concatenate([coo.row, pos, np.full(pos.size, n)])
+    j = np.concatenate([coo.col, np.full(pos.size, n), pos])
+    v = np.concatenate([coo.data, dexcess[pos], dexcess[pos]])
+    return _csc(sp.csc_matrix((v, (i, j)), shape=(n + 1, n + 1)))
+
+
+def approxchol_sddm(sddm, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False, pcgIts=None,
+                    params: ApproxCholParams | None = None, precision="fp64", options=None):
+    """`approxchol_sddm = sddmWrapLap(approxchol_lap)` (src/approxChol.jl:1862,
+    src/solverInterface.jl:324-350): solves M x = b for a symmetric, diagonally
+    dominant M with non-positive off-diagonals by grounding the diagonal excess
+    in one extra vertex and solving the extended Laplacian system on the GPU."""
+    m = _csc(sddm)
+    if m.shape[0] != m.shape[1]:
+        raise ValueError("the SDDM matrix must be square")
+    n = m.shape[0]
+    a, dval, dexcess = adj_val_and_excess(m)
+    a1 = extend_matrix(a, dval, dexcess)
+    kw = dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts, params=params,
+              precision=precision, options=options)
+    if a1.shape == m.shape:
+        # no excess: the matrix is a Laplacian (src/solverInterface.jl:338-341)
+        return approxchol_lap(a, **kw)
+    F = approxchol_lap(a1, **kw)
+    defaults = dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts)
+
+    def f(b, tol=None, maxits=None, maxtime=None, verbose=None, pcgIts=None):
+        b = np.asarray(b, dtype=np.float64)
+        if b.shape[0] != n:
+            raise ValueError(f"rhs has {b.shape[0]} rows, matrix has {n}")
+        call = {k: (v if v is not None else defaults[k]) for k, v in
+                dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts).items()}
+        xaug = F(np.concatenate([b, [-b.sum()]]), **call)
+        xaug = xaug - xaug[-1]
+        return xaug[:n]
+
+    f.solver = F
+    return f
 
 
 _seed_from_entropy_done = False

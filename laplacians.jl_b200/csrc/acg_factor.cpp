@@ -367,4 +367,161 @@ void approx_chol_deg(int64_t n, const int64_t* colptr, const int64_t* rowval,
   out.colptr[it - 1] = ldli_row_ptr;
 }
 
+// Elimination in a fixed order: approxChol(::LLMatOrd) (src/approxChol.jl:758-862;
+// the later of its two definitions, which is the one Julia keeps) on
+// LLMatOrd(a) (src/approxChol.jl:203-229) or LLMatOrd(a, perm)
+// (src/approxChol.jl:265-294), with the factor of a permuted order mapped back
+// to the original vertex ids as approxchol_lapWdeg / approxchol_lapRandom do
+// (src/approxChol.jl:1712-1713, 1770-1771).  perm (1-based, perm[k] = the
+// vertex eliminated k-th) may be null: the given order 1..n.
+void approx_chol_ord(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                     const int64_t* perm, JuliaRng* rng, HostFactor& out) {
+  if (n < 2) throw std::runtime_error("approxChol needs at least 2 vertices");
+  const int64_t base = colptr[0];
+  const int64_t m = colptr[n] - base;
+  std::vector<int64_t> invp(n + 1);
+  if (perm) {
+    std::vector<char> seen(n + 1, 0);
+    for (int64_t k = 1; k <= n; ++k) {
+      const int64_t v = perm[k - 1];
+      if (v < 1 || v > n || seen[v]) throw std::runtime_error("perm is not a permutation of 1..n");
+      seen[v] = 1;
+      invp[v] = k;
+    }
+  } else {
+    for (int64_t v = 1; v <= n; ++v) invp[v] = v;
+  }
+  // LLMatOrd: records 1..m (0 ends a column); column i holds the edges to j > i
+  std::vector<int64_t> lrow(m + 1, 0), lnext(m + 1, 0);
+  std::vector<double> lval(m + 1, 0.0);
+  std::vector<int64_t> cols(n + 1, 0);
+  int64_t rp = 1;
+  for (int64_t i0 = 1; i0 <= (perm ? n : n - 1); ++i0) {
+    const int64_t i = invp[i0];
+    int64_t next = 0;
+    for (int64_t ind = colptr[i0 - 1] - base; ind < colptr[i0] - base; ++ind) {
+      const int64_t j = invp[rowval[ind]];
+      if (i < j) {
+        lrow[rp] = j;
+        lnext[rp] = next;
+        lval[rp] = nzval[ind];
+        next = rp;
+        ++rp;
+      }
+    }
+    cols[i] = next;
+  }
+
+  out.n = n;
+  out.col.assign(n - 1, 0);
+  out.colptr.assign(n, 0);
+  out.rowval.clear();
+  out.fval.clear();
+  out.d.assign(n, 0.0);
+  std::vector<int64_t> crow, cptr, h, mrow, mptr;
+  std::vector<double> cval, mval, cumspace;
+  int64_t ldli_row_ptr = 1;
+  for (int64_t i = 1; i <= n - 1; ++i) {
+    out.col[i - 1] = i;
+    out.colptr[i - 1] = ldli_row_ptr;
+    // get_ll_col (src/approxChol.jl:387-410)
+    int64_t len = 0;
+    crow.clear();
+    cptr.clear();
+    cval.clear();
+    for (int64_t q = cols[i]; q != 0; q = lnext[q]) {
+      crow.push_back(lrow[q]);
+      cptr.push_back(q);
+      cval.push_back(lval[q]);
+      ++len;
+    }
+    if (len == 0) throw std::runtime_error("eliminated vertex has no later neighbour (graph disconnected?)");
+    // compressCol! on LLcol (src/approxChol.jl:451-492): QuickSort by row,
+    // merge equal rows keeping the first record, QuickSort by value.
+    h.resize(len);
+    for (int64_t k = 0; k < len; ++k) h[k] = k;
+    julia_quicksort(h.data(), 0, len - 1, [&](int64_t x, int64_t y) { return crow[x] < crow[y]; });
+    mrow.clear();
+    mptr.clear();
+    mval.clear();
+    int64_t currow = crow[h[0]], curptr = cptr[h[0]];
+    double curval = cval[h[0]];
+    for (int64_t k = 1; k < len; ++k) {
+      const int64_t x = h[k];
+      if (crow[x] != currow) {
+        mrow.push_back(currow);
+        mptr.push_back(curptr);
+        mval.push_back(curval);
+        currow = crow[x];
+        curval = cval[x];
+        curptr = cptr[x];
+      } else {
+        curval = curval + cval[x];
+      }
+    }
+    mrow.push_back(currow);
+    mptr.push_back(curptr);
+    mval.push_back(curval);
+    len = (int64_t)mrow.size();
+    h.resize(len);
+    for (int64_t k = 0; k < len; ++k) h[k] = k;
+    julia_quicksort(h.data(), 0, len - 1, [&](int64_t x, int64_t y) { return mval[x] < mval[y]; });
+
+    cumspace.resize(len);
+    double csum = 0.0;
+    for (int64_t k = 0; k < len; ++k) {
+      csum = csum + mval[h[k]];
+      cumspace[k] = csum;
+    }
+    double wdeg = csum;
+    double colScale = 1.0;
+    for (int64_t jo = 0; jo < len - 1; ++jo) {
+      const int64_t c = h[jo];
+      const double w = mval[c] * colScale;
+      const int64_t j = mrow[c];
+      const double f = w / wdeg;
+      const double r = julia_rand(rng) * (csum - cumspace[jo]) + cumspace[jo];
+      int64_t lo = -1, hi = len;  // searchsortedfirst over 1..len
+      while (lo < hi - 1) {
+        const int64_t mid = lo + ((hi - lo) >> 1);
+        if (cumspace[mid] < r) lo = mid; else hi = mid;
+      }
+      const int64_t koff = hi < len ? hi : len - 1;  // r can only exceed csum by rounding
+      const int64_t k = mrow[h[koff]];
+      const double newEdgeVal = w * (1.0 - f);
+      const int64_t q = mptr[c];
+      if (j < k) {  // the new edge (j, k) goes into the lower column
+        lrow[q] = k;
+        lnext[q] = cols[j];
+        lval[q] = newEdgeVal;
+        cols[j] = q;
+      } else {
+        lrow[q] = j;
+        lnext[q] = cols[k];
+        lval[q] = newEdgeVal;
+        cols[k] = q;
+      }
+      colScale = colScale * (1.0 - f);
+      wdeg = wdeg - 2.0 * w + w * w / wdeg;
+      out.rowval.push_back(j);
+      out.fval.push_back(f);
+      ++ldli_row_ptr;
+    }
+    const int64_t c = h[len - 1];
+    out.rowval.push_back(mrow[c]);
+    out.fval.push_back(1.0);
+    ++ldli_row_ptr;
+    out.d[i - 1] = mval[c] * colScale;
+  }
+  out.colptr[n - 1] = ldli_row_ptr;
+  if (perm) {
+    // LDLinv(p[col], colptr, p[rowval], fval, d[ip])
+    for (auto& v : out.col) v = perm[v - 1];
+    for (auto& v : out.rowval) v = perm[v - 1];
+    std::vector<double> d2(n);
+    for (int64_t v = 1; v <= n; ++v) d2[v - 1] = out.d[invp[v] - 1];
+    out.d.swap(d2);
+  }
+}
+
 }  // namespace acg

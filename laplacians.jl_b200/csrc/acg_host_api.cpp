@@ -55,16 +55,19 @@ int acg_sha256(const uint8_t* data, int64_t len, uint8_t out[32]) {
   return ACG_OK;
 }
 
-int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
-                   uint64_t rng_state[4], acg_factor** out) {
+namespace {
+
+// Shared by acg_approxchol (:deg) and acg_approxchol_ordered (a fixed order).
+int approxchol_entry(const char* name, int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                     const int64_t* perm, bool ordered, uint64_t rng_state[4], acg_factor** out) {
   if (!out || !colptr || !rowval || !nzval || !rng_state || n < 2) {
-    acg::set_last_error("acg_approxchol: bad arguments (need n >= 2 and non-null arrays)");
+    acg::set_last_error(std::string(name) + ": bad arguments (need n >= 2 and non-null arrays)");
     return ACG_ERR_INVALID;
   }
   *out = nullptr;
   const int64_t base = colptr[0];
   if (base != 0 && base != 1) {
-    acg::set_last_error("acg_approxchol: colptr[0] must be 0 or 1");
+    acg::set_last_error(std::string(name) + ": colptr[0] must be 0 or 1");
     return ACG_ERR_INVALID;
   }
   try {
@@ -85,7 +88,7 @@ int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval, cons
     }
     for (int64_t p = 0; p < m; ++p) {
       if (rv[p] < 1 || rv[p] > n) {
-        acg::set_last_error("acg_approxchol: row index out of range");
+        acg::set_last_error(std::string(name) + ": row index out of range");
         return ACG_ERR_INVALID;
       }
     }
@@ -93,7 +96,8 @@ int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval, cons
     std::memcpy(r.s, rng_state, sizeof(r.s));
     auto* fac = new acg_factor();
     try {
-      acg::approx_chol_deg(n, colptr, rv, nzval, &r, fac->f);
+      if (ordered) acg::approx_chol_ord(n, colptr, rv, nzval, perm, &r, fac->f);
+      else acg::approx_chol_deg(n, colptr, rv, nzval, &r, fac->f);
     } catch (...) {
       delete fac;
       throw;
@@ -102,12 +106,24 @@ int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval, cons
     *out = fac;
     return ACG_OK;
   } catch (const std::bad_alloc&) {
-    acg::set_last_error("acg_approxchol: host out of memory");
+    acg::set_last_error(std::string(name) + ": host out of memory");
     return ACG_ERR_NOMEM;
   } catch (const std::exception& e) {
-    acg::set_last_error(std::string("acg_approxchol: ") + e.what());
+    acg::set_last_error(std::string(name) + ": " + e.what());
     return ACG_ERR_INVALID;
   }
+}
+
+}  // namespace
+
+int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                   uint64_t rng_state[4], acg_factor** out) {
+  return approxchol_entry("acg_approxchol", n, colptr, rowval, nzval, nullptr, false, rng_state, out);
+}
+
+int acg_approxchol_ordered(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                           const int64_t* perm, uint64_t rng_state[4], acg_factor** out) {
+  return approxchol_entry("acg_approxchol_ordered", n, colptr, rowval, nzval, perm, true, rng_state, out);
 }
 
 int acg_factor_dims(const acg_factor* f, int64_t* n, int64_t* nnz) {

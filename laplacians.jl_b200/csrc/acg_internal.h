@@ -19,6 +19,9 @@ struct HostFactor {
 
 void approx_chol_deg(int64_t n, const int64_t* colptr, const int64_t* rowval,
                      const double* nzval, JuliaRng* rng, HostFactor& out);
+// Elimination in a fixed order (perm: 1-based, null = 1..n); see acg_factor.cpp.
+void approx_chol_ord(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                     const int64_t* perm, JuliaRng* rng, HostFactor& out);
 
 // Thread-local error text returned by acg_last_error().
 void set_last_error(const std::string& msg);

@@ -281,3 +281,132 @@ def approx_chol(colptr, rowval, nzval, rng: JuliaRng):
     ldcolptr[it - 1] = ptr_row
     return (np.array(col, np.int64), np.array(ldcolptr, np.int64), np.array(ldrowval, np.int64),
             np.array(ldfval, np.float64), np.array(d, np.float64))
+
+
+# ---- fixed-order elimination: LLMatOrd + approxChol(::LLMatOrd) ---------------
+
+class LLord:
+    """Immutable column record (src/approxCholTypes.jl:42-46)."""
+    __slots__ = ("row", "next", "val")
+
+    def __init__(self, row, nxt, val):
+        self.row = row
+        self.next = nxt
+        self.val = val
+
+
+class LLcol:
+    """Entry of a gathered column (src/approxCholTypes.jl:54-58)."""
+    __slots__ = ("row", "ptr", "val")
+
+    def __init__(self, row, ptr, val):
+        self.row = row
+        self.ptr = ptr
+        self.val = val
+
+
+def approx_chol_ord(colptr, rowval, nzval, rng: JuliaRng, perm=None):
+    """approxChol(::LLMatOrd) (src/approxChol.jl:758-862) on LLMatOrd(a)
+    (src/approxChol.jl:203-229) or LLMatOrd(a, perm) (src/approxChol.jl:265-294),
+    mapped back through perm as approxchol_lapWdeg does
+    (src/approxChol.jl:1712-1713).  colptr/rowval 1-based; perm 1-based or None."""
+    n = len(colptr) - 1
+    m = colptr[n] - 1
+    if perm is None:
+        invp = list(range(n + 1))
+        cols_of = range(1, n)  # the reference stops at n-1
+    else:
+        invp = [0] * (n + 1)
+        for k, v in enumerate(perm, start=1):
+            invp[v] = k
+        cols_of = range(1, n + 1)
+    lles = [None] * (m + 1)
+    cols = [0] * (n + 1)
+    ptr = 1
+    for i0 in cols_of:
+        i = invp[i0]
+        nxt = 0
+        for ind in range(colptr[i0 - 1], colptr[i0]):
+            j = invp[rowval[ind - 1]]
+            if i < j:
+                lles[ptr] = LLord(j, nxt, nzval[ind - 1])
+                nxt = ptr
+                ptr += 1
+        cols[i] = nxt
+
+    col = [0] * (n - 1)
+    ldcolptr = [0] * n
+    ldrowval, ldfval = [], []
+    d = [0.0] * n
+    row_ptr = 1
+    for i in range(1, n):
+        col[i - 1] = i
+        ldcolptr[i - 1] = row_ptr
+        # get_ll_col (src/approxChol.jl:387-410)
+        cs = [None]
+        p = cols[i]
+        while p != 0:
+            cs.append(LLcol(lles[p].row, p, lles[p].val))
+            p = lles[p].next
+        ln = len(cs) - 1
+        # compressCol! (src/approxChol.jl:451-492)
+        quicksort(cs, 1, ln, lambda x, y: x.row < y.row)
+        k = 0
+        cur = LLcol(cs[1].row, cs[1].ptr, cs[1].val)
+        for q in range(2, ln + 1):
+            if cs[q].row != cur.row:
+                k += 1
+                cs[k] = cur
+                cur = LLcol(cs[q].row, cs[q].ptr, cs[q].val)
+            else:
+                cur = LLcol(cur.row, cur.ptr, cur.val + cs[q].val)
+        k += 1
+        cs[k] = cur
+        ln = k
+        quicksort(cs, 1, ln, lambda x, y: x.val < y.val)
+        cum = [0.0] * (ln + 1)
+        csum = 0.0
+        for q in range(1, ln + 1):
+            csum = csum + cs[q].val
+            cum[q] = csum
+        wdeg = csum
+        col_scale = 1.0
+        for jo in range(1, ln):
+            c = cs[jo]
+            w = c.val * col_scale
+            j = c.row
+            f = w / wdeg
+            r = rng.rand() * (csum - cum[jo]) + cum[jo]
+            koff = ln
+            for kk in range(1, ln + 1):  # searchsortedfirst on 1..len
+                if not (cum[kk] < r):
+                    koff = kk
+                    break
+            kv = cs[koff].row
+            new_val = w * (1.0 - f)
+            if j < kv:
+                lles[c.ptr] = LLord(kv, cols[j], new_val)
+                cols[j] = c.ptr
+            else:
+                lles[c.ptr] = LLord(j, cols[kv], new_val)
+                cols[kv] = c.ptr
+            col_scale = col_scale * (1.0 - f)
+            wdeg = wdeg - 2 * w + w * w / wdeg
+            ldrowval.append(j)
+            ldfval.append(f)
+            row_ptr += 1
+        c = cs[ln]
+        ldrowval.append(c.row)
+        ldfval.append(1.0)
+        row_ptr += 1
+        d[i - 1] = c.val * col_scale
+    ldcolptr[n - 1] = row_ptr
+    col = np.array(col, np.int64)
+    rowv = np.array(ldrowval, np.int64)
+    d = np.array(d, np.float64)
+    if perm is not None:
+        p = np.asarray(perm, np.int64)
+        col = p[col - 1]
+        rowv = p[rowv - 1]
+        d = d[np.asarray(invp[1:], np.int64) - 1]
+    return col, np.array(ldcolptr, np.int64), rowv, np.array(ldfval, np.float64), d

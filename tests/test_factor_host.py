@@ -82,3 +82,44 @@ def test_negative_weight_rejected():
     a[0, 1] = a[1, 0] = -1.0
     with pytest.raises(Exception):
         acgpu.approx_chol(a.tocsc())
+
+
+def _ref_ordered(a, order, seed):
+    """The restatement's factor for a fixed order: the permutation comes from
+    the product's stream (as approx_chol draws it), the elimination from the
+    restatement continuing that stream."""
+    from acgpu.solvers import elimination_order
+    a = acgpu.solvers._csc(a)
+    acgpu.seed(seed)
+    p = elimination_order(a, order)
+    rng = JuliaRng(state=[int(x) for x in acgpu.rng_state()])
+    cp = (a.indptr + 1).tolist()
+    rv = (a.indices + 1).tolist()
+    return approxchol_ref.approx_chol_ord(cp, rv, a.data.tolist(), rng, None if p is None else p.tolist())
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("order", ["given", "wdeg", "random"])
+def test_ordered_factor_matches_restatement(name, make, order):
+    a = make()
+    ref = _ref_ordered(a, order, 11)
+    acgpu.seed(11)
+    f = acgpu.approx_chol(a, acgpu.ApproxCholParams(order=order))
+    got = (f.col, f.colptr, f.rowval, f.fval, f.d)
+    for x, y, what in zip(got, ref, ("col", "colptr", "rowval", "fval", "d")):
+        assert np.array_equal(np.asarray(x), np.asarray(y)), what
+    n = a.shape[0]
+    # a valid elimination order: every vertex but one eliminated once, F = colptr[end] - 1
+    assert len(set(f.col.tolist())) == n - 1 and f.colptr[-1] - 1 == f.fval.shape[0]
+
+
+def test_given_order_eliminates_in_index_order():
+    a = G.grid2(6, 5)
+    acgpu.seed(2)
+    f = acgpu.approx_chol(a, acgpu.ApproxCholParams(order="given"))
+    assert f.col.tolist() == list(range(1, a.shape[0]))
+
+
+def test_unknown_order_rejected():
+    with pytest.raises(ValueError):
+        acgpu.approx_chol(G.path_graph(4), acgpu.ApproxCholParams(order="bogus"))

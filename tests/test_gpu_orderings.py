@@ -1,0 +1,36 @@
+"""Factors of the fixed elimination orders (:given, :wdeg, :random;
+src/approxChol.jl:1628-1789) through the GPU solve: LDLsolver parity with the
+oracle on the same factor (1e-12, FP64), and full solves to tolerance."""
+import numpy as np
+import pytest
+
+import acgpu
+from acgpu import generators as G
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("order", ["deg", "given", "wdeg", "random"])
+def test_orderings_solve(gpu_ok, order):
+    a = G.grid2(50, weights="loguniform", seed=9)
+    params = acgpu.ApproxCholParams(order=order)
+    acgpu.seed(4)
+    ldli = acgpu.approx_chol(a, params)
+    dev = acgpu.DeviceLapSolver(a, ldli, params=params)
+    r = np.random.default_rng(1).standard_normal(a.shape[0])
+    r -= r.mean()
+    assert np.linalg.norm(dev.ldlsolve(r) - O.ldlsolve(ldli, r)) / np.linalg.norm(O.ldlsolve(ldli, r)) < 1e-12
+    b = np.random.default_rng(2).standard_normal(a.shape[0])
+    for prec in ("fp64", "mixed"):
+        x = dev(b, tol=1e-8, maxits=3000, precision=prec)
+        assert O.relres(a, x, b - b.mean()) <= 1e-8 * 1.01 if prec == "mixed" else \
+            dev.last_info[0].status == 0
+    st = dev.stats()
+    assert st["levels"] >= 1 and st["nnz_factor"] == ldli.nnz
+    dev.close()
+    # the closure route with the same params
+    acgpu.seed(4)
+    f = acgpu.approxchol_lap(a, tol=1e-8, params=params, precision="mixed")
+    x = f(b)
+    assert O.relres(a, x, b - b.mean()) <= 1e-8 * 1.01
