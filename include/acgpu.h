@@ -94,7 +94,8 @@ typedef struct {
   int wide_level_min;  /* levels at least this wide get a grid launch each; runs of
                           narrower levels whose values fit in shared memory run in
                           one CTA with block barriers (default 2048)              */
-  int sweep_blocks_per_sm;   /* resident blocks per SM of the single-vector sweeps (0 = 1) */
+  int sweep_blocks_per_sm;   /* resident blocks per SM of the single-vector sweeps (0 = by the
+                                DAG: 1, 2 or 4 as the tasks per level grow)              */
   int poll_mode;             /* waits on a pending value: 0 = automatic, 1 tight+sleep,
                                 2 tight only, 3 backoff                               */
   int tail;                  /* 2 = sweep the final narrow levels in one CTA from shared

@@ -202,6 +202,17 @@ def _maxits_int(maxits) -> int:
     return int(maxits)
 
 
+def _options(options: dict | None) -> AcgOptions:
+    """acg_options from a dict of knob names; a misspelled knob raises."""
+    opts = AcgOptions()
+    known = {f[0] for f in AcgOptions._fields_}
+    for k, v in (options or {}).items():
+        if k not in known:
+            raise ValueError(f"unknown solver option {k!r}; known: {sorted(known)}")
+        setattr(opts, k, int(v))
+    return opts
+
+
 class DeviceLapSolver:
     """The closure `f` of approxchol_lapGreedy (src/approxChol.jl:1624) with the
     solve on the GPU.  Holds the uploaded lap(a) and LDLinv until closed."""
@@ -214,12 +225,7 @@ class DeviceLapSolver:
         self.params = params or ApproxCholParams()
         self.defaults = dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts,
                              precision=precision)
-        opts = AcgOptions()
-        known = {f[0] for f in AcgOptions._fields_}
-        for k, v in (options or {}).items():
-            if k not in known:
-                raise ValueError(f"unknown solver option {k!r}; known: {sorted(known)}")
-            setattr(opts, k, int(v))
+        opts = _options(options)
         h = ctypes.c_void_p()
         check(lib().acg_create(self.n, a.indptr.astype(np.int64), a.indices.astype(np.int64),
                                np.ascontiguousarray(a.data), ldli.col, ldli.colptr, ldli.rowval, ldli.fval, ldli.d,
@@ -301,7 +307,8 @@ class GroupSolver:
     (blockSolver's per-component solves, src/solverInterface.jl:152-188, all at
     once).  Every graph must be connected and have at least 2 vertices."""
 
-    def __init__(self, graphs, factors=None, *, tol=1e-6, maxits=1000, maxtime=math.inf, stag_test=5):
+    def __init__(self, graphs, factors=None, *, tol=1e-6, maxits=1000, maxtime=math.inf, stag_test=5,
+                 options: dict | None = None):
         graphs = [_csc(a) for a in graphs]
         if factors is None:
             factors = [approx_chol(a) for a in graphs]
@@ -327,7 +334,7 @@ class GroupSolver:
         fval = np.concatenate(fvals)
         d = np.concatenate(ds)
         self.factor = LDLinv(col, colptr, rowval, fval, d)
-        opts = AcgOptions()
+        opts = _options(options)
         h = ctypes.c_void_p()
         check(lib().acg_create_group(len(graphs), self.offsets, self.n, a.indptr.astype(np.int64),
                                      a.indices.astype(np.int64), np.ascontiguousarray(a.data), col, col.shape[0],

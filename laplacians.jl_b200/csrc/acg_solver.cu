@@ -959,9 +959,20 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_sweep<double, false>, kSweepThreads, 0));
     ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], k_sweep<float, true>, kSweepThreads, 0));
     ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_sweep<float, false>, kSweepThreads, 0));
-    // One resident block (8 warps) per SM by default: more warps mostly add
-    // polling traffic on the L2 without shortening the dependency chains.
-    const int cap = (opts && opts->sweep_blocks_per_sm > 0) ? opts->sweep_blocks_per_sm : 1;
+    // Resident blocks (8 warps each) per SM: a deep, narrow DAG gains nothing
+    // from more warps (they add polling traffic without shortening the chains),
+    // a wide one is throughput-bound in its wide levels and gains from them.
+    // Automatic choice by the tasks per swept level (measured: the 2M
+    // path+matchings graph, ~150 per level, is fastest with 1; the 1M 3D grid,
+    // ~750, with 2; 256 graphs in one launch, thousands, with 4).
+    int cap = 1;
+    if (opts && opts->sweep_blocks_per_sm > 0) {
+      cap = opts->sweep_blocks_per_sm;
+    } else {
+      const int swept = std::max(1, (S.dt_K ? S.dt_L0 : nlev));
+      const double per_level = (double)std::max(S.ntasks_f, S.ntasks_b) / swept;
+      cap = per_level < 300.0 ? 1 : (per_level < 2000.0 ? 2 : 4);
+    }
     S.sweep_blocks[0] = sms * std::max(1, std::min(cap, std::min(occ[0], occ[1])));
     S.sweep_blocks[1] = sms * std::max(1, std::min(cap, std::min(occ[2], occ[3])));
     S.sweep_mode = (opts && opts->sweep_lanes == 1 && nseg == 1) ? 1 : 0;
