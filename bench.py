@@ -416,8 +416,9 @@ def run_orderings(args):
     n = a.shape[0]
     b = rhs(n, 13)
     out = {"workload": f"elimination orders on grid3({side}) log-uniform weights, tol 1e-8", "n": n}
-    for order in ("deg", "wdeg", "random", "given"):
-        params = acgpu.ApproxCholParams(order=order)
+    for order in ("deg", "lap2", "wdeg", "random", "given"):
+        # lap2: the split/merge elimination of approxchol_lap2 (:deg, split = merge = 2)
+        params = acgpu.ApproxCholParams("deg", 5, 2, 2) if order == "lap2" else acgpu.ApproxCholParams(order=order)
         acgpu.seed(FACTOR_SEED)
         t = time.perf_counter()
         ldli = acgpu.approx_chol(a, params)

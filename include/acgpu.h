@@ -75,6 +75,11 @@ int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval,
  * approxchol_lapWdeg / approxchol_lapRandom build it (src/approxChol.jl:1628-1789). */
 int acg_approxchol_ordered(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
                            const int64_t* perm, uint64_t rng_state[4], acg_factor** out);
+/* The split/merge elimination of approxchol_lap2 (split = merge = 2 there):
+ * approxChol(LLmatp(a, split), split, merge) (src/approxChol.jl:979-1157,
+ * 138-183) with compressAvgCol! (src/approxChol.jl:541-600). */
+int acg_approxchol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval, int64_t split,
+                         int64_t merge, uint64_t rng_state[4], acg_factor** out);
 /* n and F = length(ldli.fval). */
 int acg_factor_dims(const acg_factor* f, int64_t* n, int64_t* nnz);
 /* Copy out the LDLinv arrays in the reference layout (src/approxCholTypes.jl:73-79),

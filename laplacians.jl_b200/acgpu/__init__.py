@@ -7,14 +7,14 @@ The solves run in libacgpu.so (CUDA, sm_100a); see include/acgpu.h.
 """
 from . import generators, tuning
 from .solvers import (ApproxCholParams, DeviceLapSolver, GroupSolver, LDLinv, approx_chol, approxchol_lap, approxchol_lap1,
-                      approxchol_sddm,
+                      approxchol_lap2, approxchol_sddm,
                       components, lap, null_solver, rng_state, seed, set_rng_state, vec_to_comps)
 from .solvers import _init as _solvers_init
 from .tuning import autotune
 
 _solvers_init()
 
-__all__ = ["approxchol_lap", "approxchol_lap1", "approxchol_sddm", "ApproxCholParams", "LDLinv", "DeviceLapSolver", "GroupSolver",
+__all__ = ["approxchol_lap", "approxchol_lap1", "approxchol_lap2", "approxchol_sddm", "ApproxCholParams", "LDLinv", "DeviceLapSolver", "GroupSolver",
            "approx_chol",
            "lap", "seed", "rng_state", "set_rng_state", "components", "vec_to_comps", "null_solver", "generators",
            "autotune", "tuning"]

@@ -123,8 +123,6 @@ def elimination_order(a, order: str):
                samples its integers differently)."""
     a = _csc(a)
     n = a.shape[0]
-    if order == "given":
-        return None
     if order == "wdeg":
         v = np.asarray(a.sum(axis=0), dtype=np.float64).ravel()
         v = v * (1.0 + rand(n))
@@ -136,22 +134,30 @@ def elimination_order(a, order: str):
             j = min(int(u[t] * (i + 1)), i)
             p[i], p[j] = p[j], p[i]
         return p
-    raise ValueError(f"unknown elimination order {order!r} (deg, given, wdeg, random)")
+    return None  # any other order is the given one (src/approxChol.jl:1836-1850)
 
 
 def approx_chol(a, params: ApproxCholParams | None = None) -> LDLinv:
     """The reference's host elimination, drawing from the global stream:
     `approxChol(LLmatp(a))` for the default :deg order (src/approxChol.jl:864-977),
-    `approxChol(LLMatOrd(a[, p]))` for :given, :wdeg and :random
-    (src/approxChol.jl:758-862)."""
+    `approxChol(LLmatp(a, split), split, merge)` for :deg with split, merge >= 1
+    (src/approxChol.jl:979-1157; approxchol_lap2 uses 2, 2), and
+    `approxChol(LLMatOrd(a[, p]))` for :wdeg, :random and any other order, which
+    the reference treats as :given (src/approxChol.jl:758-862, 1791-1851)."""
     a = _csc(a)
     n = a.shape[0]
-    order = (params or ApproxCholParams()).order
+    params = params or ApproxCholParams()
+    order = params.order
     L = lib()
     h = ctypes.c_void_p()
     cp = a.indptr.astype(np.int64) + 1
     rv = a.indices.astype(np.int64) + 1
-    if order == "deg":
+    if order == "deg" and params.split >= 1:
+        if params.merge < 1:
+            raise NotImplementedError("approxChol(llmat, split) without merging is not built; use merge >= 1")
+        check(L.acg_approxchol_split(n, cp, rv, np.ascontiguousarray(a.data), int(params.split), int(params.merge),
+                                     _RNG, ctypes.byref(h)))
+    elif order == "deg":
         check(L.acg_approxchol(n, cp, rv, np.ascontiguousarray(a.data), _RNG, ctypes.byref(h)))
     else:
         p = elimination_order(a, order)
@@ -443,8 +449,6 @@ def approxchol_lap1(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False
     """Dispatch on params.order (src/approxChol.jl:1791-1851); the :deg order is
     approxchol_lapGreedy (src/approxChol.jl:1581-1626)."""
     params = params or ApproxCholParams()
-    if params.split >= 1:
-        raise NotImplementedError("split/merge elimination (approxchol_lap2) is not built")
     t1 = time.time()
     ldli = approx_chol(a, params)
     s = DeviceLapSolver(a, ldli, tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts,
@@ -496,6 +500,15 @@ def approxchol_lap(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False,
             solvers.append(approxchol_lap1(asub, **kw))
     return _BlockSolver(comps, solvers, dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose,
                                              pcgIts=pcgIts))
+
+
+def approxchol_lap2(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False, pcgIts=None,
+                    params: ApproxCholParams | None = None, precision="fp64", options=None):
+    """`approxchol_lap2` (src/approxChol.jl:1559-1578): approxchol_lap with the
+    split/merge elimination, ApproxCholParams(:deg, stag_test, 2, 2)."""
+    st = (params or ApproxCholParams()).stag_test
+    return approxchol_lap(a, tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose, pcgIts=pcgIts,
+                          params=ApproxCholParams("deg", st, 2, 2), precision=precision, options=options)
 
 
 def adj_val_and_excess(sddm):

@@ -41,32 +41,35 @@ struct LinkedCols {
   std::vector<int64_t> degs;  // initial degrees (1-based)
 };
 
-// Approximate priority queue on degrees (ApproxCholPQ, split = 1).
+// Approximate priority queue on degrees (ApproxCholPQ; split = 1 for the :deg
+// elimination, > 1 for the split/merge one, whose keys are split x degrees).
 struct DegreeQueue {
   int64_t n = 0;
+  int64_t split = 1;
   int64_t minlist = 1;
   int64_t nitems = 0;
   std::vector<int64_t> prev, next, key;  // indexed by 1-based vertex id; 0 = none
-  std::vector<int64_t> lists;            // indexed 1..2n+1
+  std::vector<int64_t> lists;            // indexed 1..2*split*n+1
 
   int64_t key_map(int64_t x) const {
-    const int64_t k = n, upper = 2 * n + 1;
+    const int64_t k = split * n, upper = 2 * split * n + 1;
     if (x <= k) return x;
     int64_t m = k + x / k;
     return m < upper ? m : upper;
   }
 
-  void init(const std::vector<int64_t>& degs, int64_t nv) {
+  void init(const std::vector<int64_t>& degs, int64_t nv, int64_t sp = 1) {
     n = nv;
+    split = sp;
     prev.assign(n + 1, 0);
     next.assign(n + 1, 0);
     key.assign(n + 1, 0);
-    lists.assign(2 * n + 2, 0);
+    lists.assign(2 * split * n + 2, 0);
     minlist = 1;
     nitems = n;
     for (int64_t i = 1; i <= n; ++i) {
       int64_t k = degs[i];
-      if (k < 1 || k > 2 * n + 1) throw std::runtime_error("vertex degree out of queue range");
+      if (k < 1 || k > 2 * split * n + 1) throw std::runtime_error("vertex degree out of queue range");
       int64_t h = lists[k];
       if (h > 0) {
         prev[i] = 0; next[i] = h; key[i] = k;
@@ -114,7 +117,7 @@ struct DegreeQueue {
   void inc(int64_t i) {
     int64_t oldlist = key_map(key[i]);
     int64_t newlist = key_map(key[i] + 1);
-    if (newlist > 2 * n + 1) throw std::runtime_error("degree queue key overflow");
+    if (newlist > 2 * split * n + 1) throw std::runtime_error("degree queue key overflow");
     if (newlist != oldlist) {
       move(i, key[i] + 1, oldlist, newlist);
     } else {
@@ -522,6 +525,221 @@ void approx_chol_ord(int64_t n, const int64_t* colptr, const int64_t* rowval, co
     for (int64_t v = 1; v <= n; ++v) d2[v - 1] = out.d[invp[v] - 1];
     out.d.swap(d2);
   }
+}
+
+// The split/merge elimination of approxchol_lap2: approxChol(a, split, merge)
+// (src/approxChol.jl:979-1157) on LLmatp(a, split) (src/approxChol.jl:138-183),
+// averaging parallel edges with compressAvgCol! (src/approxChol.jl:541-600).
+// Every edge becomes `split` parallel records of weight w/split; record k of
+// CSC entry p (0-based) is split*p + k, paired with record k of the entry's
+// transpose.
+void approx_chol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                       int64_t split, int64_t merge, JuliaRng* rng, HostFactor& out) {
+  if (n < 2) throw std::runtime_error("approxChol needs at least 2 vertices");
+  if (split < 1 || merge < 1) throw std::runtime_error("split and merge must be at least 1");
+  const int64_t base = colptr[0];
+  const int64_t nnz = colptr[n] - base;
+  LinkedCols a;
+  a.n = n;
+  a.row.resize(split * nnz);
+  a.val.resize(split * nnz);
+  a.next.resize(split * nnz);
+  a.rev.resize(split * nnz);
+  a.head.assign(n + 1, -1);
+  a.degs.assign(n + 1, 0);
+  for (int64_t c = 0; c < n; ++c) {
+    const int64_t p0 = colptr[c] - base, p1 = colptr[c + 1] - base;
+    if (p1 <= p0) throw std::runtime_error("vertex " + std::to_string(c + 1) + " has no edges");
+    a.degs[c + 1] = split * (p1 - p0);
+    // the first entry: its last copy ends the column, the others chain to it
+    int64_t prevrec = split * p0 + split - 1;
+    a.row[prevrec] = rowval[p0];
+    a.val[prevrec] = nzval[p0] / (double)split;
+    a.next[prevrec] = prevrec;
+    for (int64_t k = 0; k < split - 1; ++k) {
+      const int64_t r = split * p0 + k;
+      a.row[r] = rowval[p0];
+      a.val[r] = nzval[p0] / (double)split;
+      a.next[r] = prevrec;
+      prevrec = r;
+    }
+    for (int64_t p = p0 + 1; p < p1; ++p) {
+      for (int64_t k = 0; k < split; ++k) {
+        const int64_t r = split * p + k;
+        a.row[r] = rowval[p];
+        a.val[r] = nzval[p] / (double)split;
+        a.next[r] = prevrec;
+        prevrec = r;
+      }
+    }
+    a.head[c + 1] = prevrec;
+  }
+  {
+    std::vector<int64_t> cursor(n, 0);
+    for (int64_t c = 0; c < n; ++c) {
+      for (int64_t p = colptr[c] - base; p < colptr[c + 1] - base; ++p) {
+        const int64_t r = rowval[p] - 1;
+        const int64_t q = colptr[r] - base + cursor[r]++;
+        if (q >= colptr[r + 1] - base || rowval[q] != c + 1)
+          throw std::runtime_error("adjacency matrix is not structurally symmetric with sorted rows");
+        for (int64_t k = 0; k < split; ++k) a.rev[split * p + k] = split * q + k;
+      }
+    }
+  }
+
+  out.n = n;
+  out.col.assign(n - 1, 0);
+  out.colptr.assign(n, 0);
+  out.rowval.clear();
+  out.fval.clear();
+  out.d.assign(n, 0.0);
+  DegreeQueue pq;
+  pq.init(a.degs, n, split);
+  std::vector<int64_t> colspace(n);
+  std::vector<double> vals(n), csr(n);
+  int64_t it = 1;
+  int64_t ldli_row_ptr = 1;
+  auto by_row = [&](int64_t x, int64_t y) { return a.row[x] < a.row[y]; };
+  auto by_val_row = [&](int64_t x, int64_t y) {
+    return a.val[x] < a.val[y] || (a.val[x] == a.val[y] && a.row[x] < a.row[y]);
+  };
+  while (it < n) {
+    const int64_t i = pq.pop();
+    out.col[it - 1] = i;
+    out.colptr[it - 1] = ldli_row_ptr;
+    ++it;
+    // get_ll_col
+    int64_t len = 0;
+    int64_t rec = a.head[i];
+    while (true) {
+      if (a.val[rec] > 0.0) {
+        if (len >= (int64_t)colspace.size()) colspace.resize(2 * colspace.size() + 1);
+        colspace[len++] = rec;
+      }
+      if (a.next[rec] == rec) break;
+      rec = a.next[rec];
+    }
+    if (len == 0) throw std::runtime_error("eliminated vertex has no live edges (graph disconnected?)");
+    // compressAvgCol!: QuickSort by row; average each run of parallel edges
+    // (at most `merge` of them survive); QuickSort by (value, row).
+    julia_quicksort(colspace.data(), 0, len - 1, by_row);
+    int64_t ptr = 0;
+    int64_t cur = 0, nxt = 0;
+    while (nxt < len && a.row[colspace[cur]] == a.row[colspace[nxt]]) ++nxt;
+    while (cur < len) {
+      const int64_t num = nxt - cur;
+      double mul_sum = 0.0;
+      for (int64_t q = cur; q < nxt; ++q) mul_sum += a.val[colspace[q]];
+      if (num <= merge) {
+        const double nv = mul_sum / (double)num;
+        for (int64_t q = cur; q < nxt; ++q) {
+          const int64_t cr = colspace[q];
+          a.val[cr] = nv;
+          a.val[a.rev[cr]] = nv;
+          colspace[ptr++] = cr;
+        }
+      } else {
+        const double nv = mul_sum / (double)merge;
+        for (int64_t q = cur; q < cur + merge; ++q) {
+          const int64_t cr = colspace[q];
+          a.val[cr] = nv;
+          a.val[a.rev[cr]] = nv;
+          colspace[ptr++] = cr;
+        }
+        const int64_t currow = a.row[colspace[cur]];
+        for (int64_t q = cur + merge; q < nxt; ++q) {
+          a.val[a.rev[colspace[q]]] = 0.0;
+          pq.dec(currow);
+        }
+      }
+      cur = nxt;
+      while (nxt < len && a.row[colspace[cur]] == a.row[colspace[nxt]]) ++nxt;
+    }
+    len = ptr;
+    julia_quicksort(colspace.data(), 0, len - 1, by_val_row);
+
+    if ((int64_t)vals.size() < len) {
+      vals.resize(len);
+      csr.resize(len);
+    }
+    double csum = 0.0;
+    for (int64_t q = 0; q < len; ++q) {
+      csum = csum + a.val[colspace[q]];
+      vals[q] = a.val[colspace[q]];
+    }
+    double csum_rev = 0.0;  // csr[q] = sum of the values from q to the end
+    for (int64_t q = len - 1; q >= 0; --q) {
+      csum_rev += a.val[colspace[q]];
+      csr[q] = csum_rev;
+    }
+    double wdeg = csum;
+    double colScale = 1.0;
+    int64_t next_edge = 0;  // the first entry that is not a parallel copy of the current neighbour
+    double final_d = 0.0;
+    for (int64_t jo = 0; jo < len - 1; ++jo) {
+      const bool is_new = jo == next_edge;
+      while (next_edge < len && a.row[colspace[jo]] == a.row[colspace[next_edge]]) ++next_edge;
+      if (next_edge == len) {
+        // only copies of the last neighbour remain: no self loop is created
+        for (int64_t q = jo; q < len - 1; ++q) {
+          const int64_t cr = colspace[q];
+          final_d += vals[q] * colScale;
+          if (it < n) pq.dec(a.row[cr]);
+          a.val[a.rev[cr]] = 0.0;
+        }
+        break;
+      }
+      const int64_t llr = colspace[jo];
+      const double w = vals[jo] * colScale;
+      const int64_t j = a.row[llr];
+      const int64_t revj = a.rev[llr];
+      double f = w / wdeg;
+      vals[jo] = 0.0;
+      const double r = julia_rand(rng) * csr[next_edge];
+      // searchsortedlast on the non-increasing csr: the last q with csr[q] >= r
+      int64_t lo = -1, hi = len;
+      while (lo < hi - 1) {
+        const int64_t mid = lo + ((hi - lo) >> 1);
+        if (csr[mid] < r) hi = mid; else lo = mid;
+      }
+      const int64_t koff = lo < 0 ? 0 : lo;
+      const int64_t k = a.row[colspace[koff]];
+      pq.inc(k);
+      const double newEdgeVal = a.val[llr] * csr[next_edge] / csum;
+      a.row[revj] = k;
+      a.val[revj] = newEdgeVal;
+      a.rev[revj] = llr;
+      const int64_t khead = a.head[k];
+      a.head[k] = llr;
+      a.next[llr] = khead;
+      a.rev[llr] = revj;
+      a.val[llr] = newEdgeVal;
+      a.row[llr] = j;
+      if (is_new) {
+        out.rowval.push_back(j);
+        out.fval.push_back(f);
+        ++ldli_row_ptr;
+      } else {
+        out.fval.back() = out.fval.back() + f;
+      }
+      if (jo == next_edge - 1) {  // the last copy of this neighbour
+        f = out.fval.back();
+        colScale = colScale * (1.0 - f);
+        const double omf = 1.0 - f;
+        wdeg = wdeg * (omf * omf);
+      }
+    }
+    const int64_t llr = colspace[len - 1];
+    final_d += vals[len - 1] * colScale;
+    const int64_t j = a.row[llr];
+    if (it < n) pq.dec(j);
+    a.val[a.rev[llr]] = 0.0;
+    out.rowval.push_back(j);
+    out.fval.push_back(1.0);
+    ++ldli_row_ptr;
+    out.d[i - 1] = final_d;
+  }
+  out.colptr[it - 1] = ldli_row_ptr;
 }
 
 }  // namespace acg

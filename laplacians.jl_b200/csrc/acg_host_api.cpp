@@ -58,8 +58,10 @@ int acg_sha256(const uint8_t* data, int64_t len, uint8_t out[32]) {
 namespace {
 
 // Shared by acg_approxchol (:deg) and acg_approxchol_ordered (a fixed order).
+// mode 0: :deg; 1: a fixed order (perm, null = given); 2: split/merge
 int approxchol_entry(const char* name, int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
-                     const int64_t* perm, bool ordered, uint64_t rng_state[4], acg_factor** out) {
+                     const int64_t* perm, int mode, int64_t split, int64_t merge, uint64_t rng_state[4],
+                     acg_factor** out) {
   if (!out || !colptr || !rowval || !nzval || !rng_state || n < 2) {
     acg::set_last_error(std::string(name) + ": bad arguments (need n >= 2 and non-null arrays)");
     return ACG_ERR_INVALID;
@@ -96,7 +98,8 @@ int approxchol_entry(const char* name, int64_t n, const int64_t* colptr, const i
     std::memcpy(r.s, rng_state, sizeof(r.s));
     auto* fac = new acg_factor();
     try {
-      if (ordered) acg::approx_chol_ord(n, colptr, rv, nzval, perm, &r, fac->f);
+      if (mode == 1) acg::approx_chol_ord(n, colptr, rv, nzval, perm, &r, fac->f);
+      else if (mode == 2) acg::approx_chol_split(n, colptr, rv, nzval, split, merge, &r, fac->f);
       else acg::approx_chol_deg(n, colptr, rv, nzval, &r, fac->f);
     } catch (...) {
       delete fac;
@@ -118,12 +121,21 @@ int approxchol_entry(const char* name, int64_t n, const int64_t* colptr, const i
 
 int acg_approxchol(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
                    uint64_t rng_state[4], acg_factor** out) {
-  return approxchol_entry("acg_approxchol", n, colptr, rowval, nzval, nullptr, false, rng_state, out);
+  return approxchol_entry("acg_approxchol", n, colptr, rowval, nzval, nullptr, 0, 1, 1, rng_state, out);
 }
 
 int acg_approxchol_ordered(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
                            const int64_t* perm, uint64_t rng_state[4], acg_factor** out) {
-  return approxchol_entry("acg_approxchol_ordered", n, colptr, rowval, nzval, perm, true, rng_state, out);
+  return approxchol_entry("acg_approxchol_ordered", n, colptr, rowval, nzval, perm, 1, 1, 1, rng_state, out);
+}
+
+int acg_approxchol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval, int64_t split,
+                         int64_t merge, uint64_t rng_state[4], acg_factor** out) {
+  if (split < 1 || merge < 1 || split > 64) {
+    acg::set_last_error("acg_approxchol_split: need 1 <= split <= 64 and merge >= 1");
+    return ACG_ERR_INVALID;
+  }
+  return approxchol_entry("acg_approxchol_split", n, colptr, rowval, nzval, nullptr, 2, split, merge, rng_state, out);
 }
 
 int acg_factor_dims(const acg_factor* f, int64_t* n, int64_t* nnz) {

@@ -22,6 +22,9 @@ void approx_chol_deg(int64_t n, const int64_t* colptr, const int64_t* rowval,
 // Elimination in a fixed order (perm: 1-based, null = 1..n); see acg_factor.cpp.
 void approx_chol_ord(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
                      const int64_t* perm, JuliaRng* rng, HostFactor& out);
+// The split/merge elimination of approxchol_lap2; see acg_factor.cpp.
+void approx_chol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                       int64_t split, int64_t merge, JuliaRng* rng, HostFactor& out);
 
 // Thread-local error text returned by acg_last_error().
 void set_last_error(const std::string& msg);

@@ -93,12 +93,13 @@ def quicksort(v, lo, hi, lt):
 # ---- ApproxCholPQ -------------------------------------------------------------
 
 class PQ:
-    def __init__(self, degs, n):
+    def __init__(self, degs, n, split=1):
         self.n = n
+        self.split = split
         self.prev = [0] * (n + 1)
         self.next = [0] * (n + 1)
         self.key = [0] * (n + 1)
-        self.lists = [0] * (2 * n + 2)
+        self.lists = [0] * (2 * split * n + 2)
         self.minlist = 1
         self.nitems = n
         for i in range(1, n + 1):
@@ -112,7 +113,7 @@ class PQ:
             self.lists[key] = i
 
     def keymap(self, x):
-        k, upper = self.n, 2 * self.n + 1
+        k, upper = self.split * self.n, 2 * self.split * self.n + 1
         return x if x <= k else min(upper, k + x // k)
 
     def pop(self):
@@ -410,3 +411,177 @@ def approx_chol_ord(colptr, rowval, nzval, rng: JuliaRng, perm=None):
         rowv = p[rowv - 1]
         d = d[np.asarray(invp[1:], np.int64) - 1]
     return col, np.array(ldcolptr, np.int64), rowv, np.array(ldfval, np.float64), d
+
+
+# ---- split/merge elimination: LLmatp(a, split) + approxChol(a, split, merge) ---
+
+def approx_chol_split(colptr, rowval, nzval, rng: JuliaRng, split=2, merge=2):
+    """approxChol(::LLmatp, split, merge) (src/approxChol.jl:979-1157) on
+    LLmatp(a, split) (src/approxChol.jl:138-183) with compressAvgCol!
+    (src/approxChol.jl:541-600).  colptr/rowval 1-based."""
+    n = len(colptr) - 1
+    m = colptr[n] - 1
+    # LLmatp(a, split): llelems[split*(ind-1)+k], k = 1..split
+    degs = [0] * (n + 1)
+    llelems = [None] * (split * m + 1)
+    cols = [None] * (n + 1)
+    for i in range(1, n + 1):
+        degs[i] = split * (colptr[i] - colptr[i - 1])
+        ind = colptr[i - 1]
+        j = rowval[ind - 1]
+        v = nzval[ind - 1] / split
+        llpend = LLp(j, v)
+        llelems[split * ind] = llpend
+        nxt = llpend
+        for k in range(1, split):
+            e = LLp(j, v)
+            e.next = nxt
+            llelems[split * (ind - 1) + k] = e
+            nxt = e
+        for ind in range(colptr[i - 1] + 1, colptr[i]):
+            j = rowval[ind - 1]
+            v = nzval[ind - 1] / split
+            for k in range(1, split + 1):
+                e = LLp(j, v)
+                e.next = nxt
+                llelems[split * (ind - 1) + k] = e
+                nxt = e
+        cols[i] = nxt
+    pos = {}
+    for c in range(1, n + 1):
+        for ind in range(colptr[c - 1], colptr[c]):
+            pos[(rowval[ind - 1], c)] = ind
+    for c in range(1, n + 1):
+        for ind in range(colptr[c - 1], colptr[c]):
+            flip = pos[(c, rowval[ind - 1])]
+            for k in range(1, split + 1):
+                llelems[split * (ind - 1) + k].reverse = llelems[split * (flip - 1) + k]
+
+    pq = PQ(degs, n, split)
+    col = [0] * (n - 1)
+    ldcolptr = [0] * n
+    ldrowval, ldfval = [], []
+    d = [0.0] * n
+    row_ptr = 1
+    it = 1
+    while it < n:
+        i = pq.pop()
+        col[it - 1] = i
+        ldcolptr[it - 1] = row_ptr
+        it += 1
+        cs = [None]
+        ll = cols[i]
+        while ll.next is not ll:
+            if ll.val > 0:
+                cs.append(ll)
+            ll = ll.next
+        if ll.val > 0:
+            cs.append(ll)
+        ln = len(cs) - 1
+        # compressAvgCol!
+        quicksort(cs, 1, ln, lambda x, y: x.row < y.row)
+        cur, nxt, ptr = 1, 1, 0
+        while nxt <= ln and cs[cur].row == cs[nxt].row:
+            nxt += 1
+        while cur <= ln:
+            num = nxt - cur
+            mul_sum = 0.0
+            for q in range(cur, nxt):
+                mul_sum += cs[q].val
+            if num <= merge:
+                nv = mul_sum / num
+                for q in range(cur, nxt):
+                    cs[q].val = nv
+                    cs[q].reverse.val = nv
+                    ptr += 1
+                    cs[ptr] = cs[q]
+            else:
+                nv = mul_sum / merge
+                for q in range(cur, cur + merge):
+                    cs[q].val = nv
+                    cs[q].reverse.val = nv
+                    ptr += 1
+                    cs[ptr] = cs[q]
+                currow = cs[cur].row
+                for q in range(cur + merge, nxt):
+                    cs[q].reverse.val = 0.0
+                    pq.dec(currow)
+            cur = nxt
+            while nxt <= ln and cs[cur].row == cs[nxt].row:
+                nxt += 1
+        ln = ptr
+        quicksort(cs, 1, ln, lambda x, y: (x.val, x.row) < (y.val, y.row))
+        vals = [0.0] * (ln + 1)
+        csum = 0.0
+        for q in range(1, ln + 1):
+            csum = csum + cs[q].val
+            vals[q] = cs[q].val
+        csr = [0.0] * (ln + 2)
+        crev = 0.0
+        for q in range(ln, 0, -1):
+            crev += cs[q].val
+            csr[q] = crev
+        wdeg = csum
+        col_scale = 1.0
+        next_edge = 1
+        final_d = 0.0
+        for jo in range(1, ln):
+            is_new = jo == next_edge
+            while next_edge <= ln and cs[jo].row == cs[next_edge].row:
+                next_edge += 1
+            if next_edge == ln + 1:
+                q = jo
+                while q <= ln - 1:
+                    e = cs[q]
+                    final_d += vals[q] * col_scale
+                    if it < n:
+                        pq.dec(e.row)
+                    e.reverse.val = 0.0
+                    q += 1
+                break
+            ll = cs[jo]
+            w = vals[jo] * col_scale
+            j = ll.row
+            revj = ll.reverse
+            f = w / wdeg
+            vals[jo] = 0.0
+            r = rng.rand() * csr[next_edge]
+            koff = 0  # searchsortedlast under the reverse order: last q with csr[q] >= r
+            for q in range(1, ln + 1):
+                if not (csr[q] < r):
+                    koff = q
+            k = cs[koff].row
+            pq.inc(k)
+            new_val = ll.val * csr[next_edge] / csum
+            revj.row = k
+            revj.val = new_val
+            revj.reverse = ll
+            khead = cols[k]
+            cols[k] = ll
+            ll.next = khead
+            ll.reverse = revj
+            ll.val = new_val
+            ll.row = j
+            if is_new:
+                ldrowval.append(j)
+                ldfval.append(f)
+                row_ptr += 1
+            else:
+                ldfval[-1] = ldfval[-1] + f
+            if jo == next_edge - 1:
+                f = ldfval[-1]
+                col_scale = col_scale * (1.0 - f)
+                wdeg = wdeg * ((1.0 - f) * (1.0 - f))
+        ll = cs[ln]
+        final_d += vals[ln] * col_scale
+        j = ll.row
+        if it < n:
+            pq.dec(j)
+        ll.reverse.val = 0.0
+        ldrowval.append(j)
+        ldfval.append(1.0)
+        row_ptr += 1
+        d[i - 1] = final_d
+    ldcolptr[it - 1] = row_ptr
+    return (np.array(col, np.int64), np.array(ldcolptr, np.int64), np.array(ldrowval, np.int64),
+            np.array(ldfval, np.float64), np.array(d, np.float64))

@@ -120,6 +120,33 @@ def test_given_order_eliminates_in_index_order():
     assert f.col.tolist() == list(range(1, a.shape[0]))
 
 
-def test_unknown_order_rejected():
-    with pytest.raises(ValueError):
-        acgpu.approx_chol(G.path_graph(4), acgpu.ApproxCholParams(order="bogus"))
+def test_other_orders_are_the_given_order():
+    # the reference's dispatch sends any order but :deg/:wdeg/:random to
+    # approxchol_lapGiven (src/approxChol.jl:1836-1850)
+    a = G.grid2(5)
+    acgpu.seed(3)
+    f1 = acgpu.approx_chol(a, acgpu.ApproxCholParams(order="bogus"))
+    acgpu.seed(3)
+    f2 = acgpu.approx_chol(a, acgpu.ApproxCholParams(order="given"))
+    assert np.array_equal(f1.fval, f2.fval) and np.array_equal(f1.rowval, f2.rowval)
+
+
+def _ref_split(a, seed, split, merge):
+    a = acgpu.solvers._csc(a)
+    cp = (a.indptr + 1).tolist()
+    rv = (a.indices + 1).tolist()
+    return approxchol_ref.approx_chol_split(cp, rv, a.data.tolist(), JuliaRng(seed), split, merge)
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("split,merge", [(2, 2), (3, 2), (2, 1)])
+def test_split_merge_factor_matches_restatement(name, make, split, merge):
+    a = make()
+    ref = _ref_split(a, 5, split, merge)
+    acgpu.seed(5)
+    f = acgpu.approx_chol(a, acgpu.ApproxCholParams("deg", 5, split, merge))
+    got = (f.col, f.colptr, f.rowval, f.fval, f.d)
+    for x, y, what in zip(got, ref, ("col", "colptr", "rowval", "fval", "d")):
+        assert np.array_equal(np.asarray(x), np.asarray(y)), what
+    n = a.shape[0]
+    assert len(set(f.col.tolist())) == n - 1 and f.colptr[-1] - 1 == f.fval.shape[0]

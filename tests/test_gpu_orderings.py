@@ -34,3 +34,23 @@ def test_orderings_solve(gpu_ok, order):
     f = acgpu.approxchol_lap(a, tol=1e-8, params=params, precision="mixed")
     x = f(b)
     assert O.relres(a, x, b - b.mean()) <= 1e-8 * 1.01
+
+
+def test_approxchol_lap2(gpu_ok):
+    """approxchol_lap2: the split/merge factor (src/approxChol.jl:1559-1578)
+    through the same GPU solve."""
+    a = G.grid3(14, weights="loguniform", seed=12)
+    params = acgpu.ApproxCholParams("deg", 5, 2, 2)
+    acgpu.seed(6)
+    ldli = acgpu.approx_chol(a, params)
+    dev = acgpu.DeviceLapSolver(a, ldli, params=params)
+    r = np.random.default_rng(3).standard_normal(a.shape[0])
+    r -= r.mean()
+    y = O.ldlsolve(ldli, r)
+    assert np.linalg.norm(dev.ldlsolve(r) - y) / np.linalg.norm(y) < 1e-12
+    dev.close()
+    b = np.random.default_rng(4).standard_normal(a.shape[0])
+    acgpu.seed(6)
+    f = acgpu.approxchol_lap2(a, tol=1e-8, precision="mixed")
+    x = f(b)
+    assert O.relres(a, x, b - b.mean()) <= 1e-8 * 1.01
