@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kVecThreads) kg_pq(const T* __restrict__ p, co
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) kg_update(int n, T* x3, const T* __restrict__ p, const T* __restrict__ q,
                                                          T* __restrict__ r, T* __restrict__ s_out, T* __restrict__ y_out,
-                                                         GroupArgs g, LoopCtl ctl) {
+                                                         GroupArgs g, LoopCtl ctl, int vs) {
   if (g.gst->done) return;
   const SegChunk c = g.chunks[blockIdx.x];
   const PcgState* sc = &g.st[c.seg];
@@ -128,8 +128,8 @@ __global__ void __launch_bounds__(kVecThreads) kg_update(int n, T* x3, const T* 
   const T pend = pending_value<T>();
   double acc[3] = {0.0, 0.0, 0.0};
   for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
-    s_out[i] = pend;
-    y_out[i] = pend;
+    s_out[(size_t)i * vs] = pend;
+    y_out[(size_t)i * vs] = pend;
     if (!act) continue;
     const T xv = (T)((double)xc[i] + al * (double)p[i]);
     const T rv = (T)((double)r[i] + (-al) * (double)q[i]);
@@ -147,11 +147,11 @@ __global__ void __launch_bounds__(kVecThreads) kg_update(int n, T* x3, const T* 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) kg_ysum(const T* __restrict__ y, GroupArgs g, LoopCtl ctl) {
+__global__ void __launch_bounds__(kVecThreads) kg_ysum(const T* __restrict__ y, GroupArgs g, LoopCtl ctl, int vs) {
   if (g.gst->done) return;
   const SegChunk c = g.chunks[blockIdx.x];
   double acc[1] = {0.0};
-  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) acc[0] += (double)y[i];
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) acc[0] += (double)y[(size_t)i * vs];
   double tot[1];
   if (seg_reduce<1>(acc, c, g, 2, tot) && threadIdx.x == 0) {
     PcgState* s = &g.st[c.seg];
@@ -165,14 +165,14 @@ __global__ void __launch_bounds__(kVecThreads) kg_ysum(const T* __restrict__ y, 
 
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) kg_zdot(T* __restrict__ yz, const T* __restrict__ r, T* __restrict__ p,
-                                                       GroupArgs g, double eps, int init, LoopCtl ctl) {
+                                                       GroupArgs g, double eps, int init, LoopCtl ctl, int vs) {
   if (g.gst->done) return;
   const SegChunk c = g.chunks[blockIdx.x];
   const double mu = g.st[c.seg].mean;
   double acc[2] = {0.0, 0.0};
   for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
-    const T z = (T)((double)yz[i] - mu);
-    yz[i] = z;
+    const T z = (T)((double)yz[(size_t)i * vs] - mu);
+    yz[(size_t)i * vs] = z;
     if (init) p[i] = z;
     acc[0] += (double)z * (double)r[i];
     acc[1] += fabs((double)z);
@@ -185,13 +185,15 @@ __global__ void __launch_bounds__(kVecThreads) kg_zdot(T* __restrict__ yz, const
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) kg_pupdate(const T* __restrict__ z, T* __restrict__ p, GroupArgs g) {
+__global__ void __launch_bounds__(kVecThreads) kg_pupdate(const T* __restrict__ z, T* __restrict__ p, GroupArgs g,
+                                                          int vs) {
   if (g.gst->done) return;
   const SegChunk c = g.chunks[blockIdx.x];
   const PcgState* s = &g.st[c.seg];
   if (s->done) return;
   const double beta = s->beta;
-  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) p[i] = (T)((double)z[i] + beta * (double)p[i]);
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x)
+    p[i] = (T)((double)z[(size_t)i * vs] + beta * (double)p[i]);
 }
 
 // b_int = b_ext[perm]; per-graph sums -> means.  Block 0 also clears the group flags.
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(kVecThreads) kg_gather_in(const int* __restric
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) kg_center(double* __restrict__ bm, T* __restrict__ r, T* __restrict__ x0,
                                                          T* __restrict__ s_out, T* __restrict__ y_out, GroupArgs g,
-                                                         LoopCtl ctl) {
+                                                         LoopCtl ctl, int vs) {
   const SegChunk c = g.chunks[blockIdx.x];
   const double mu = g.st[c.seg].mean;
   const T pend = pending_value<T>();
@@ -227,8 +229,8 @@ __global__ void __launch_bounds__(kVecThreads) kg_center(double* __restrict__ bm
     bm[i] = v;
     r[i] = (T)v;
     x0[i] = T(0);
-    s_out[i] = pend;
-    y_out[i] = pend;
+    s_out[(size_t)i * vs] = pend;
+    y_out[(size_t)i * vs] = pend;
     acc[0] += v * v;
     acc[1] += fabs(v);
   }
