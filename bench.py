@@ -13,9 +13,10 @@ reference's :deg elimination (not timed; its time is reported as factor_s).
 
 Metric: solves/s (whole job; replicas: each GPU solves its own right-hand
 sides on its own copy of the factor, no collective on the data path).
-`value` times device-resident inputs; `e2e` goes through the C ABI entry
-acg_solve with pinned host buffers, host<->device copies inside the timed
-region.  --impl reference times the CPU restatement of the reference's
+`value` times device-resident inputs; `e2e` goes through the C ABI entries
+acg_solve_async / acg_wait with pinned host buffers, every step's
+host<->device copies inside the timed region (two steps in flight: one step's
+copies overlap the previous step's solve).  --impl reference times the CPU restatement of the reference's
 solve (pcg + LDLsolver, single-threaded per solve) on all host cores.
 """
 from __future__ import annotations
@@ -245,28 +246,49 @@ def run_acgpu(args):
     refs = np.array([r[1] for r in results], dtype=float)
     res = np.array([r[2] for r in results])
 
-    # end to end: pinned host blocks through acg_solve (H2D + D2H inside the timed region)
+    # end to end: pinned host blocks through the asynchronous C entry
+    # (acg_solve_async / acg_wait), every step's H2D and D2H inside the timed
+    # region; two requests in flight, so one step's copies overlap the
+    # previous step's solve
     hb = torch.empty((args.steps, k, n), dtype=torch.float64, pin_memory=True)
-    hx = torch.empty((k, n), dtype=torch.float64, pin_memory=True)
+    hx = torch.empty((2, k, n), dtype=torch.float64, pin_memory=True)
     hb_np = hb.numpy()
-    hx_np = hx.numpy()
     for i in range(args.steps):
         for c in range(k):
             hb_np[i, c] = rhs(n, 5_000_000 + 1_000_000 * rank + 1000 * i + c)
-    hb_flat = [np.ascontiguousarray(hb_np[i]).reshape(-1) for i in range(args.steps)]
-    hx_flat = hx_np.reshape(-1)
-    check(L.acg_solve(dev._h, hb_flat[0], hx_flat, k, n, TOL, MAXITS, float("inf"), 5, prec, infos))
+    e2e_bad = []
+
+    def submit(i):
+        req = ctypes.c_void_p()
+        check(L.acg_solve_async(dev._h, hb[i].data_ptr(), hx[i % 2].data_ptr(), k, n, TOL, MAXITS, float("inf"), 5,
+                                prec, ctypes.byref(req)))
+        return req
+
+    def finish(req):
+        check(L.acg_wait(req, infos))
+        e2e_bad.extend(c for c in range(k) if infos[c].status != 0 or infos[c].true_relres > TOL)
+
+    for req in [submit(0), submit(min(1, args.steps - 1))]:  # builds both slots' graphs
+        finish(req)
+    e2e_bad.clear()
     barrier(world)
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     e2.record()
+    inflight = []
     for i in range(args.steps):
-        check(L.acg_solve(dev._h, hb_flat[i], hx_flat, k, n, TOL, MAXITS, float("inf"), 5, prec, infos))
+        inflight.append(submit(i))
+        if len(inflight) == 2:
+            finish(inflight.pop(0))
+    while inflight:
+        finish(inflight.pop(0))
     e3.record()
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = max_over_ranks(e2.elapsed_time(e3), world)
+    if e2e_bad:
+        raise RuntimeError(f"{len(e2e_bad)} end-to-end solves missed the tolerance")
 
     # one right-hand side alone: latency of a single solve
     single = []

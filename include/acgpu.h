@@ -199,6 +199,26 @@ int acg_solver_stats(const acg_solver* h, acg_stats* out);
  * Returns 0 (all converged), the largest ACG_STOP_* code, or an error (<0). */
 int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol, int64_t maxits,
               double maxtime, int stag_test, int precision, acg_solve_info* info);
+/* ---- asynchronous solves (serving) ---------------------------------------
+ * acg_solve_async enqueues one batched solve of 1 <= nrhs <= 64 columns of b
+ * (column-major, ldb >= n; x has the same layout) and returns at once with a
+ * request.  A solver runs its requests in submission order; while one solves,
+ * the next one's copy in and the previous one's copy out proceed on their own
+ * streams (two requests in flight per solver: a third submit first waits for
+ * the oldest to finish).  b and x must stay valid until acg_wait; copies run
+ * asynchronously for page-locked b and x, and x in pageable memory is filled
+ * by acg_wait.  acg_poll returns 1 when the request has finished (acg_wait
+ * will not block), 0 while it runs, < 0 on error.  acg_wait blocks until the
+ * request has finished, fills info[nrhs] (optional), frees the request and
+ * returns what acg_solve would have.  Requests still open when their solver
+ * is destroyed are finished first and may still be waited.  The reference
+ * has no asynchronous entry: its closure solves one vector per call
+ * (src/approxChol.jl:1624, src/pcg.jl:256). */
+typedef struct acg_request acg_request;
+int acg_solve_async(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol,
+                    int64_t maxits, double maxtime, int stag_test, int precision, acg_request** out);
+int acg_poll(acg_request* r);
+int acg_wait(acg_request* r, acg_solve_info* info);
 /* As acg_solve for one right-hand side already in device memory. */
 int acg_solve_device(acg_solver* h, const double* b_dev, double* x_dev, double tol, int64_t maxits, double maxtime,
                      int stag_test, int precision, acg_solve_info* info);

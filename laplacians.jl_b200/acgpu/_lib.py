@@ -93,6 +93,11 @@ SIGNATURES = [
     ("acg_solve_batch_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                               ctypes.c_int64, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
                                               ctypes.c_int, ctypes.c_int, ctypes.POINTER(AcgSolveInfo)]),
+    ("acg_solve_async", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                       ctypes.c_int64, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
+                                       ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("acg_poll", ctypes.c_int, [ctypes.c_void_p]),
+    ("acg_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AcgSolveInfo)]),
     ("acg_ldlsolve", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_int]),
     ("acg_lap_mul", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_int]),
     ("acg_time_kernels", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,

@@ -283,6 +283,27 @@ class DeviceLapSolver:
         x = X.T.reshape(b.shape)
         return x
 
+    def solve_async(self, b, tol=None, maxits=None, maxtime=None, precision=None) -> "AsyncSolve":
+        """Enqueue the solve of b (n, or n x k with k <= 64) and return at once
+        (acg_solve_async).  The solver runs its requests in order, overlapping
+        one request's host copies with another's solve."""
+        d = self.defaults
+        tol = d["tol"] if tol is None else tol
+        maxits = d["maxits"] if maxits is None else maxits
+        maxtime = d["maxtime"] if maxtime is None else maxtime
+        precision = d["precision"] if precision is None else precision
+        b = np.asarray(b, dtype=np.float64)
+        if b.shape[0] != self.n:
+            raise ValueError(f"rhs has {b.shape[0]} rows, solver has {self.n}")
+        cols = b.reshape(self.n, -1)
+        B = np.ascontiguousarray(cols.T)
+        X = np.empty_like(B)
+        req = ctypes.c_void_p()
+        check(lib().acg_solve_async(self._h, B.ctypes.data, X.ctypes.data, B.shape[0], self.n, float(tol),
+                                    _maxits_int(maxits), float(maxtime), int(self.params.stag_test),
+                                    _PRECISIONS[precision], ctypes.byref(req)))
+        return AsyncSolve(req, B, X, b.shape)
+
     # one-shot device operations used by the parity tests
     def ldlsolve(self, r, precision="fp64"):
         r = np.ascontiguousarray(r, dtype=np.float64)
@@ -305,6 +326,40 @@ class DeviceLapSolver:
         y = np.empty_like(x)
         check(lib().acg_lap_mul(self._h, x, y, _PRECISIONS[precision]))
         return y
+
+
+class AsyncSolve:
+    """A solve enqueued by DeviceLapSolver.solve_async.  Holds its right-hand
+    sides and solution block until wait() (the library reads and writes them
+    asynchronously)."""
+
+    def __init__(self, req, B, X, shape):
+        self._req = req
+        self._B, self._X, self._shape = B, X, shape
+        self._lib = lib()
+        self.info: list[AcgSolveInfo] = []
+        self.rc = None
+
+    def done(self) -> bool:
+        """True once the solve has finished (wait() will not block)."""
+        if self._req is None:
+            return True
+        return check(self._lib.acg_poll(self._req)) == 1
+
+    def wait(self):
+        """Block until the solve has finished; returns x shaped like b."""
+        if self._req is not None:
+            k = self._X.shape[0]
+            infos = (AcgSolveInfo * k)()
+            req, self._req = self._req, None
+            self.rc = check(self._lib.acg_wait(req, infos))
+            self.info = list(infos)
+        return self._X.T.reshape(self._shape)
+
+    def __del__(self):
+        if getattr(self, "_req", None) is not None:
+            self._lib.acg_wait(self._req, None)
+            self._req = None
 
 
 class GroupSolver:

@@ -79,34 +79,24 @@ __device__ __forceinline__ bool row_pending(const Row<T, CPL>& r) {
 }
 
 // Slow path: poll the row (in L2) until no value is pending or the bound is
-// hit; returns false when the wait gave up.  Keeps the caller's row in
-// registers (the caller reloads it).
+// hit.  Returns the row as the last poll saw it, ready (rows are written once
+// per sweep, so no second load is needed), or zeros when the wait gave up.
 template <typename T, int CPL>
-__device__ __noinline__ bool wait_row_ready(const T* p, BatchShared* bs) {
+__device__ __noinline__ Row<T, CPL> wait_row_slow(const T* p, BatchShared* bs) {
+  Row<T, CPL> r;
   for (unsigned int spins = 1;; ++spins) {
     if (spins >= 64) __nanosleep(64);
-    Row<T, CPL> r;
     ld_row<CPL>(r, p);
-    if (!row_pending(r)) return true;
-    if ((spins & 1023u) == 0 && *((volatile int*)&bs->sweep_error)) return false;
+    if (!row_pending(r)) return r;
+    if ((spins & 1023u) == 0 && *((volatile int*)&bs->sweep_error)) break;
     if (spins >= kSpinLimit) {
       atomicExch(&bs->sweep_error, 1);
-      return false;
+      break;
     }
   }
-}
-
-template <typename T, int CPL>
-__device__ __forceinline__ void wait_row(Row<T, CPL>& r, const T* p, BatchShared* bs) {
-  ld_row<CPL>(r, p);
-  if (row_pending(r)) {
-    if (wait_row_ready<T, CPL>(p, bs)) {
-      ld_row<CPL>(r, p);
-    } else {
 #pragma unroll
-      for (int j = 0; j < CPL; ++j) r.v[j] = T(0);
-    }
-  }
+  for (int j = 0; j < CPL; ++j) r.v[j] = T(0);
+  return r;
 }
 
 template <int CPL>
@@ -216,15 +206,7 @@ __global__ void __launch_bounds__(kSweepThreads) kb_sweep(int ntasks, const Swee
 #pragma unroll
         for (int u = 0; u < EB; ++u) {
           if (ids[u] < 0) continue;
-          if (row_pending(vals[u])) {
-            const T* pr = out + (size_t)ids[u] * kp + gl * CPL;
-            if (wait_row_ready<T, CPL>(pr, bs)) {
-              ld_row<CPL>(vals[u], pr);
-            } else {
-#pragma unroll
-              for (int q = 0; q < CPL; ++q) vals[u].v[q] = T(0);
-            }
-          }
+          if (row_pending(vals[u])) vals[u] = wait_row_slow<T, CPL>(out + (size_t)ids[u] * kp + gl * CPL, bs);
 #pragma unroll
           for (int q = 0; q < CPL; ++q) acc[q] += cs[u] * vals[u].v[q];
         }

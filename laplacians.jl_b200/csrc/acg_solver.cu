@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -138,7 +139,8 @@ struct SolverImpl {
 
   // batched solves: kp right-hand sides per launch (vertex-major n x kp blocks)
   int batch_kp = 0;  // capacity of the batch buffers
-  DevBuf<double> bb_ext, bx_ext, bbm, br64, bxf, bpartials;
+  DevBuf<double> bb_ext[2], bx_ext[2];  // external-order blocks, one pair per slot (slot 1: asynchronous solves)
+  DevBuf<double> bbm, br64, bxf, bpartials;
   DevBuf<float> br32, bs32, by32, bp32, bq32, bx3_32;
   DevBuf<double> bs64, by64, bp64, bq64, bx3_64;
   PcgState* bst = nullptr;
@@ -159,14 +161,40 @@ struct SolverImpl {
   size_t dt_part_cols = 0;               // columns dt_part holds
   int ntasks_bb = 0, ntasks_fb = 0;      // task tables of the batched sweeps
   DevBuf<SweepTask> tasks_bb, tasks_fb;
-  cudaGraphExec_t bexec[2][4] = {};
+  cudaGraphExec_t bexec[2][2][4] = {};  // [slot][precision][log2(kp/8)]
+
+  // asynchronous batched solves (acg_solve_async): two slots, each with its
+  // own external blocks and graphs, so that one request's host copies run
+  // while the other request solves.  Copies in run on h2d_stream, copies out
+  // on d2h_stream, solves on `stream`.
+  struct AsyncSlot {
+    cudaEvent_t h2d = nullptr, start = nullptr, done = nullptr, d2h = nullptr;
+    PcgState* h_init = nullptr;    // pinned: the request's initial column states
+    PcgState* h_out = nullptr;     // pinned: its final column states
+    BatchShared* h_bsh = nullptr;  // pinned
+    acg_request* owner = nullptr;  // request whose results are not yet collected
+  };
+  bool async_on = false;
+  cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
+  AsyncSlot slots[2];
+  int next_slot = 0;
 
   ~SolverImpl() {
     for (auto& e : exec)
       if (e) cudaGraphExecDestroy(e);
-    for (auto& row : bexec)
-      for (auto& e : row)
-        if (e) cudaGraphExecDestroy(e);
+    for (auto& per_slot : bexec)
+      for (auto& row : per_slot)
+        for (auto& e : row)
+          if (e) cudaGraphExecDestroy(e);
+    for (AsyncSlot& a : slots) {
+      for (cudaEvent_t e : {a.h2d, a.start, a.done, a.d2h})
+        if (e) cudaEventDestroy(e);
+      if (a.h_init) cudaFreeHost(a.h_init);
+      if (a.h_out) cudaFreeHost(a.h_out);
+      if (a.h_bsh) cudaFreeHost(a.h_bsh);
+    }
+    if (h2d_stream) cudaStreamDestroy(h2d_stream);
+    if (d2h_stream) cudaStreamDestroy(d2h_stream);
     if (bst) cudaFree(bst);
     if (bsh) cudaFree(bsh);
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -1364,7 +1392,7 @@ void enqueue_biteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* y, 
 }
 
 template <int CPL>
-cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S) {
+cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S, int slot) {
   constexpr int kp = CPL * kBatchLanes;
   cudaStream_t s = S.stream;
   const int n = S.n;
@@ -1376,7 +1404,7 @@ cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S) {
   LoopCtl ctl{h, 1};
   double* x3 = S.bx3_64.p;
   begin_into(s, top, {});
-  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bb_ext.p, (long long)n, S.bbm.p, S.bst, S.bsh,
+  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bb_ext[slot].p, (long long)n, S.bbm.p, S.bst, S.bsh,
                                                   S.bpartials.p);
   kb_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, x3, S.bs64.p, S.by64.p, S.bst,
                                                        S.bsh, S.bpartials.p, ctl);
@@ -1395,7 +1423,7 @@ cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S) {
   kb_take_best<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, x3, S.bxf.p, S.bst);
   kb_true_residual<CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.bxf.p, S.bbm.p,
                                                            nullptr, S.bst, S.bsh, S.bpartials.p);
-  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, S.bx_ext.p, (long long)n, S.bsh);
+  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, S.bx_ext[slot].p, (long long)n, S.bsh);
   end_into(s);
   (void)N;
   cudaGraphExec_t exec;
@@ -1405,7 +1433,7 @@ cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S) {
 }
 
 template <int CPL>
-cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S) {
+cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S, int slot) {
   constexpr int kp = CPL * kBatchLanes;
   cudaStream_t s = S.stream;
   const int n = S.n;
@@ -1416,7 +1444,7 @@ cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S) {
   ACG_CUDA(cudaGraphConditionalHandleCreate(&ho, top, 1u, cudaGraphCondAssignDefault));
   LoopCtl octl{ho, 1};
   begin_into(s, top, {});
-  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bb_ext.p, (long long)n, S.bbm.p, S.bst, S.bsh,
+  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bb_ext[slot].p, (long long)n, S.bbm.p, S.bst, S.bsh,
                                                   S.bpartials.p);
   kb_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, S.bxf.p, (double*)nullptr,
                                                        (double*)nullptr, S.bst, S.bsh, S.bpartials.p, octl);
@@ -1448,7 +1476,7 @@ cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S) {
   kb_outer_decide<<<1, kMaxBatch, 0, s>>>(S.bst, S.bsh, kp, octl);
   end_into(s);
   begin_into(s, top, {onode});
-  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, S.bx_ext.p, (long long)n, S.bsh);
+  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, S.bx_ext[slot].p, (long long)n, S.bsh);
   end_into(s);
   cudaGraphExec_t exec;
   ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
@@ -1501,14 +1529,19 @@ void ensure_batch(SolverImpl& S, int kp) {
   }
   if (kp <= S.batch_kp) return;
   // growing the buffers invalidates every captured batch graph
-  for (auto& row : S.bexec)
-    for (auto& e : row)
-      if (e) {
-        cudaGraphExecDestroy(e);
-        e = nullptr;
-      }
+  for (auto& per_slot : S.bexec)
+    for (auto& row : per_slot)
+      for (auto& e : row)
+        if (e) {
+          cudaGraphExecDestroy(e);
+          e = nullptr;
+        }
   const size_t N = (size_t)S.n * kp;
-  for (DevBuf<double>* b : {&S.bb_ext, &S.bx_ext, &S.bbm, &S.br64, &S.bxf, &S.bs64, &S.by64, &S.bp64, &S.bq64})
+  if (S.async_on) {
+    S.bb_ext[1].alloc(N);
+    S.bx_ext[1].alloc(N);
+  }
+  for (DevBuf<double>* b : {&S.bb_ext[0], &S.bx_ext[0], &S.bbm, &S.br64, &S.bxf, &S.bs64, &S.by64, &S.bp64, &S.bq64})
     b->alloc(N);
   S.bx3_64.alloc(3 * N);
   for (DevBuf<float>* b : {&S.br32, &S.bs32, &S.by32, &S.bp32, &S.bq32}) b->alloc(N);
@@ -1516,24 +1549,7 @@ void ensure_batch(SolverImpl& S, int kp) {
   S.batch_kp = kp;
 }
 
-// Solve k <= 64 right-hand sides (column-major, leading dimensions ldb/ldx)
-// in one batched graph launch.
-int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t ldx, int k, cudaMemcpyKind kin,
-                cudaMemcpyKind kout, double tol, int64_t maxits, double maxtime, int stag_test, int precision,
-                acg_solve_info* info) {
-  cudaStream_t s = S.stream;
-  const int kp = round_kp(k);
-  std::unique_lock<std::recursive_mutex> glk(g_device_mu);
-  ensure_batch(S, std::max(kp, S.batch_kp));
-  cudaGraphExec_t& ge = S.bexec[precision][kp_index(kp)];
-  if (!ge) {
-    with_cpl(kp, [&](auto cpl) {
-      constexpr int C = decltype(cpl)::value;
-      ge = precision == 0 ? build_batch_fp64_graph<C>(S) : build_batch_mixed_graph<C>(S);
-    });
-  }
-  glk.unlock();
-  PcgState* h = S.h_bst;
+void init_batch_states(PcgState* h, int kp, double tol, int64_t maxits, double maxtime, int stag_test) {
   std::memset(h, 0, sizeof(PcgState) * kMaxBatch);
   for (int c = 0; c < kp; ++c) {
     h[c].tol = tol;
@@ -1546,26 +1562,10 @@ int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t 
     h[c].max_outer = 40;
     h[c].inner_tol = std::min(0.25, std::max(h[c].min_inner_tol, 0.5 * tol));
   }
-  BatchShared hb = {};
-  hb.k = k;
-  ACG_CUDA(cudaMemcpyAsync(S.bst, h, sizeof(PcgState) * kp, cudaMemcpyHostToDevice, s));
-  ACG_CUDA(cudaMemcpyAsync(S.bsh, &hb, sizeof(BatchShared), cudaMemcpyHostToDevice, s));
-  ACG_CUDA(cudaMemcpy2DAsync(S.bb_ext.p, sizeof(double) * S.n, B, sizeof(double) * ldb, sizeof(double) * S.n, k, kin,
-                             s));
-  cudaEvent_t e0, e1;
-  ACG_CUDA(cudaEventCreate(&e0));
-  ACG_CUDA(cudaEventCreate(&e1));
-  ACG_CUDA(cudaEventRecord(e0, s));
-  ACG_CUDA(cudaGraphLaunch(ge, s));
-  ACG_CUDA(cudaEventRecord(e1, s));
-  ACG_CUDA(cudaMemcpy2DAsync(X, sizeof(double) * ldx, S.bx_ext.p, sizeof(double) * S.n, sizeof(double) * S.n, k, kout,
-                             s));
-  ACG_CUDA(cudaMemcpyAsync(h, S.bst, sizeof(PcgState) * kp, cudaMemcpyDeviceToHost, s));
-  ACG_CUDA(cudaStreamSynchronize(s));
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+}
+
+// Per-column results of a batched solve; returns the worst column's code.
+int batch_results(int levels, const PcgState* h, int k, int precision, float ms, acg_solve_info* info) {
   int worst = 0;
   for (int c = 0; c < k; ++c) {
     if (info) {
@@ -1576,13 +1576,63 @@ int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t 
       info[c].true_relres = h[c].nr_true;
       info[c].solve_ms = ms;
       info[c].status = h[c].status;
-      info[c].levels = S.nlev;
+      info[c].levels = levels;
     }
     const int rc = status_to_rc(h[c].status);
     if (rc < 0) return rc;
     worst = std::max(worst, rc);
   }
   return worst;
+}
+
+cudaGraphExec_t& batch_graph(SolverImpl& S, int slot, int precision, int kp) {
+  cudaGraphExec_t& ge = S.bexec[slot][precision][kp_index(kp)];
+  if (!ge) {
+    with_cpl(kp, [&](auto cpl) {
+      constexpr int C = decltype(cpl)::value;
+      ge = precision == 0 ? build_batch_fp64_graph<C>(S, slot) : build_batch_mixed_graph<C>(S, slot);
+    });
+  }
+  return ge;
+}
+
+void drain_async(SolverImpl& S);
+
+// Solve k <= 64 right-hand sides (column-major, leading dimensions ldb/ldx)
+// in one batched graph launch.
+int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t ldx, int k, cudaMemcpyKind kin,
+                cudaMemcpyKind kout, double tol, int64_t maxits, double maxtime, int stag_test, int precision,
+                acg_solve_info* info) {
+  cudaStream_t s = S.stream;
+  const int kp = round_kp(k);
+  drain_async(S);  // the asynchronous slots share the batch buffers
+  std::unique_lock<std::recursive_mutex> glk(g_device_mu);
+  ensure_batch(S, std::max(kp, S.batch_kp));
+  cudaGraphExec_t ge = batch_graph(S, 0, precision, kp);
+  glk.unlock();
+  PcgState* h = S.h_bst;
+  init_batch_states(h, kp, tol, maxits, maxtime, stag_test);
+  BatchShared hb = {};
+  hb.k = k;
+  ACG_CUDA(cudaMemcpyAsync(S.bst, h, sizeof(PcgState) * kp, cudaMemcpyHostToDevice, s));
+  ACG_CUDA(cudaMemcpyAsync(S.bsh, &hb, sizeof(BatchShared), cudaMemcpyHostToDevice, s));
+  ACG_CUDA(cudaMemcpy2DAsync(S.bb_ext[0].p, sizeof(double) * S.n, B, sizeof(double) * ldb, sizeof(double) * S.n, k,
+                             kin, s));
+  cudaEvent_t e0, e1;
+  ACG_CUDA(cudaEventCreate(&e0));
+  ACG_CUDA(cudaEventCreate(&e1));
+  ACG_CUDA(cudaEventRecord(e0, s));
+  ACG_CUDA(cudaGraphLaunch(ge, s));
+  ACG_CUDA(cudaEventRecord(e1, s));
+  ACG_CUDA(cudaMemcpy2DAsync(X, sizeof(double) * ldx, S.bx_ext[0].p, sizeof(double) * S.n, sizeof(double) * S.n, k,
+                             kout, s));
+  ACG_CUDA(cudaMemcpyAsync(h, S.bst, sizeof(PcgState) * kp, cudaMemcpyDeviceToHost, s));
+  ACG_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return batch_results(S.nlev, h, k, precision, ms, info);
 }
 
 // ============================================================================
@@ -1834,6 +1884,7 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
 }
 
 void time_batch(SolverImpl& S, int precision, int kp, int reps, acg_kernel_times* out) {
+  drain_async(S);
   ensure_batch(S, std::max(kp, S.batch_kp));
   with_cpl(kp, [&](auto cpl) {
     constexpr int C = decltype(cpl)::value;
@@ -1851,6 +1902,129 @@ void time_batch(SolverImpl& S, int precision, int kp, int reps, acg_kernel_times
 struct acg_solver {
   acg::SolverImpl impl;
 };
+
+// A batched solve enqueued by acg_solve_async.  Its results (the columns'
+// final states, the solve time) are copied here when the request is collected:
+// by acg_wait, or earlier when its slot is needed by a later request.
+struct acg_request {
+  acg_solver* h = nullptr;  // null once the solver was destroyed (the results were collected first)
+  int slot = 0, k = 0, kp = 0, precision = 0, levels = 0;
+  double* x = nullptr;  // host destination
+  int64_t ldx = 0;
+  bool pinned_x = false;  // page-locked: copied by d2h_stream, else at collection
+  bool collected = false;
+  int rc = ACG_OK;        // a failure met while collecting
+  float ms = 0.f;
+  acg::PcgState st[acg::kMaxBatch];
+};
+
+namespace acg {
+namespace {
+
+void ensure_async(SolverImpl& S) {
+  if (S.async_on) return;
+  ACG_CUDA(cudaStreamCreateWithFlags(&S.h2d_stream, cudaStreamNonBlocking));
+  ACG_CUDA(cudaStreamCreateWithFlags(&S.d2h_stream, cudaStreamNonBlocking));
+  for (SolverImpl::AsyncSlot& a : S.slots) {
+    ACG_CUDA(cudaEventCreateWithFlags(&a.h2d, cudaEventDisableTiming));
+    ACG_CUDA(cudaEventCreate(&a.start));
+    ACG_CUDA(cudaEventCreate(&a.done));
+    ACG_CUDA(cudaEventCreateWithFlags(&a.d2h, cudaEventDisableTiming));
+    ACG_CUDA(cudaMallocHost(&a.h_init, sizeof(PcgState) * kMaxBatch));
+    ACG_CUDA(cudaMallocHost(&a.h_out, sizeof(PcgState) * kMaxBatch));
+    ACG_CUDA(cudaMallocHost(&a.h_bsh, sizeof(BatchShared)));
+  }
+  if (S.batch_kp) {
+    const size_t N = (size_t)S.n * S.batch_kp;
+    S.bb_ext[1].alloc(N);
+    S.bx_ext[1].alloc(N);
+  }
+  S.async_on = true;
+}
+
+// Wait for the slot's request to finish and copy its results into it.
+void collect(SolverImpl& S, int slot) {
+  SolverImpl::AsyncSlot& a = S.slots[slot];
+  acg_request* r = a.owner;
+  if (!r) return;
+  a.owner = nullptr;
+  r->collected = true;
+  cudaError_t e = cudaEventSynchronize(a.d2h);
+  if (e == cudaSuccess && !r->pinned_x)
+    e = cudaMemcpy2D(r->x, sizeof(double) * r->ldx, S.bx_ext[slot].p, sizeof(double) * S.n, sizeof(double) * S.n,
+                     r->k, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_last_error(std::string("asynchronous solve: ") + cudaGetErrorString(e));
+    r->rc = ACG_ERR_CUDA;
+    return;
+  }
+  std::memcpy(r->st, a.h_out, sizeof(PcgState) * r->kp);
+  cudaEventElapsedTime(&r->ms, a.start, a.done);
+}
+
+void drain_async(SolverImpl& S) {
+  if (!S.async_on) return;
+  collect(S, 0);
+  collect(S, 1);
+}
+
+// Enqueue one batched solve of k <= 64 columns from host memory: the copy in
+// on h2d_stream, the graph on the solver's stream, the copy out on
+// d2h_stream, chained by events.  A slot is reused only after its previous
+// request was collected, so its blocks and pinned states are free.
+int submit_async(acg_solver* h, const double* B, double* X, int k, int64_t ld, double tol, int64_t maxits,
+                 double maxtime, int stag_test, int precision, acg_request** out) {
+  SolverImpl& S = h->impl;
+  const int kp = round_kp(k);
+  std::unique_lock<std::recursive_mutex> glk(g_device_mu);
+  ensure_async(S);
+  if (kp > S.batch_kp) drain_async(S);  // growing the blocks frees the ones in flight
+  ensure_batch(S, std::max(kp, S.batch_kp));
+  const int slot = S.next_slot;
+  SolverImpl::AsyncSlot& a = S.slots[slot];
+  collect(S, slot);
+  cudaGraphExec_t ge = batch_graph(S, slot, precision, kp);
+  glk.unlock();
+  auto req = std::make_unique<acg_request>();
+  req->h = h;
+  req->slot = slot;
+  req->k = k;
+  req->kp = kp;
+  req->precision = precision;
+  req->levels = S.nlev;
+  req->x = X;
+  req->ldx = ld;
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, X) == cudaSuccess) req->pinned_x = pa.type == cudaMemoryTypeHost;
+  else cudaGetLastError();
+  init_batch_states(a.h_init, kp, tol, maxits, maxtime, stag_test);
+  *a.h_bsh = BatchShared{};
+  a.h_bsh->k = k;
+  const size_t row = sizeof(double) * S.n;
+  ACG_CUDA(cudaMemcpy2DAsync(S.bb_ext[slot].p, row, B, sizeof(double) * ld, row, k, cudaMemcpyHostToDevice,
+                             S.h2d_stream));
+  ACG_CUDA(cudaEventRecord(a.h2d, S.h2d_stream));
+  ACG_CUDA(cudaStreamWaitEvent(S.stream, a.h2d, 0));
+  ACG_CUDA(cudaMemcpyAsync(S.bst, a.h_init, sizeof(PcgState) * kp, cudaMemcpyHostToDevice, S.stream));
+  ACG_CUDA(cudaMemcpyAsync(S.bsh, a.h_bsh, sizeof(BatchShared), cudaMemcpyHostToDevice, S.stream));
+  ACG_CUDA(cudaEventRecord(a.start, S.stream));
+  ACG_CUDA(cudaGraphLaunch(ge, S.stream));
+  ACG_CUDA(cudaMemcpyAsync(a.h_out, S.bst, sizeof(PcgState) * kp, cudaMemcpyDeviceToHost, S.stream));
+  ACG_CUDA(cudaEventRecord(a.done, S.stream));
+  ACG_CUDA(cudaStreamWaitEvent(S.d2h_stream, a.done, 0));
+  if (req->pinned_x)
+    ACG_CUDA(cudaMemcpy2DAsync(X, sizeof(double) * ld, S.bx_ext[slot].p, row, row, k, cudaMemcpyDeviceToHost,
+                               S.d2h_stream));
+  ACG_CUDA(cudaEventRecord(a.d2h, S.d2h_stream));
+  S.next_slot = slot ^ 1;
+  a.owner = req.get();
+  *out = req.release();
+  return ACG_OK;
+}
+
+}  // namespace
+}  // namespace acg
 
 namespace {
 
@@ -1938,6 +2112,13 @@ int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, cons
 void acg_destroy(acg_solver* h) {
   if (!h) return;
   std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
+  {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    acg_request* pending[2] = {h->impl.slots[0].owner, h->impl.slots[1].owner};
+    acg::drain_async(h->impl);  // requests not yet waited keep their results
+    for (acg_request* r : pending)
+      if (r) r->h = nullptr;
+  }
   cudaStreamSynchronize(h->impl.stream);
   delete h;
 }
@@ -1964,7 +2145,7 @@ int acg_solver_stats(const acg_solver* h, acg_stats* out) {
   add(S.b_ext); add(S.x_ext); add(S.bm); add(S.r64); add(S.s64); add(S.y64); add(S.p64); add(S.q64); add(S.x3_64);
   add(S.xf); add(S.r32); add(S.s32); add(S.y32); add(S.p32); add(S.q32); add(S.x3_32); add(S.partials);
   add(S.tasks_f); add(S.tasks_b);
-  add(S.bb_ext); add(S.bx_ext); add(S.bbm); add(S.br64); add(S.bxf); add(S.bpartials); add(S.br32); add(S.bs32);
+  add(S.bb_ext[0]); add(S.bx_ext[0]); add(S.bb_ext[1]); add(S.bx_ext[1]); add(S.bbm); add(S.br64); add(S.bxf); add(S.bpartials); add(S.br32); add(S.bs32);
   add(S.by32); add(S.bp32); add(S.bq32); add(S.bx3_32); add(S.bs64); add(S.by64); add(S.bp64); add(S.bq64);
   add(S.bx3_64);
   out->device_bytes = (int64_t)bytes;
@@ -1999,6 +2180,60 @@ int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t l
       worst = std::max(worst, rc);
     }
     return worst;
+  });
+}
+
+int acg_solve_async(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol,
+                    int64_t maxits, double maxtime, int stag_test, int precision, acg_request** out) {
+  if (out) *out = nullptr;
+  if (!h || !b || !x || !out || nrhs < 1 || nrhs > acg::kMaxBatch || ldb < h->impl.n ||
+      (precision != 0 && precision != 1) || h->impl.nseg > 1) {
+    acg::set_last_error("acg_solve_async: bad arguments (1 <= nrhs <= 64, ldb >= n, one graph)");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_solve_async", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    return acg::submit_async(h, b, x, (int)nrhs, ldb, tol, maxits, maxtime, stag_test, precision, out);
+  });
+}
+
+int acg_poll(acg_request* r) {
+  if (!r) {
+    acg::set_last_error("acg_poll: null request");
+    return ACG_ERR_INVALID;
+  }
+  acg_solver* h = r->h;
+  if (!h) return 1;
+  std::lock_guard<std::mutex> lk(h->impl.mu);
+  if (r->collected) return 1;
+  const cudaError_t e = cudaEventQuery(h->impl.slots[r->slot].d2h);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) return 0;
+  cudaGetLastError();
+  acg::set_last_error(std::string("acg_poll: ") + cudaGetErrorString(e));
+  return ACG_ERR_CUDA;
+}
+
+int acg_wait(acg_request* r, acg_solve_info* info) {
+  if (!r) {
+    acg::set_last_error("acg_wait: null request");
+    return ACG_ERR_INVALID;
+  }
+  std::unique_ptr<acg_request> own(r);
+  return guarded("acg_wait", [&]() {
+    acg_solver* h = r->h;
+    if (h) {
+      cudaEvent_t ev = nullptr;
+      {
+        std::lock_guard<std::mutex> lk(h->impl.mu);
+        if (!r->collected) ev = h->impl.slots[r->slot].d2h;
+      }
+      if (ev) cudaEventSynchronize(ev);  // without the lock: other threads may submit meanwhile
+      std::lock_guard<std::mutex> lk(h->impl.mu);
+      if (!r->collected) acg::collect(h->impl, r->slot);
+    }
+    if (r->rc != ACG_OK) return r->rc;
+    return acg::batch_results(r->levels, r->st, r->k, r->precision, r->ms, info);
   });
 }
 

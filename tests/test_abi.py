@@ -53,6 +53,11 @@ def test_bad_arguments_are_errors():
     assert rc < 0
     st = np.zeros(4, np.uint64)
     assert L.acg_approxchol(1, z, z, f, st, ctypes.byref(h)) == -1
+    # the asynchronous entries reject null handles and requests without a device
+    req = ctypes.c_void_p()
+    assert L.acg_solve_async(None, None, None, 1, 1, 1e-8, 10, 1.0, 5, 0, ctypes.byref(req)) == -1
+    assert L.acg_poll(None) == -1
+    assert L.acg_wait(None, None) == -1
 
 
 def _header_struct_fields(tag):
