@@ -87,6 +87,17 @@ int acg_factor_dims(const acg_factor* f, int64_t* n, int64_t* nnz);
 int acg_factor_export(const acg_factor* f, int64_t* col, int64_t* colptr, int64_t* rowval,
                       double* fval, double* d);
 void acg_factor_free(acg_factor* f);
+/* Binary LDLinv file (little-endian): "ACGLDLI1", int64 n, int64 F, int64 1
+ * (index base), then col[n-1], colptr[n], rowval[F] (int64) and fval[F], d[n]
+ * (float64), the fields of LDLinv (src/approxCholTypes.jl:73-79) as Julia
+ * stores them.  The reference has no such file: it lets a host that runs the
+ * reference's own elimination hand the factor over, and factors be cached.
+ * acg_ldlinv_load checks the header, the size and the structure (colptr from
+ * 1 to F+1 without decreasing, ids in [1, n]); read the arrays back with
+ * acg_factor_dims / acg_factor_export. */
+int acg_ldlinv_save(const char* path, int64_t n, const int64_t* col, const int64_t* colptr, const int64_t* rowval,
+                    const double* fval, const double* d, int64_t nnz);
+int acg_ldlinv_load(const char* path, acg_factor** out);
 
 /* ---- device solver ------------------------------------------------------ */
 typedef struct acg_solver acg_solver;

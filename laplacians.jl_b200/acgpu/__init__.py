@@ -2,10 +2,10 @@
 
 Public interface (mirrors the reference's names and keyword semantics):
     approxchol_lap, ApproxCholParams, lap, seed (Random.seed!), approx_chol,
-    DeviceLapSolver, components, generators.
+    DeviceLapSolver, components, generators, io (read_graph / writeIJV, LDLinv files).
 The solves run in libacgpu.so (CUDA, sm_100a); see include/acgpu.h.
 """
-from . import generators, tuning
+from . import generators, io, tuning
 from .solvers import (ApproxCholParams, DeviceLapSolver, GroupSolver, LDLinv, approx_chol, approxchol_lap, approxchol_lap1,
                       approxchol_lap2, approxchol_sddm,
                       components, lap, null_solver, rng_state, seed, set_rng_state, vec_to_comps)
@@ -17,4 +17,4 @@ _solvers_init()
 __all__ = ["approxchol_lap", "approxchol_lap1", "approxchol_lap2", "approxchol_sddm", "ApproxCholParams", "LDLinv", "DeviceLapSolver", "GroupSolver",
            "approx_chol",
            "lap", "seed", "rng_state", "set_rng_state", "components", "vec_to_comps", "null_solver", "generators",
-           "autotune", "tuning"]
+           "autotune", "tuning", "io"]

@@ -74,6 +74,9 @@ SIGNATURES = [
     ("acg_factor_dims", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     ("acg_factor_export", ctypes.c_int, [ctypes.c_void_p, i64p, i64p, i64p, f64p, f64p]),
     ("acg_factor_free", None, [ctypes.c_void_p]),
+    ("acg_ldlinv_save", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64, i64p, i64p, i64p, f64p, f64p,
+                                       ctypes.c_int64]),
+    ("acg_ldlinv_load", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
     ("acg_device_check", ctypes.c_int, []),
     ("acg_create", ctypes.c_int, [ctypes.c_int64, i64p, i64p, f64p, i64p, i64p, i64p, f64p, f64p, ctypes.c_int64,
                                   ctypes.c_int, ctypes.POINTER(AcgOptions), ctypes.POINTER(ctypes.c_void_p)]),

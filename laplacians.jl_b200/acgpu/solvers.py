@@ -163,10 +163,17 @@ def approx_chol(a, params: ApproxCholParams | None = None) -> LDLinv:
         p = elimination_order(a, order)
         pp = None if p is None else p.ctypes.data_as(ctypes.c_void_p)
         check(L.acg_approxchol_ordered(n, cp, rv, np.ascontiguousarray(a.data), pp, _RNG, ctypes.byref(h)))
+    return _take_factor(h)
+
+
+def _take_factor(h) -> LDLinv:
+    """Copy a library factor handle (acg_factor) into an LDLinv and free it."""
+    L = lib()
     try:
         nn = ctypes.c_int64()
         F = ctypes.c_int64()
         check(L.acg_factor_dims(h, ctypes.byref(nn), ctypes.byref(F)))
+        n = nn.value
         col = np.empty(n - 1, np.int64)
         colptr = np.empty(n, np.int64)
         rowval = np.empty(F.value, np.int64)

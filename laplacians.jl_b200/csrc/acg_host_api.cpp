@@ -1,5 +1,6 @@
 // C-ABI entry points that run on the host only: the Julia-compatible random
 // stream and the approximate Cholesky elimination.  See include/acgpu.h.
+#include <cstdio>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -164,5 +165,99 @@ int acg_factor_export(const acg_factor* f, int64_t* col, int64_t* colptr, int64_
 }
 
 void acg_factor_free(acg_factor* f) { delete f; }
+
+// ---- binary LDLinv file ------------------------------------------------------
+//
+// Little-endian: the 8 bytes "ACGLDLI1", int64 n, int64 F, int64 index base
+// (always 1), then col[n-1], colptr[n], rowval[F] as int64 and fval[F], d[n]
+// as float64: the LDLinv fields of src/approxCholTypes.jl:73-79 as Julia
+// stores them.
+
+int acg_ldlinv_save(const char* path, int64_t n, const int64_t* col, const int64_t* colptr, const int64_t* rowval,
+                    const double* fval, const double* d, int64_t nnz) {
+  if (!path || n < 1 || nnz < 0 || !colptr || !d || (n > 1 && !col) || (nnz > 0 && (!rowval || !fval))) {
+    acg::set_last_error("acg_ldlinv_save: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  FILE* fh = std::fopen(path, "wb");
+  if (!fh) {
+    acg::set_last_error(std::string("acg_ldlinv_save: cannot open ") + path);
+    return ACG_ERR_INVALID;
+  }
+  const int64_t head[3] = {n, nnz, 1};
+  bool ok = std::fwrite("ACGLDLI1", 1, 8, fh) == 8 && std::fwrite(head, sizeof(int64_t), 3, fh) == 3;
+  ok = ok && std::fwrite(col, sizeof(int64_t), (size_t)(n - 1), fh) == (size_t)(n - 1);
+  ok = ok && std::fwrite(colptr, sizeof(int64_t), (size_t)n, fh) == (size_t)n;
+  ok = ok && std::fwrite(rowval, sizeof(int64_t), (size_t)nnz, fh) == (size_t)nnz;
+  ok = ok && std::fwrite(fval, sizeof(double), (size_t)nnz, fh) == (size_t)nnz;
+  ok = ok && std::fwrite(d, sizeof(double), (size_t)n, fh) == (size_t)n;
+  ok = (std::fclose(fh) == 0) && ok;
+  if (!ok) {
+    acg::set_last_error(std::string("acg_ldlinv_save: write failed: ") + path);
+    return ACG_ERR_INVALID;
+  }
+  return ACG_OK;
+}
+
+int acg_ldlinv_load(const char* path, acg_factor** out) {
+  if (!path || !out) {
+    acg::set_last_error("acg_ldlinv_load: null argument");
+    return ACG_ERR_INVALID;
+  }
+  *out = nullptr;
+  FILE* fh = std::fopen(path, "rb");
+  if (!fh) {
+    acg::set_last_error(std::string("acg_ldlinv_load: cannot open ") + path);
+    return ACG_ERR_INVALID;
+  }
+  auto fail = [&](const char* why) {
+    std::fclose(fh);
+    acg::set_last_error(std::string("acg_ldlinv_load: ") + why + ": " + path);
+    return ACG_ERR_INVALID;
+  };
+  char magic[8];
+  int64_t head[3];
+  if (std::fread(magic, 1, 8, fh) != 8 || std::memcmp(magic, "ACGLDLI1", 8) != 0) return fail("not an LDLinv file");
+  if (std::fread(head, sizeof(int64_t), 3, fh) != 3) return fail("truncated header");
+  const int64_t n = head[0], nnz = head[1];
+  if (n < 1 || nnz < 0 || head[2] != 1) return fail("bad header");
+  // the payload must be exactly the size the header announces
+  std::fseek(fh, 0, SEEK_END);
+  const long long bytes = std::ftell(fh);
+  const long long want = 32 + 8LL * ((n - 1) + n + nnz + nnz + n);
+  if (bytes != want) return fail("file size does not match its header");
+  std::fseek(fh, 32, SEEK_SET);
+  try {
+    auto* f = new acg_factor();
+    acg::HostFactor& h = f->f;
+    h.n = n;
+    h.col.resize((size_t)(n - 1));
+    h.colptr.resize((size_t)n);
+    h.rowval.resize((size_t)nnz);
+    h.fval.resize((size_t)nnz);
+    h.d.resize((size_t)n);
+    bool ok = std::fread(h.col.data(), sizeof(int64_t), h.col.size(), fh) == h.col.size();
+    ok = ok && std::fread(h.colptr.data(), sizeof(int64_t), h.colptr.size(), fh) == h.colptr.size();
+    ok = ok && std::fread(h.rowval.data(), sizeof(int64_t), h.rowval.size(), fh) == h.rowval.size();
+    ok = ok && std::fread(h.fval.data(), sizeof(double), h.fval.size(), fh) == h.fval.size();
+    ok = ok && std::fread(h.d.data(), sizeof(double), h.d.size(), fh) == h.d.size();
+    // structure: colptr runs from 1 to F+1 without decreasing, ids in [1, n]
+    ok = ok && h.colptr[0] == 1 && h.colptr[(size_t)(n - 1)] == nnz + 1;
+    for (size_t i = 1; ok && i < h.colptr.size(); ++i) ok = h.colptr[i] >= h.colptr[i - 1];
+    for (size_t i = 0; ok && i < h.col.size(); ++i) ok = h.col[i] >= 1 && h.col[i] <= n;
+    for (size_t i = 0; ok && i < h.rowval.size(); ++i) ok = h.rowval[i] >= 1 && h.rowval[i] <= n;
+    if (!ok) {
+      delete f;
+      return fail("malformed factor");
+    }
+    std::fclose(fh);
+    *out = f;
+    return ACG_OK;
+  } catch (const std::bad_alloc&) {
+    std::fclose(fh);
+    acg::set_last_error("acg_ldlinv_load: host out of memory");
+    return ACG_ERR_NOMEM;
+  }
+}
 
 }  // extern "C"
