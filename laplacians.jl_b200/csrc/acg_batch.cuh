@@ -135,8 +135,20 @@ __device__ __forceinline__ void st_row(double* p, const double (&v)[CPL]) {
 // gl + j*gw of the vertex (the first four rounds are prefetched with the
 // task), broadcasts it to its group, and the group loads the input rows in
 // batches of EB with every load issued before any is checked.
+//
+// Blocks per SM the register budget is fitted to.  The FP32 64-column sweep
+// is held to 128 registers so that two blocks share an SM: its wide levels
+// are bound by how many tasks are in flight, and twice the warps outweigh
+// the few spilled registers (measured on the 1M grid: forward 1.05 ->
+// 0.90 ms, backward 1.24 -> 1.04 ms; loading 4 rows per batch instead of 8
+// to avoid the spills was slower, 1.08 / 1.10 ms).
+template <typename T, int CPL>
+__host__ __device__ constexpr int kb_sweep_min_blocks() {
+  return (sizeof(T) == 4 && CPL == 8) ? 2 : 1;
+}
+
 template <typename T, int CPL, bool kForward>
-__global__ void __launch_bounds__(kSweepThreads) kb_sweep(int ntasks, const SweepTask* __restrict__ tasks,
+__global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>()) kb_sweep(int ntasks, const SweepTask* __restrict__ tasks,
                                                           const int* __restrict__ idx, const T* __restrict__ coef,
                                                           const T* __restrict__ aux, const T* sfwd,
                                                           T* out, T* mark, BatchShared* bs) {
