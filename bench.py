@@ -298,7 +298,7 @@ def run_acgpu(args):
                                  MAXITS, float("inf"), 5, prec, infos))
         single.append(infos[0].solve_ms)
 
-    # roofline of the dominant kernel (the forward LDLinv sweep), timed live
+    # roofline of the dominant kernel (the longer LDLinv sweep), timed live
     kt = dev.time_kernels_batch(k, args.precision, reps=5) if k > 1 else dev.time_kernels(args.precision, reps=5)
     stats = dev.stats()
     peaks = {}

@@ -23,7 +23,7 @@ struct BatchShared {
   int all_done;     // every column stopped
   int sweep_error;  // a bounded sweep wait gave up
   int k;            // right-hand sides in this launch (the rest of kp is padding)
-  int pad;
+  int l1_due;       // kb_yzr deferred the third L1 test of some column to kb_pupdate_z
   unsigned int counter[16];
 };
 
@@ -543,7 +543,8 @@ __global__ void __launch_bounds__(kBVecThreads) kb_ysum(int n, int kp, const T* 
   }
 }
 
-// z = y - mean (in place); rho = z.r, |z|_1; the iteration's remaining scalar steps
+// The pre-loop step of a batched solve (init 1 or 2, see pcg_scalar_zdot):
+// z = y - mean (in place), p = z; rho = z.r, |z|_1
 template <typename T>
 __global__ void __launch_bounds__(kBVecThreads) kb_zdot(int n, int kp, T* __restrict__ yz, const T* __restrict__ r,
                                                         T* __restrict__ p, PcgState* st, BatchShared* bs,
@@ -587,28 +588,109 @@ __global__ void __launch_bounds__(kBVecThreads) kb_zdot(int n, int kp, T* __rest
   }
 }
 
+// The loop body's tail in two passes instead of three (kb_ysum, kb_zdot,
+// kb_pupdate).  z = y - mean is never stored: kb_yzr sums y, y.r and r per
+// column in one pass over y and r, and rho = (y - mean).r is y.r - mean * r.1
+// (r.1 vanishes up to rounding: r stays orthogonal to the constant vector).
+// The third L1 test needs |z|_1, which only every 10th iteration reads; on
+// those iterations kb_yzr leaves the column's test, maxtime and maxits (in the
+// reference's order) to kb_pupdate_z, which forms z while it updates p and
+// sums |z|_1 on the way.  p of a column stopped by those tests is updated
+// once more, which nothing reads: x comes from bestx.
 template <typename T>
-__global__ void __launch_bounds__(kBVecThreads) kb_pupdate(int n, int kp, const T* __restrict__ z, T* __restrict__ p,
-                                                           const PcgState* st, const BatchShared* bs) {
+__global__ void __launch_bounds__(kBVecThreads) kb_yzr(int n, int kp, const T* __restrict__ y, const T* __restrict__ r,
+                                                       PcgState* st, BatchShared* bs, double* partials, double eps,
+                                                       LoopCtl ctl) {
   if (bs->all_done) return;
+  const size_t N = (size_t)n * kp;
+  const size_t S = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (; i + (kBU - 1) * S < N; i += kBU * S) {
+    T yv[kBU], rv[kBU];
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      yv[u] = y[i + u * S];
+      rv[u] = r[i + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) {
+      acc[0] += (double)yv[u];
+      acc[1] += (double)yv[u] * (double)rv[u];
+      acc[2] += (double)rv[u];
+    }
+  }
+  for (; i < N; i += S) {
+    acc[0] += (double)y[i];
+    acc[1] += (double)y[i] * (double)r[i];
+    acc[2] += (double)r[i];
+  }
+  double tot[3];
+  if (batch_reduce<3>(acc, kp, partials, &bs->counter[8], tot)) {
+    const int c = threadIdx.x;
+    bool deferred = false;
+    if (c < kp) {
+      const double mu = tot[0] / (double)n;
+      st[c].mean = mu;
+      if (bs->sweep_error && !st[c].done) mark_stop(&st[c], kSweepTimeout);
+      if (!st[c].done && !pcg_scalar_rho(&st[c], tot[1] - mu * tot[2])) {
+        if (st[c].itcnt % 10 == 0)
+          deferred = true;
+        else
+          pcg_scalar_tail(&st[c], eps);
+      }
+    }
+    const int any = __syncthreads_or(deferred);
+    if (threadIdx.x == 0) bs->l1_due = any;
+    batch_check_all(st, bs, kp, ctl);
+  }
+}
+
+// z = y - mean, p = z + beta p (columns still running); on the iterations
+// kb_yzr deferred, also |z|_1 and the deferred tests.
+template <typename T>
+__global__ void __launch_bounds__(kBVecThreads) kb_pupdate_z(int n, int kp, const T* __restrict__ y, T* __restrict__ p,
+                                                             PcgState* st, BatchShared* bs, double* partials,
+                                                             double eps, LoopCtl ctl) {
+  if (bs->all_done) return;
+  const bool l1 = bs->l1_due != 0;  // the same for every thread of the launch
   const size_t N = (size_t)n * kp;
   const size_t S = (size_t)gridDim.x * blockDim.x;
   const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = (int)(i0 % kp);
-  if (st[c].done) return;
+  const double mu = st[c].mean;
   const double beta = st[c].beta;
-  size_t i = i0;
+  double acc[1] = {0.0};
+  size_t i = st[c].done ? N : i0;
   for (; i + (kBU - 1) * S < N; i += kBU * S) {
-    T zv[kBU], pv[kBU];
+    T yv[kBU], pv[kBU];
 #pragma unroll
     for (int u = 0; u < kBU; ++u) {
-      zv[u] = z[i + u * S];
+      yv[u] = y[i + u * S];
       pv[u] = p[i + u * S];
     }
 #pragma unroll
-    for (int u = 0; u < kBU; ++u) p[i + u * S] = (T)((double)zv[u] + beta * (double)pv[u]);
+    for (int u = 0; u < kBU; ++u) {
+      const T z = (T)((double)yv[u] - mu);
+      p[i + u * S] = (T)((double)z + beta * (double)pv[u]);
+      acc[0] += fabs((double)z);
+    }
   }
-  for (; i < N; i += S) p[i] = (T)((double)z[i] + beta * (double)p[i]);
+  for (; i < N; i += S) {
+    const T z = (T)((double)y[i] - mu);
+    p[i] = (T)((double)z + beta * (double)p[i]);
+    acc[0] += fabs((double)z);
+  }
+  if (!l1) return;
+  double tot[1];
+  if (batch_reduce<1>(acc, kp, partials, &bs->counter[9], tot)) {
+    const int cc = threadIdx.x;
+    if (cc < kp && !st[cc].done && st[cc].itcnt % 10 == 0) {
+      st[cc].sum_abs_z = tot[0];
+      pcg_scalar_tail(&st[cc], eps);
+    }
+    batch_check_all(st, bs, kp, ctl);
+  }
 }
 
 // ---- set-up and wrap-up ------------------------------------------------------

@@ -86,20 +86,10 @@ __device__ __forceinline__ bool pcg_scalar_update(PcgState* st, double rr, doubl
   return false;
 }
 
-// after z = pre(r), rho = z.r: stagnation, inf, beta, third L1 test, maxtime,
-// maxits (src/pcg.jl:365-432).  init: the pre-loop rho (1 also starts the clock).
-__device__ __forceinline__ bool pcg_scalar_zdot(PcgState* st, double zr, double sum_abs_z, double eps, int init) {
-  st->sum_abs_z = sum_abs_z;
-  if (init) {
-    st->rho = zr;
-    st->best_rho = zr;
-    st->stag_count = 0;
-    if (init == 1) st->t_start = globaltimer_ns();
-    if (st->itcnt >= st->maxits) return mark_stop(st, kMaxits);
-    return false;
-  }
+// after z = pre(r), rho = z.r: the rho stagnation test, inf and beta
+// (src/pcg.jl:365-404).
+__device__ __forceinline__ bool pcg_scalar_rho(PcgState* st, double rho) {
   const double oldrho = st->rho;
-  const double rho = zr;
   st->rho = rho;
   const double thr = 1.0 - 1.0 / (double)st->stag_test;
   if (rho < st->best_rho * thr) {
@@ -115,11 +105,33 @@ __device__ __forceinline__ bool pcg_scalar_zdot(PcgState* st, double zr, double 
   const double beta = rho / oldrho;
   st->beta = beta;
   if (isinf(beta)) return mark_stop(st, kInf);
-  if (st->itcnt % 10 == 0 && beta * st->sum_abs_p < eps * st->sum_abs_z) return mark_stop(st, kStagP);
+  return false;
+}
+
+// the rest of the iteration: the third L1 test (every 10th iteration, with
+// st->sum_abs_z of this iteration's z), maxtime and maxits (src/pcg.jl:406-432)
+__device__ __forceinline__ bool pcg_scalar_tail(PcgState* st, double eps) {
+  if (st->itcnt % 10 == 0 && st->beta * st->sum_abs_p < eps * st->sum_abs_z) return mark_stop(st, kStagP);
   const double el = (double)(globaltimer_ns() - st->t_start) * 1e-9;
   if (el > st->maxtime_s) return mark_stop(st, kMaxtime);
   if (st->itcnt >= st->maxits) return mark_stop(st, kMaxits);
   return false;
+}
+
+// after z = pre(r), rho = z.r: stagnation, inf, beta, third L1 test, maxtime,
+// maxits (src/pcg.jl:365-432).  init: the pre-loop rho (1 also starts the clock).
+__device__ __forceinline__ bool pcg_scalar_zdot(PcgState* st, double zr, double sum_abs_z, double eps, int init) {
+  st->sum_abs_z = sum_abs_z;
+  if (init) {
+    st->rho = zr;
+    st->best_rho = zr;
+    st->stag_count = 0;
+    if (init == 1) st->t_start = globaltimer_ns();
+    if (st->itcnt >= st->maxits) return mark_stop(st, kMaxits);
+    return false;
+  }
+  if (pcg_scalar_rho(st, zr)) return true;
+  return pcg_scalar_tail(st, eps);
 }
 
 __device__ __forceinline__ void clear_loop(const LoopCtl& ctl) {

@@ -75,3 +75,26 @@ def test_batch_repeatable(grid):
     X1 = dev(B, tol=1e-9)
     X2 = dev(B, tol=1e-9)
     assert np.array_equal(X1, X2)
+
+
+def test_batch_stop_codes_on_the_tenth_iterations(grid):
+    """The third L1 test, maxtime and maxits of every 10th iteration run after
+    the p update (where |z|_1 is summed): maxits landing on those iterations
+    stops every column there, and a tolerance no solve reaches ends every
+    column with a stagnation code (src/pcg.jl:288-432), as a lone solve does."""
+    a, ldli, dev = grid
+    n = a.shape[0]
+    B = np.random.default_rng(31).standard_normal((n, 8))
+    for maxits in (10, 20):
+        dev(B, tol=1e-14, maxits=maxits)
+        for c in range(8):
+            assert dev.last_info[c].iterations == maxits and dev.last_info[c].status == 1
+    X = dev(B, tol=1e-30, maxits=400)
+    infos = list(dev.last_info)
+    stagnation = {2, 3, 4, 6}
+    for c in range(8):
+        assert infos[c].status in stagnation, (c, infos[c].status)
+        assert O.relres(a, X[:, c], B[:, c] - B[:, c].mean()) < 1e-10
+    its = [0]
+    dev(B[:, 5], tol=1e-30, maxits=400, pcgIts=its)
+    assert dev.last_info[0].status in stagnation
