@@ -314,6 +314,7 @@ def run_acgpu(args):
     sweep_ms = kt[direction + "_sweep_ms"]
     sweep_bytes = kt[direction + "_sweep_bytes"]
     achieved = sweep_bytes / (sweep_ms * 1e-3) / 1e9
+    swept_levels = int(stats["levels"] - stats["dense_levels"])
     traffic = None
     prof = ROOT / "profiles" / (f"kb_sweep_{direction}_grid3_100_k64.md" if k > 1
                                 else f"k_sweep_{direction}_grid3_100.md")
@@ -355,6 +356,8 @@ def run_acgpu(args):
                          "algorithmic_bytes_per_launch": sweep_bytes, "launch_ms": sweep_ms,
                          "forward_sweep_ms": kt["forward_sweep_ms"], "backward_sweep_ms": kt["backward_sweep_ms"],
                          "dense_tail_ms": kt["dense_ms"], "dense_tail_vertices": stats["dense_vertices"],
+                         # the sweep walks the DAG's head levels one after another: time per level
+                         "swept_levels": swept_levels, "us_per_level": 1e3 * sweep_ms / max(1, swept_levels),
                          "spmv_ms": kt["spmv_ms"], "spmv_gbs": kt["spmv_bytes"] / (kt["spmv_ms"] * 1e-3) / 1e9},
             "cpu_baseline": cpu,
             "clocks": clocks,

@@ -273,13 +273,16 @@ int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg
  * already in device memory, without allocating: every piece of scratch comes
  * from one fixed device array inside the library (ACG_NOALLOC_MAX_N vertices
  * at most, about 6.4 MB, reserved on each GPU that loads the library until
- * the process exits).  Meant for callers that must not allocate at that
- * moment, e.g. work enqueued while a stream is captured into a CUDA graph, or
- * a serving loop whose device memory is a fixed pool.  The scratch address is
- * looked up once per device inside acg_create (set-up).  Work is enqueued on
- * `stream` (a cudaStream_t; NULL = the legacy default stream); outside stream
- * capture the call also waits for it and reports a sweep that gave up as
- * ACG_ERR_TIMEOUT.  Every call shares the one array: calls whose work
+ * the process exits).  Meant for callers that must not allocate while they
+ * solve: a serving loop whose device memory is a fixed pool sized at start-up,
+ * a host runtime whose own allocator owns the GPU's memory, or a caller that
+ * cannot let cudaMalloc/cudaFree synchronize the device under its other
+ * streams.  The scratch address is looked up once per device inside
+ * acg_create (set-up).  Work is enqueued on `stream` (a cudaStream_t; NULL =
+ * the legacy default stream); the call then waits for it and reports a sweep
+ * that gave up as ACG_ERR_TIMEOUT.  The array keeps the last call's contents;
+ * each call clears the state that must start at zero (the stop flags and
+ * reduction tickets) itself.  Every call shares the one array: calls whose work
  * overlaps on the GPU (different streams, or different solvers, at the same
  * time) race and corrupt each other's results.  Graphs with more than
  * ACG_NOALLOC_MAX_N vertices are rejected with ACG_ERR_INVALID. */

@@ -136,15 +136,17 @@ __device__ __forceinline__ void st_row(double* p, const double (&v)[CPL]) {
 // task), broadcasts it to its group, and the group loads the input rows in
 // batches of EB with every load issued before any is checked.
 //
-// Blocks per SM the register budget is fitted to.  The FP32 64-column sweep
-// is held to 128 registers so that two blocks share an SM: its wide levels
-// are bound by how many tasks are in flight, and twice the warps outweigh
-// the few spilled registers (measured on the 1M grid: forward 1.05 ->
-// 0.90 ms, backward 1.24 -> 1.04 ms; loading 4 rows per batch instead of 8
-// to avoid the spills was slower, 1.08 / 1.10 ms).
+// Blocks per SM the register budget is fitted to.  The FP32 sweeps of 32 and
+// 64 columns are held to 128 registers so that two blocks share an SM: their
+// wide levels are bound by how many tasks are in flight, and twice the warps
+// outweigh the few spilled registers (measured on the 1M grid, 64 columns:
+// forward 1.05 -> 0.90 ms, backward 1.24 -> 1.04 ms, with 140-148 B of
+// spills; loading 4 rows per batch instead of 8 to avoid the spills was
+// slower, 1.08 / 1.10 ms; 32 columns: 0.90 / 0.95 -> 0.66 / 0.78 ms, no
+// spills).  The narrower FP32 sweeps fit two blocks anyway.
 template <typename T, int CPL>
 __host__ __device__ constexpr int kb_sweep_min_blocks() {
-  return (sizeof(T) == 4 && CPL == 8) ? 2 : 1;
+  return (sizeof(T) == 4 && CPL >= 4) ? 2 : 1;
 }
 
 template <typename T, int CPL, bool kForward>

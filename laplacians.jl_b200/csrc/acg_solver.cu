@@ -1135,9 +1135,10 @@ void ldlsolve_impl(SolverImpl& S, T* rbuf, T* sbuf, T* ybuf) {
 // ---- allocation-free LDLsolver ----------------------------------------------
 //
 // Some callers cannot allocate device memory at the moment they apply the
-// preconditioner: work enqueued while a stream is being captured into a CUDA
-// graph (the allocator may not be called then), or a serving loop whose device
-// memory comes from a pool that must not grow after start-up.  For them
+// preconditioner: a serving loop whose device memory comes from a pool that
+// must not grow after start-up, a host runtime whose own allocator owns the
+// GPU's memory, or a caller that cannot let cudaMalloc/cudaFree synchronize
+// the device under its other streams.  For them
 // acg_ldlsolve_noalloc keeps every piece of its scratch (the input in solver
 // order, the forward and backward sweep vectors, the reduction partials, the
 // dense tail's partial tiles and the scalar state) in the one fixed array
@@ -2379,14 +2380,10 @@ int acg_ldlsolve_noalloc(acg_solver* h, const double* r_dev, double* y_dev, int 
     if (precision == 0) acg::ldlsolve_noalloc_impl<double>(S, s, r_dev, y_dev, S.noalloc_scratch);
     else acg::ldlsolve_noalloc_impl<float>(S, s, r_dev, y_dev, S.noalloc_scratch);
     ACG_CUDA(cudaGetLastError());
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    ACG_CUDA(cudaStreamIsCapturing(s, &cap));
-    if (cap == cudaStreamCaptureStatusNone) {
-      ACG_CUDA(cudaStreamSynchronize(s));
-      if (acg::noalloc_sweep_error(S.noalloc_scratch)) {
-        acg::set_last_error("acg_ldlsolve_noalloc: a bounded sweep wait gave up");
-        return ACG_ERR_TIMEOUT;
-      }
+    ACG_CUDA(cudaStreamSynchronize(s));
+    if (acg::noalloc_sweep_error(S.noalloc_scratch)) {
+      acg::set_last_error("acg_ldlsolve_noalloc: a bounded sweep wait gave up");
+      return ACG_ERR_TIMEOUT;
     }
     return ACG_OK;
   });

@@ -1,8 +1,9 @@
 """GPU test of the allocation-free preconditioner entry point.
 
 acg_ldlsolve_noalloc serves callers that may not allocate device memory when
-they apply the preconditioner (work recorded inside a CUDA-graph capture, or a
-loop running from a fixed memory pool).  It must give the same y as the
+they apply the preconditioner (a serving loop running from a fixed memory
+pool, a host runtime whose own allocator owns the GPU's memory, or a caller
+that cannot let cudaMalloc/cudaFree synchronize the device).  It must give the same y as the
 ordinary entry point acg_ldlsolve, call after call, while taking all of its
 scratch from the library's fixed array.  This file is collected last so that a
 run stopping at the first failure has already run every other test; it also
