@@ -18,6 +18,13 @@ constexpr int kMaxBatch = 64;
 constexpr int kBVecThreads = 512;
 constexpr int kBVecBlocks = 148 * 2;
 constexpr int kBatchLanes = 8;  // lanes per vertex in the batched sweeps and mat-vec
+// Rounds of a task's entries the batched sweeps prefetch with the task.  At
+// the default heavy threshold of 8 a light task's vertices have at most 8
+// entries (one round on 8 lanes) and a heavy task's one round covers 32;
+// longer rows load their later rounds as they go.  One round instead of four frees the registers that spilled at two
+// blocks per SM (140 -> 52 B per thread at 64 FP32 columns; forward 0.895 ->
+// 0.834 ms, backward 1.036 -> 0.977 ms on the 1M grid).
+constexpr int kBatchEntryUnroll = 1;
 
 struct BatchShared {
   int all_done;     // every column stopped
@@ -163,15 +170,15 @@ __global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>()) 
   const int W = (int)((gridDim.x * blockDim.x) >> 5);
   int t = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   SweepTask r1 = load_task(tasks, t + W, ntasks);
-  SweepEntries<T> e0;
+  SweepEntries<T, kBatchEntryUnroll> e0;
   {
     const SweepTask r0 = load_task(tasks, t, ntasks);
-    load_entries<T, true, false>(e0, r0, lane, idx, coef, coef, coef);
+    load_entries<T, true, false, kBatchEntryUnroll>(e0, r0, lane, idx, coef, coef, coef);
   }
   for (; t < ntasks; t += W) {
     const SweepTask r2 = load_task(tasks, t + 2 * W, ntasks);
-    SweepEntries<T> e1;
-    load_entries<T, true, false>(e1, r1, lane, idx, coef, coef, coef);
+    SweepEntries<T, kBatchEntryUnroll> e1;
+    load_entries<T, true, false, kBatchEntryUnroll>(e1, r1, lane, idx, coef, coef, coef);
     const int gw = e0.gw;  // 32 for a heavy task, 8 for a light one (uniform per warp)
     const int k0 = e0.k0 - (gw == 32 ? lane : gl);  // first entry of this lane's vertex
     T acc[CPL];
@@ -190,11 +197,11 @@ __global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>()) 
     for (int j = 0; j < rounds; ++j) {
       int myid;
       T myc;
-      if (j < kEntryUnroll) {
+      if (j < kBatchEntryUnroll) {
         myid = e0.id[0];
         myc = e0.c[0];
 #pragma unroll
-        for (int q = 1; q < kEntryUnroll; ++q)
+        for (int q = 1; q < kBatchEntryUnroll; ++q)
           if (q == j) {
             myid = e0.id[q];
             myc = e0.c[q];

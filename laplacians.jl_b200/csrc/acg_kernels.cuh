@@ -418,12 +418,12 @@ struct alignas(16) SweepTask {
   int p[6];
 };
 
-template <typename T>
+template <typename T, int U = kEntryUnroll>
 struct SweepEntries {
   int v, k0, k1, gw;
   bool active;
-  int id[kEntryUnroll];
-  T c[kEntryUnroll];
+  int id[U];
+  T c[U];
   T a, own;
 };
 
@@ -442,8 +442,8 @@ __device__ __forceinline__ SweepTask load_task(const SweepTask* __restrict__ tas
   return r;
 }
 
-template <typename T, bool kForward, bool kLoadAux = true>
-__device__ __forceinline__ void load_entries(SweepEntries<T>& e, const SweepTask& r, int lane,
+template <typename T, bool kForward, bool kLoadAux = true, int U = kEntryUnroll>
+__device__ __forceinline__ void load_entries(SweepEntries<T, U>& e, const SweepTask& r, int lane,
                                              const int* __restrict__ idx, const T* __restrict__ coef,
                                              const T* __restrict__ aux, const T* __restrict__ sfwd, int vs = 1) {
   const bool heavy = r.cnt_heavy & 1;
@@ -464,7 +464,7 @@ __device__ __forceinline__ void load_entries(SweepEntries<T>& e, const SweepTask
   e.a = (kLoadAux && e.active) ? __ldg(&aux[e.v]) : T(0);
   e.own = (kLoadAux && !kForward && e.active) ? __ldg(&sfwd[(size_t)e.v * vs]) : T(0);
 #pragma unroll
-  for (int j = 0; j < kEntryUnroll; ++j) {
+  for (int j = 0; j < U; ++j) {
     const int k = e.k0 + j * gw;
     e.id[j] = k < k1 ? __ldg(&idx[k]) : -1;
     e.c[j] = k < k1 ? __ldg(&coef[k]) : T(0);
