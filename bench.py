@@ -246,6 +246,25 @@ def run_acgpu(args):
     refs = np.array([r[1] for r in results], dtype=float)
     res = np.array([r[2] for r in results])
 
+    # error against an FP64 reference solution (outside the timed region): the
+    # last step's right-hand sides solved again by the FP64 PCG to 1e-12 on
+    # the same factor; x is compared after removing its mean (L's null space)
+    X64 = torch.empty_like(X)
+    infos64 = (AcgSolveInfo * k)()
+    last = nsteps - 1
+    if k == 1:
+        check(L.acg_solve_device(dev._h, ctypes.c_void_p(B[last].data_ptr()), ctypes.c_void_p(X64.data_ptr()),
+                                 1e-12, MAXITS, float("inf"), 5, 0, infos64))
+    else:
+        check(L.acg_solve_batch_device(dev._h, ctypes.c_void_p(B[last].data_ptr()), ctypes.c_void_p(X64.data_ptr()),
+                                       k, n, 1e-12, MAXITS, float("inf"), 5, 0, infos64))
+    torch.cuda.synchronize()
+    xc = X - X.mean(dim=1, keepdim=True)
+    xr = X64 - X64.mean(dim=1, keepdim=True)
+    err_fp64 = float(((xc - xr).norm(dim=1) / xr.norm(dim=1)).max())
+    ref_relres = max(infos64[c].true_relres for c in range(k))
+    ref_converged = sum(1 for c in range(k) if infos64[c].status == 0)
+
     # end to end: pinned host blocks through the asynchronous C entry
     # (acg_solve_async / acg_wait), every step's H2D and D2H inside the timed
     # region; two requests in flight, so one step's copies overlap the
@@ -347,7 +366,12 @@ def run_acgpu(args):
                                  "batching": f"{k} independent single-RHS solves per step in one batched launch",
                                  "pcg_iterations_mean": float(its.mean()), "refinements_mean": float(refs.mean()),
                                  "true_relres_max": float(res.max()), "factor_s": factor_s, "upload_s": upload_s,
-                                 "levels": stats["levels"], "factor_nnz": stats["nnz_factor"]}),
+                                 "levels": stats["levels"], "factor_nnz": stats["nnz_factor"],
+                                 "error_vs_fp64_reference": {
+                                     "max_rel_error": err_fp64, "reference_true_relres_max": ref_relres,
+                                     "reference_columns_converged": ref_converged,
+                                     "reference": "FP64 PCG to 1e-12 on the same LDLinv (this library's FP64 "
+                                                  "path), last step's right-hand sides, x with its mean removed"}}),
             "single_rhs": {"latency_ms": float(np.median(single)), "solves_per_s": 1e3 / float(np.median(single))},
             "e2e": {"value": world * args.steps * k / (e2e_ms * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": 8 * n * k, "d2h_bytes_per_step": 8 * n * k},
