@@ -21,9 +21,10 @@ constexpr int kBatchLanes = 8;  // lanes per vertex in the batched sweeps and ma
 // Rounds of a task's entries the batched sweeps prefetch with the task.  At
 // the default heavy threshold of 8 a light task's vertices have at most 8
 // entries (one round on 8 lanes) and a heavy task's one round covers 32;
-// longer rows load their later rounds as they go.  One round instead of four frees the registers that spilled at two
-// blocks per SM (140 -> 52 B per thread at 64 FP32 columns; forward 0.895 ->
-// 0.834 ms, backward 1.036 -> 0.977 ms on the 1M grid).
+// longer rows load their later rounds as they go.  One round instead of four
+// frees the registers that spilled at two blocks per SM (140 -> 52 B per
+// thread at 64 FP32 columns; forward 0.895 -> 0.834 ms, backward 1.036 ->
+// 0.977 ms on the 1M grid).
 constexpr int kBatchEntryUnroll = 1;
 
 struct BatchShared {
@@ -203,8 +204,8 @@ __device__ __forceinline__ void st_stream_row(double* p, const double (&v)[CPL],
 // a heavy task puts its one vertex on all four groups, group g taking the
 // entries 8g..8g+7 of every round of 32, and the four partial sums are
 // combined with shuffles.  In round j lane l of a group holds entry
-// gl + j*gw of the vertex (the first four rounds are prefetched with the
-// task), broadcasts it to its group, and the group loads the input rows in
+// gl + j*gw of the vertex (the first kBatchEntryUnroll rounds are prefetched
+// with the task), broadcasts it to its group, and the group loads the input rows in
 // batches of EB with every load issued before any is checked.
 //
 // Blocks per SM the register budget is fitted to.  The FP32 sweeps of 32 and
@@ -221,10 +222,10 @@ __host__ __device__ constexpr int kb_sweep_min_blocks() {
 }
 
 template <typename T, int CPL, bool kForward>
-__global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>()) kb_sweep(int ntasks, const SweepTask* __restrict__ tasks,
-                                                          const int* __restrict__ idx, const T* __restrict__ coef,
-                                                          const T* __restrict__ aux, const T* sfwd,
-                                                          T* out, T* mark, BatchShared* bs) {
+__global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>())
+    kb_sweep(int ntasks, const SweepTask* __restrict__ tasks, const int* __restrict__ idx,
+             const T* __restrict__ coef, const T* __restrict__ aux, const T* sfwd, T* out, T* mark,
+             BatchShared* bs) {
   if (bs->all_done) return;
   constexpr int kp = CPL * kBatchLanes;
   // rows loaded per batch: a whole slot of 8 entries where registers allow
