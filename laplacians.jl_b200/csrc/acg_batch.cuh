@@ -86,27 +86,6 @@ __device__ __forceinline__ bool row_pending(const Row<T, CPL>& r) {
   return any;
 }
 
-// Slow path: poll the row (in L2) until no value is pending or the bound is
-// hit.  Returns the row as the last poll saw it, ready (rows are written once
-// per sweep, so no second load is needed), or zeros when the wait gave up.
-template <typename T, int CPL>
-__device__ __noinline__ Row<T, CPL> wait_row_slow(const T* p, BatchShared* bs) {
-  Row<T, CPL> r;
-  for (unsigned int spins = 1;; ++spins) {
-    if (spins >= 64) __nanosleep(64);
-    ld_row<CPL>(r, p);
-    if (!row_pending(r)) return r;
-    if ((spins & 1023u) == 0 && *((volatile int*)&bs->sweep_error)) break;
-    if (spins >= kSpinLimit) {
-      atomicExch(&bs->sweep_error, 1);
-      break;
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < CPL; ++j) r.v[j] = T(0);
-  return r;
-}
-
 template <int CPL>
 __device__ __forceinline__ void st_row(float* p, const float (&v)[CPL]) {
   if constexpr (CPL % 4 == 0) {
@@ -294,10 +273,43 @@ __global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>())
 #pragma unroll
         for (int u = 0; u < EB; ++u)
           if (ids[u] >= 0) ld_row<CPL>(vals[u], out + (size_t)ids[u] * kp + gl * CPL);
+        unsigned pend = 0;
+#pragma unroll
+        for (int u = 0; u < EB; ++u)
+          if (ids[u] >= 0 && row_pending(vals[u])) pend |= 1u << u;
+        // Rows seen pending are polled again together, every poll of a round
+        // in flight at once, until none is pending.  Waiting for them one at
+        // a time paid a full L2 round trip for each stale row even when it
+        // had become ready during the earlier waits (measured on the 1M grid
+        // at 64 columns: backward 0.953 -> 0.823 ms, forward 0.816 -> 0.789
+        // ms).  A row read ready is final: rows are written once per sweep.
+        // The wait is bounded: after kSpinLimit rounds, or once another wait
+        // has given up, the sweep error is raised and the rows still pending
+        // read as zeros.
+        for (unsigned int spins = 1; pend; ++spins) {
+          if (spins >= 64) __nanosleep(64);
+#pragma unroll
+          for (int u = 0; u < EB; ++u)
+            if ((pend >> u) & 1u) ld_row<CPL>(vals[u], out + (size_t)ids[u] * kp + gl * CPL);
+          unsigned still = 0;
+#pragma unroll
+          for (int u = 0; u < EB; ++u)
+            if (((pend >> u) & 1u) && row_pending(vals[u])) still |= 1u << u;
+          pend = still;
+          if (pend && (((spins & 1023u) == 0 && *((volatile int*)&bs->sweep_error)) || spins >= kSpinLimit)) {
+            atomicExch(&bs->sweep_error, 1);
+#pragma unroll
+            for (int u = 0; u < EB; ++u)
+              if ((pend >> u) & 1u) {
+#pragma unroll
+                for (int q = 0; q < CPL; ++q) vals[u].v[q] = T(0);
+              }
+            break;
+          }
+        }
 #pragma unroll
         for (int u = 0; u < EB; ++u) {
           if (ids[u] < 0) continue;
-          if (row_pending(vals[u])) vals[u] = wait_row_slow<T, CPL>(out + (size_t)ids[u] * kp + gl * CPL, bs);
 #pragma unroll
           for (int q = 0; q < CPL; ++q) acc[q] += cs[u] * vals[u].v[q];
         }
