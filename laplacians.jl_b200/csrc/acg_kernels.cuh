@@ -499,12 +499,50 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const Sweep
     T xv[kEntryUnroll];
 #pragma unroll
     for (int j = 0; j < kEntryUnroll; ++j) xv[j] = e0.id[j] >= 0 ? ld_relaxed(&out[(size_t)e0.id[j] * vs]) : T(0);
+    // FP32: inputs seen pending are polled again together (all polls of a
+    // round in flight), not one wait after another; bounded like every wait.
+    // Single-vector mixed solve on the 1M grid: 39.5 -> 36.9 ms.  FP64 keeps
+    // the waits one by one: with joint polls, 256 graphs in one FP64 launch
+    // (many graphs, thousands of tasks per level) went from 146.7 to 156.3 ms.
+    unsigned pend = 0;
+    if constexpr (sizeof(T) == 4) {
 #pragma unroll
-    for (int j = 0; j < kEntryUnroll; ++j) {
-      if (e0.id[j] < 0) continue;
-      if (is_pending(xv[j])) xv[j] = wait_value_slow(&out[(size_t)e0.id[j] * vs], st, poll_mode);
-      acc += e0.c[j] * xv[j];
+      for (int j = 0; j < kEntryUnroll; ++j)
+        if (e0.id[j] >= 0 && is_pending(xv[j])) pend |= 1u << j;
+    } else {
+#pragma unroll
+      for (int j = 0; j < kEntryUnroll; ++j)
+        if (e0.id[j] >= 0 && is_pending(xv[j])) xv[j] = wait_value_slow(&out[(size_t)e0.id[j] * vs], st, poll_mode);
     }
+    unsigned int sleep_ns = 32;
+    for (unsigned int spins = 1; pend; ++spins) {
+      if (poll_mode == 0) {
+        if (spins >= 64) __nanosleep(64);
+      } else if (poll_mode == 2) {
+        if (spins >= 4) {
+          __nanosleep(sleep_ns);
+          if (sleep_ns < 1024) sleep_ns <<= 1;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kEntryUnroll; ++j)
+        if ((pend >> j) & 1u) xv[j] = ld_relaxed(&out[(size_t)e0.id[j] * vs]);
+      unsigned still = 0;
+#pragma unroll
+      for (int j = 0; j < kEntryUnroll; ++j)
+        if (((pend >> j) & 1u) && is_pending(xv[j])) still |= 1u << j;
+      pend = still;
+      if (pend && (((spins & 1023u) == 0 && *((volatile int*)&st->sweep_error)) || spins >= kSpinLimit)) {
+        atomicExch(&st->sweep_error, 1);
+#pragma unroll
+        for (int j = 0; j < kEntryUnroll; ++j)
+          if ((pend >> j) & 1u) xv[j] = T(0);
+        break;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kEntryUnroll; ++j)
+      if (e0.id[j] >= 0) acc += e0.c[j] * xv[j];
     for (int k = e0.k0 + kEntryUnroll * gw; k < e0.k1; k += gw)
       acc += __ldg(&coef[k]) * wait_value(&out[(size_t)__ldg(&idx[k]) * vs], st, poll_mode);
     __syncwarp();  // reconverge after the divergent waits before the shuffles
