@@ -58,14 +58,52 @@ def build_workload():
     return a, ldli, time.perf_counter() - t
 
 
+def build_workload_host_only():
+    """The same graph and factor without the GPU library: the generators
+    module is loaded by path (plain numpy/scipy, not through the acgpu package,
+    whose import maps libacgpu.so) and the host elimination comes from
+    libacghost.so, the CUDA-free host part of the product (the elimination
+    stays on the host in both arms and is not timed)."""
+    import importlib.util
+    import types
+    spec = importlib.util.spec_from_file_location(
+        "acg_generators", ROOT / "laplacians.jl_b200" / "acgpu" / "generators.py")
+    G = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(G)
+    a = G.grid3(GRID_SIDE, weights="loguniform", seed=WEIGHT_SEED)
+    L = ctypes.CDLL(str(ROOT / "laplacians.jl_b200" / "acgpu" / "libacghost.so"))
+    L.acg_last_error.restype = ctypes.c_char_p
+    state = np.zeros(4, dtype=np.uint64)
+    ptr = lambda arr: arr.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    if L.acg_rng_seed(ctypes.c_uint64(FACTOR_SEED), ptr(state)) != 0:
+        raise RuntimeError(L.acg_last_error().decode())
+    n = a.shape[0]
+    cp = a.indptr.astype(np.int64) + 1
+    rv = a.indices.astype(np.int64) + 1
+    nz = np.ascontiguousarray(a.data, dtype=np.float64)
+    h = ctypes.c_void_p()
+    t = time.perf_counter()
+    if L.acg_approxchol(ctypes.c_int64(n), ptr(cp), ptr(rv), ptr(nz), ptr(state), ctypes.byref(h)) != 0:
+        raise RuntimeError(L.acg_last_error().decode())
+    factor_s = time.perf_counter() - t
+    nn, F = ctypes.c_int64(), ctypes.c_int64()
+    L.acg_factor_dims(h, ctypes.byref(nn), ctypes.byref(F))
+    f = types.SimpleNamespace(col=np.empty(n - 1, np.int64), colptr=np.empty(n, np.int64),
+                              rowval=np.empty(F.value, np.int64), fval=np.empty(F.value), d=np.empty(n))
+    L.acg_factor_export(h, ptr(f.col), ptr(f.colptr), ptr(f.rowval), ptr(f.fval), ptr(f.d))
+    L.acg_factor_free(h)
+    f.n, f.nnz = n, F.value
+    return a, f, factor_s
+
+
 def rhs(n, seed):
     b = np.random.default_rng(seed).standard_normal(n)
     return b - b.mean()
 
 
-def config(n, extra=None):
+def config(n, extra=None, precision="fp32 PCG in fp64 refinement"):
     c = {"workload": f"grid3({GRID_SIDE}) log-uniform weights [1e-3,1], 1 zero-mean Gaussian RHS per solve, tol 1e-8",
-         "n": n, "precision": "fp32 PCG in fp64 refinement",
+         "n": n, "precision": precision,
          "l2": "inputs larger than L2 (factor + Laplacian > 126 MB), no flush"}
     if extra:
         c.update(extra)
@@ -125,12 +163,11 @@ class ClockSampler:
 
 # ---- CPU baseline (the oracle port) ------------------------------------------
 
-def cpu_solve_time(a, ldli, b, its_hint, budget_s=25.0):
+def cpu_solve_time(orc, b, its_hint, budget_s=25.0):
     """One-thread time of one solve of the workload with the CPU restatement.
-    Runs the full solve when it fits the budget; otherwise times a bounded
-    number of PCG iterations and scales to its_hint iterations."""
-    import oracle as O
-    orc = O.OracleSolver(a, ldli)
+    Runs the full solve when it fits the budget (then also returns its x and
+    iteration count); otherwise times a bounded number of PCG iterations and
+    scales to its_hint iterations."""
     t = time.perf_counter()
     orc(b, tol=TOL, maxits=2)
     t2 = time.perf_counter() - t
@@ -138,13 +175,47 @@ def cpu_solve_time(a, ldli, b, its_hint, budget_s=25.0):
     full = per_it * (its_hint + 1)
     if full <= budget_s:
         t = time.perf_counter()
-        _, its, _, _ = orc(b, tol=TOL, maxits=MAXITS)
-        return time.perf_counter() - t, f"one full solve at tol 1e-8 ({its} PCG iterations, FP64)"
+        x, its, _, _ = orc(b, tol=TOL, maxits=MAXITS)
+        return time.perf_counter() - t, f"one full solve at tol 1e-8 ({its} PCG iterations, FP64)", x, its
     m = max(2, int(budget_s / per_it) - 1)
     t = time.perf_counter()
     orc(b, tol=0.0, maxits=m)
     el = time.perf_counter() - t
-    return el / (m + 1) * (its_hint + 1), f"{m} FP64 PCG iterations timed, scaled to {its_hint} iterations"
+    return el / (m + 1) * (its_hint + 1), f"{m} FP64 PCG iterations timed, scaled to {its_hint} iterations", None, None
+
+
+def _rel_centered(x, y):
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    x = x - x.mean()
+    y = y - y.mean()
+    return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+
+
+def oracle_leg(a, ldli, dev, b_cols, x_mixed, its_hint):
+    """The CPU baseline leg: the oracle (the C restatement of the reference's
+    pcg + LDLsolver) times one full solve of the workload on one thread, and
+    checks the GPU on the same factor (outside every timed region):
+      * the FP64 GPU PCG on that right-hand side against the oracle's solve at
+        tol 1e-8: iteration counts and x (mean removed);
+      * the mixed-precision solutions of the timed run (two of its columns)
+        against the oracle's FP64 PCG to tol 1e-12."""
+    import oracle as O
+    orc = O.OracleSolver(a, ldli)
+    t_cpu, sample, xo, ito = cpu_solve_time(orc, b_cols[0], its_hint)
+    cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": 1, "kind": "port", "sample": sample}
+    check = {"oracle": "oracle/acg_oracle.c (FP64 pcg + LDLsolver restatement) on the same LDLinv"}
+    if xo is not None:
+        x64 = dev(b_cols[0], tol=TOL, maxits=MAXITS, precision="fp64")
+        check["fp64_gpu_vs_oracle_tol_1e-8"] = {"gpu_its": int(dev.last_info[0].iterations), "oracle_its": int(ito),
+                                               "x_rel_diff": _rel_centered(x64, xo)}
+    errs = []
+    for c in range(len(b_cols)):
+        xe, ite, rce, _ = orc(b_cols[c], tol=1e-12, maxits=4 * MAXITS)
+        errs.append({"column": c, "mixed_x_rel_error": _rel_centered(x_mixed[c], xe), "oracle_its": int(ite),
+                     "oracle_true_relres": O.relres(a, xe, b_cols[c])})
+    check["mixed_vs_oracle_tol_1e-12"] = errs
+    return cpu, check
 
 
 # ---- arms -------------------------------------------------------------------------
@@ -211,13 +282,14 @@ def run_acgpu(args):
     X = torch.empty((k, n), dtype=torch.float64, device="cuda")
     infos = (AcgSolveInfo * k)()
 
-    def solve_step(i):
+    def solve_step(i, prec_override=None):
+        pr = prec if prec_override is None else prec_override
         if k == 1:
             rc = L.acg_solve_device(dev._h, ctypes.c_void_p(B[i].data_ptr()), ctypes.c_void_p(X.data_ptr()), TOL,
-                                    MAXITS, float("inf"), 5, prec, infos)
+                                    MAXITS, float("inf"), 5, pr, infos)
         else:
             rc = L.acg_solve_batch_device(dev._h, ctypes.c_void_p(B[i].data_ptr()), ctypes.c_void_p(X.data_ptr()),
-                                          k, n, TOL, MAXITS, float("inf"), 5, prec, infos)
+                                          k, n, TOL, MAXITS, float("inf"), 5, pr, infos)
         check(rc)
         return [(infos[c].iterations, infos[c].refinements, infos[c].true_relres, infos[c].status) for c in range(k)]
 
@@ -246,24 +318,30 @@ def run_acgpu(args):
     refs = np.array([r[1] for r in results], dtype=float)
     res = np.array([r[2] for r in results])
 
-    # error against an FP64 reference solution (outside the timed region): the
-    # last step's right-hand sides solved again by the FP64 PCG to 1e-12 on
-    # the same factor; x is compared after removing its mean (L's null space)
-    X64 = torch.empty_like(X)
-    infos64 = (AcgSolveInfo * k)()
+    # the mixed solutions of the last timed step, checked against the oracle below
+    X_last = X.clone()
     last = nsteps - 1
-    if k == 1:
-        check(L.acg_solve_device(dev._h, ctypes.c_void_p(B[last].data_ptr()), ctypes.c_void_p(X64.data_ptr()),
-                                 1e-12, MAXITS, float("inf"), 5, 0, infos64))
-    else:
-        check(L.acg_solve_batch_device(dev._h, ctypes.c_void_p(B[last].data_ptr()), ctypes.c_void_p(X64.data_ptr()),
-                                       k, n, 1e-12, MAXITS, float("inf"), 5, 0, infos64))
-    torch.cuda.synchronize()
-    xc = X - X.mean(dim=1, keepdim=True)
-    xr = X64 - X64.mean(dim=1, keepdim=True)
-    err_fp64 = float(((xc - xr).norm(dim=1) / xr.norm(dim=1)).max())
-    ref_relres = max(infos64[c].true_relres for c in range(k))
-    ref_converged = sum(1 for c in range(k) if infos64[c].status == 0)
+
+    # the plain FP64 GPU path on the same batched workload (device-resident
+    # right-hand sides, the same steps): the metric's "mixed vs FP64" arm
+    fp64 = None
+    if not args.no_extras:
+        fsteps = min(args.steps, 3)
+        solve_step(0, prec_override=0)  # captures the FP64 graphs
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record()
+        fres = []
+        for i in range(args.warmup, args.warmup + fsteps):
+            fres += solve_step(i, prec_override=0)
+        f1.record()
+        torch.cuda.synchronize()
+        fms = max_over_ranks(f0.elapsed_time(f1), world)
+        fbad = [r for r in fres if r[3] != 0 or r[2] > TOL]
+        fp64 = {"solves_per_s": world * fsteps * k / (fms * 1e-3), "steps": fsteps, "ms_per_step": fms / fsteps,
+                "pcg_iterations_mean": float(np.mean([r[0] for r in fres])),
+                "true_relres_max": float(max(r[2] for r in fres)), "all_converged": not fbad}
 
     # end to end: pinned host blocks through the asynchronous C entry
     # (acg_solve_async / acg_wait), every step's H2D and D2H inside the timed
@@ -349,11 +427,18 @@ def run_acgpu(args):
     per_ref = 6 + 2 * kt["forward_launches"]
     launches = args.steps * (3 + refs.max() * per_ref + its.max() * per_it)
 
+    extras = {}
+    if not args.no_extras:
+        extras = run_extras(args, rank, world)
+
     if rank == 0:
         cpu = None
+        oracle_check = None
         if world == 1 and not args.no_cpu:
-            t_cpu, sample = cpu_solve_time(a, ldli, rhs(n, 424242), int(round(its.mean())))
-            cpu = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": 1, "kind": "port", "sample": sample}
+            ncheck = min(2, k)
+            b_cols = [B[last, c].cpu().numpy() for c in range(ncheck)]
+            x_mixed = [X_last[c].cpu().numpy() for c in range(ncheck)]
+            cpu, oracle_check = oracle_leg(a, ldli, dev, b_cols, x_mixed, int(round(its.mean())))
         value = world * args.steps * k / (ms * 1e-3)
         kern = (f"kb_sweep<float,{k // 8 if k >= 8 else 1},{direction}> (batched LDLinv {direction} sweep, {k} columns)"
                 if k > 1 else f"k_sweep<float,{direction}> (LDLinv {direction} sweep)")
@@ -366,12 +451,11 @@ def run_acgpu(args):
                                  "batching": f"{k} independent single-RHS solves per step in one batched launch",
                                  "pcg_iterations_mean": float(its.mean()), "refinements_mean": float(refs.mean()),
                                  "true_relres_max": float(res.max()), "factor_s": factor_s, "upload_s": upload_s,
-                                 "levels": stats["levels"], "factor_nnz": stats["nnz_factor"],
-                                 "error_vs_fp64_reference": {
-                                     "max_rel_error": err_fp64, "reference_true_relres_max": ref_relres,
-                                     "reference_columns_converged": ref_converged,
-                                     "reference": "FP64 PCG to 1e-12 on the same LDLinv (this library's FP64 "
-                                                  "path), last step's right-hand sides, x with its mean removed"}}),
+                                 "levels": stats["levels"], "factor_nnz": stats["nnz_factor"]}),
+            "fp64_batched": fp64,
+            "mixed_over_fp64": (value / fp64["solves_per_s"]) if fp64 else None,
+            "oracle_check": oracle_check,
+            **extras,
             "single_rhs": {"latency_ms": float(np.median(single)), "solves_per_s": 1e3 / float(np.median(single))},
             "e2e": {"value": world * args.steps * k / (e2e_ms * 1e-3), "unit": "solves/s",
                     "h2d_bytes_per_step": 8 * n * k, "d2h_bytes_per_step": 8 * n * k},
@@ -429,29 +513,8 @@ def run_grid2_200(args):
 def run_matchings_2m(args):
     """Path over a random permutation + 4 random perfect matchings, n = 2M,
     lognormal(0, 2) weights; mixed precision to 1e-8; level count and LDLinv GB/s."""
-    import acgpu
-    from acgpu import generators as G
     n = 2_000_000 if GRID_SIDE == 100 else GRID_SIDE ** 3
-    a = G.path_plus_matchings(n, k=4, sigma=2.0, seed=3)
-    acgpu.seed(FACTOR_SEED)
-    t = time.perf_counter()
-    ldli = acgpu.approx_chol(a)
-    factor_s = time.perf_counter() - t
-    dev = acgpu.DeviceLapSolver(a, ldli)
-    b = rhs(n, 12)
-    out = {"workload": "path+4 matchings n=2M lognormal(0,2)", "n": n, "avg_degree": a.nnz / n,
-           "factor_nnz": ldli.nnz, "factor_s": factor_s, "levels": dev.stats()["levels"]}
-    for prec in ("mixed", "fp64"):
-        for _ in range(2):
-            x, info = _device_solve(dev, b, prec, TOL)
-        kt = dev.time_kernels(prec, reps=3)
-        out[prec] = {"solve_ms": info.solve_ms, "its": info.iterations, "refinements": info.refinements,
-                     "true_relres": info.true_relres, "status": info.status,
-                     "forward_ms": kt["forward_ms"], "backward_ms": kt["backward_ms"],
-                     "ldlinv_forward_gbs": kt["forward_bytes"] / (kt["forward_ms"] * 1e-3) / 1e9,
-                     "ldlinv_backward_gbs": kt["backward_bytes"] / (kt["backward_ms"] * 1e-3) / 1e9}
-    print(json.dumps(out), flush=True)
-    dev.close()
+    print(json.dumps(matchings_2m_record(n)), flush=True)
 
 
 def run_orderings(args):
@@ -599,22 +662,15 @@ def serving_graph_pool(count, seed):
     return pool
 
 
-def run_serving(args):
-    """Poisson stream of solve requests over a pool of cached graphs, 1-16
-    right-hand sides each, tol 1e-8: continuous batching (mixed precision)
-    against the unbatched FP64 GPU path (one request at a time, one RHS per solve)."""
-    import acgpu
+def serve_stream(pool, factors, nreq, rate, hbm_gb, seed=7):
+    """One Poisson stream of nreq requests (1-16 right-hand sides each, tol
+    1e-8) over the cached graphs of pool, served twice: continuous batching in
+    mixed precision, and the unbatched FP64 GPU path (one request at a time,
+    one right-hand side per solve).  Returns the latency/throughput record of
+    each."""
     from acgpu.serving import SolveServer
-    pool = serving_graph_pool(args.serving_graphs, seed=2024)
-    factors = {}
-    t = time.perf_counter()
-    for i, (gid, a) in enumerate(pool):
-        acgpu.seed(1000 + i)
-        factors[gid] = acgpu.approx_chol(a)
-    factor_s = time.perf_counter() - t
-    rng = np.random.default_rng(7)
-    nreq = args.serving_requests
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serving_rate, nreq))
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
     picks = rng.integers(len(pool), size=nreq)
     ks = rng.integers(1, 17, size=nreq)
     rhs_blocks = [np.random.default_rng(10_000 + r).standard_normal((pool[picks[r]][1].shape[0], int(ks[r])))
@@ -622,7 +678,7 @@ def run_serving(args):
     results = {}
     for label, kw in (("batched_mixed", dict(precision="mixed", slots=4)),
                       ("unbatched_fp64", dict(precision="fp64", slots=1, unbatched=True))):
-        server = SolveServer(hbm_budget=int(args.serving_hbm_gb * (1 << 30)), **kw)
+        server = SolveServer(hbm_budget=int(hbm_gb * (1 << 30)), **kw)
         for gid, a in pool:
             server.register(gid, a, ldli=factors[gid])
         with server:
@@ -644,13 +700,80 @@ def run_serving(args):
             st = server.latency_stats()
             st["true_relres_max"] = worst
             results[label] = st
+    results["speedup_solves_per_s"] = (results["batched_mixed"]["solves_per_s"] /
+                                       results["unbatched_fp64"]["solves_per_s"])
+    return results
+
+
+def factor_pool(pool, seed0):
+    import acgpu
+    factors = {}
+    t = time.perf_counter()
+    for i, (gid, a) in enumerate(pool):
+        acgpu.seed(seed0 + i)
+        factors[gid] = acgpu.approx_chol(a)
+    return factors, time.perf_counter() - t
+
+
+def run_serving(args):
+    """Poisson stream of solve requests over a pool of cached graphs, 1-16
+    right-hand sides each, tol 1e-8: continuous batching (mixed precision)
+    against the unbatched FP64 GPU path (one request at a time, one RHS per solve)."""
+    pool = serving_graph_pool(args.serving_graphs, seed=2024)
+    factors, factor_s = factor_pool(pool, 1000)
+    results = serve_stream(pool, factors, args.serving_requests, args.serving_rate, args.serving_hbm_gb)
     out = {"workload": "serving: Poisson arrivals, graphs from 2D/3D grids, matchings, RGG, "
                        "n log-uniform [1e3,1e6], lognormal(0,1) weights, 1-16 RHS, tol 1e-8",
-           "graphs": [(gid, int(a.shape[0])) for gid, a in pool], "requests": nreq,
-           "arrival_rate_per_s": args.serving_rate, "factor_s_total": factor_s, **results,
-           "speedup_solves_per_s": results["batched_mixed"]["solves_per_s"] / results["unbatched_fp64"]["solves_per_s"]}
+           "graphs": [(gid, int(a.shape[0])) for gid, a in pool], "requests": args.serving_requests,
+           "arrival_rate_per_s": args.serving_rate, "factor_s_total": factor_s, **results}
     print(json.dumps(out), flush=True)
 
+
+def matchings_2m_record(n=2_000_000):
+    """The 2,000,000-vertex path + 4 random perfect matchings graph
+    (lognormal(0, 2) weights): DAG level count, LDLinv sweep bandwidth and one
+    mixed and one FP64 solve to tol 1e-8 (one right-hand side)."""
+    import acgpu
+    from acgpu import generators as G
+    a = G.path_plus_matchings(n, k=4, sigma=2.0, seed=3)
+    acgpu.seed(FACTOR_SEED)
+    t = time.perf_counter()
+    ldli = acgpu.approx_chol(a)
+    factor_s = time.perf_counter() - t
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    b = rhs(n, 12)
+    out = {"workload": f"path + 4 random matchings, n={n}, lognormal(0,2) weights, 1 RHS, tol 1e-8", "n": n,
+           "avg_degree": a.nnz / n, "factor_nnz": ldli.nnz, "factor_s": factor_s, "levels": dev.stats()["levels"]}
+    for prec in ("mixed", "fp64"):
+        for _ in range(2):
+            x, info = _device_solve(dev, b, prec, TOL)
+        kt = dev.time_kernels(prec, reps=3)
+        out[prec] = {"solve_ms": info.solve_ms, "its": info.iterations, "refinements": info.refinements,
+                     "true_relres": info.true_relres, "status": info.status,
+                     "forward_ms": kt["forward_ms"], "backward_ms": kt["backward_ms"],
+                     "ldlinv_forward_gbs": kt["forward_bytes"] / (kt["forward_ms"] * 1e-3) / 1e9,
+                     "ldlinv_backward_gbs": kt["backward_bytes"] / (kt["backward_ms"] * 1e-3) / 1e9}
+    dev.close()
+    return out
+
+
+def run_extras(args, rank, world):
+    """The rest of the metric, beside the headline (N = 1 only; each takes
+    seconds): serving p50/p99 on a short Poisson stream, and the 2M
+    path+matchings graph's level count and LDLinv GB/s."""
+    if world > 1 or rank != 0:
+        return {}
+    out = {}
+    pool = serving_graph_pool(8, seed=2024)
+    factors, factor_s = factor_pool(pool, 1000)
+    t = time.perf_counter()
+    res = serve_stream(pool, factors, 100, 40.0, args.serving_hbm_gb)
+    out["serving"] = {"workload": "100 requests, Poisson 40/s, 8 cached graphs (2D/3D grids, matchings, RGG, "
+                                  "n log-uniform [1e3,1e6], lognormal(0,1) weights), 1-16 RHS each, tol 1e-8",
+                      "graphs": [(gid, int(a.shape[0])) for gid, a in pool], "factor_s_total": factor_s,
+                      "wall_s": time.perf_counter() - t, **res}
+    out["path_matchings_2m"] = matchings_2m_record()
+    return out
 
 
 def run_reference(args):
@@ -661,7 +784,7 @@ def run_reference(args):
     if rank != 0:
         return
     import oracle as O
-    a, ldli, factor_s = build_workload()
+    a, ldli, factor_s = build_workload_host_only()
     n = a.shape[0]
     threads = max(1, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count())
     solver = O.OracleSolver(a, ldli)  # read-only; the C solve keeps its state on the stack/heap per call
@@ -699,7 +822,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config(n, {"parallelism": f"{threads} host threads", "factor_s": factor_s}),
+            "config": config(n, {"parallelism": f"{threads} host threads", "factor_s": factor_s},
+                             precision="fp64 PCG (CPU restatement of the reference's solve)"),
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -712,7 +836,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="acgpu", choices=["acgpu", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg (and its oracle check)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the extra keys (FP64 arm, serving latency, 2M path+matchings graph)")
     ap.add_argument("--side", type=int, default=GRID_SIDE, help="grid side (100 = the benchmark workload)")
     ap.add_argument("--rhs", type=int, default=64, help="independent right-hand sides per step (batched)")
     ap.add_argument("--workload", default="grid3",

@@ -129,6 +129,13 @@ typedef struct {
   int sweep_stride;          /* 1 = one value per vertex in the one-vector sweep vectors;
                                 0 = one 32-byte sector per vertex (faster: values that
                                 different SMs write at once never share a sector)     */
+  int spin_limit;            /* polls of a pending value before a sweep wait gives up and
+                                the solve returns ACG_ERR_TIMEOUT (0 = 4,194,304, a few
+                                seconds)                                                */
+  int test_unproduced_task;  /* testing only (0 = off): k > 0 blanks the k-th record of
+                                the forward sweep tables, so its vertices' values are never
+                                produced and the waits on them run out; a test of the
+                                bounded waits that neither faults nor hangs the GPU     */
 } acg_options;
 
 /* Shape of an uploaded solver. */
@@ -285,7 +292,10 @@ int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg
  * reduction tickets) itself.  Every call shares the one array: calls whose work
  * overlaps on the GPU (different streams, or different solvers, at the same
  * time) race and corrupt each other's results.  Graphs with more than
- * ACG_NOALLOC_MAX_N vertices are rejected with ACG_ERR_INVALID. */
+ * ACG_NOALLOC_MAX_N vertices are rejected with ACG_ERR_INVALID, and so are a
+ * group solver (acg_create_group), a current device other than the solver's
+ * and a stream that belongs to another device: the call checks these on the
+ * host before it enqueues anything. */
 #define ACG_NOALLOC_MAX_N 131072
 int acg_ldlsolve_noalloc(acg_solver* h, const double* r_dev, double* y_dev, int precision, void* stream);
 

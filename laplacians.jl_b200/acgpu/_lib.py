@@ -32,7 +32,8 @@ class AcgOptions(ctypes.Structure):
                 ("sweep_blocks_per_sm", ctypes.c_int), ("poll_mode", ctypes.c_int), ("tail", ctypes.c_int),
                 ("batch_bwd_heavy", ctypes.c_int), ("batch_fwd_heavy", ctypes.c_int),
                 ("batch_blocks_per_sm", ctypes.c_int), ("sweep_heavy", ctypes.c_int),
-                ("dense_tail", ctypes.c_int), ("sweep_stride", ctypes.c_int)]
+                ("dense_tail", ctypes.c_int), ("sweep_stride", ctypes.c_int),
+                ("spin_limit", ctypes.c_int), ("test_unproduced_task", ctypes.c_int)]
 
 
 class AcgStats(ctypes.Structure):

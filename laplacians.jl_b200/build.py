@@ -4,7 +4,11 @@
 
 Host C++ (the elimination, the Julia-compatible random stream, the C ABI) and
 the CUDA kernels are compiled by nvcc into one shared library that exports
-the symbols declared in include/acgpu.h.
+the symbols declared in include/acgpu.h.  The host part alone (the "host"
+sections of include/acgpu.h: random stream, elimination, LDLinv files) is
+also linked into libacghost.so, which needs no CUDA runtime: a CPU-only
+caller (the benchmark's reference arm) builds factors with it without
+mapping the GPU library.
 """
 from __future__ import annotations
 
@@ -17,6 +21,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "acgpu" / "libacgpu.so"
+HOST_OUT = PKG / "acgpu" / "libacghost.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CU_SOURCES = ["acg_solver.cu"]
@@ -32,9 +37,9 @@ def _sources():
 
 
 def up_to_date() -> bool:
-    if not OUT.exists():
+    if not OUT.exists() or not HOST_OUT.exists():
         return False
-    t = OUT.stat().st_mtime
+    t = min(OUT.stat().st_mtime, HOST_OUT.stat().st_mtime)
     return all(p.stat().st_mtime <= t for p in _sources())
 
 
@@ -50,6 +55,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         cmd = [NVCC, *common, "-Xcompiler", "-ffp-contract=off", "-x", "c++", "-c", str(CSRC / src), "-o", str(obj)]
         _run(cmd, verbose)
         objs.append(obj)
+    host_tmp = HOST_OUT.with_suffix(".so.tmp")
+    _run([NVCC, "-shared", "-o", str(host_tmp), *map(str, objs)], verbose)
+    os.replace(host_tmp, HOST_OUT)
     for src in CU_SOURCES:
         obj = objdir / (src + ".o")
         cmd = [NVCC, *common, *GENCODE, "-lineinfo", "-c", str(CSRC / src), "-o", str(obj)]

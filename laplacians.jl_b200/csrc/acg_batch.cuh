@@ -204,7 +204,7 @@ template <typename T, int CPL, bool kForward>
 __global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>())
     kb_sweep(int ntasks, const SweepTask* __restrict__ tasks, const int* __restrict__ idx,
              const T* __restrict__ coef, const T* __restrict__ aux, const T* sfwd, T* out, T* mark,
-             BatchShared* bs) {
+             BatchShared* bs, unsigned spin_limit) {
   if (bs->all_done) return;
   constexpr int kp = CPL * kBatchLanes;
   // rows loaded per batch: a whole slot of 8 entries where registers allow
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>())
         // had become ready during the earlier waits (measured on the 1M grid
         // at 64 columns: backward 0.953 -> 0.823 ms, forward 0.816 -> 0.789
         // ms).  A row read ready is final: rows are written once per sweep.
-        // The wait is bounded: after kSpinLimit rounds, or once another wait
+        // The wait is bounded: after spin_limit rounds, or once another wait
         // has given up, the sweep error is raised and the rows still pending
         // read as zeros.
         for (unsigned int spins = 1; pend; ++spins) {
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>())
           for (int u = 0; u < EB; ++u)
             if (((pend >> u) & 1u) && row_pending(vals[u])) still |= 1u << u;
           pend = still;
-          if (pend && (((spins & 1023u) == 0 && *((volatile int*)&bs->sweep_error)) || spins >= kSpinLimit)) {
+          if (pend && (((spins & 1023u) == 0 && *((volatile int*)&bs->sweep_error)) || spins >= spin_limit)) {
             atomicExch(&bs->sweep_error, 1);
 #pragma unroll
             for (int u = 0; u < EB; ++u)
@@ -856,6 +856,9 @@ __global__ void __launch_bounds__(kVecThreads) kb_center(int n, int kp, double* 
         s->nr = 0.0;
         s->outer_done = 1;
         mark_stop(s, kConverged);
+      } else if (!isfinite(s->nb)) {  // a NaN or Inf entry in this column
+        s->outer_done = 1;
+        mark_stop(s, kBadInput);
       }
     }
     if (threadIdx.x == 0) {

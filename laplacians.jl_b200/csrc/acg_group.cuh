@@ -256,6 +256,9 @@ __global__ void __launch_bounds__(kVecThreads) kg_center(double* __restrict__ bm
       s->nr = 0.0;
       mark_stop(s, kConverged);
       seg_stopped(g, ctl);
+    } else if (!isfinite(s->nb)) {  // a NaN or Inf entry in this graph's right-hand side
+      mark_stop(s, kBadInput);
+      seg_stopped(g, ctl);
     }
   }
 }

@@ -344,7 +344,8 @@ __global__ void __launch_bounds__(kThinThreads, 1) k_thin(int l0, int l1, const 
 // level order (task t by warp t mod W); a task's inputs come from strictly
 // earlier tasks, so with all warps co-resident (cooperative launch) the
 // earliest unfinished task can always proceed.  Each wait polls the L2 copy
-// with relaxed GPU-scope loads and gives up after kSpinLimit polls, raising
+// with relaxed GPU-scope loads and gives up after spin_limit polls (a launch
+// argument, kSpinLimit unless the solver's options set another), raising
 // PcgState::sweep_error instead of hanging.
 constexpr unsigned int kPendingF32 = 0x7fc0deadu;
 constexpr unsigned long long kPendingF64 = 0x7ff8dead0000deadull;
@@ -382,7 +383,7 @@ __device__ __forceinline__ void st_relaxed(double* p, double v) {
 // Poll until the value is no longer pending.  poll_mode 0: tight polls, then
 // 64 ns sleeps; 1: tight polls only; 2: exponential backoff 32 ns .. 1 us.
 template <typename T>
-__device__ __noinline__ T wait_value_slow(const T* p, PcgState* st, int poll_mode) {
+__device__ __noinline__ T wait_value_slow(const T* p, PcgState* st, int poll_mode, unsigned spin_limit) {
   unsigned int sleep_ns = 32;
   for (unsigned int spins = 1;; ++spins) {
     if (poll_mode == 0) {
@@ -396,7 +397,7 @@ __device__ __noinline__ T wait_value_slow(const T* p, PcgState* st, int poll_mod
     const T x = ld_relaxed(p);
     if (!is_pending(x)) return x;
     if ((spins & 1023u) == 0 && *((volatile int*)&st->sweep_error)) return T(0);
-    if (spins >= kSpinLimit) {
+    if (spins >= spin_limit) {
       atomicExch(&st->sweep_error, 1);
       return T(0);
     }
@@ -404,9 +405,9 @@ __device__ __noinline__ T wait_value_slow(const T* p, PcgState* st, int poll_mod
 }
 
 template <typename T>
-__device__ __forceinline__ T wait_value(const T* p, PcgState* st, int poll_mode) {
+__device__ __forceinline__ T wait_value(const T* p, PcgState* st, int poll_mode, unsigned spin_limit) {
   const T x = ld_relaxed(p);
-  return is_pending(x) ? wait_value_slow(p, st, poll_mode) : x;
+  return is_pending(x) ? wait_value_slow(p, st, poll_mode, spin_limit) : x;
 }
 
 // A task record (32 bytes): {first vertex, (count << 1) | heavy, p[0..4]} with
@@ -478,7 +479,8 @@ template <typename T, bool kForward>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const SweepTask* __restrict__ tasks,
                                                          const int* __restrict__ idx, const T* __restrict__ coef,
                                                          const T* __restrict__ aux, const T* __restrict__ sfwd, T* out,
-                                                         PcgState* st, int poll_mode, int vs) {
+                                                         PcgState* st, int poll_mode, int vs,
+                                                         unsigned spin_limit) {
   if (st->done) return;
   const int lane = threadIdx.x & 31;
   const int W = (int)((gridDim.x * blockDim.x) >> 5);
@@ -512,7 +514,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const Sweep
     } else {
 #pragma unroll
       for (int j = 0; j < kEntryUnroll; ++j)
-        if (e0.id[j] >= 0 && is_pending(xv[j])) xv[j] = wait_value_slow(&out[(size_t)e0.id[j] * vs], st, poll_mode);
+        if (e0.id[j] >= 0 && is_pending(xv[j])) xv[j] = wait_value_slow(&out[(size_t)e0.id[j] * vs], st, poll_mode, spin_limit);
     }
     unsigned int sleep_ns = 32;
     for (unsigned int spins = 1; pend; ++spins) {
@@ -532,7 +534,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const Sweep
       for (int j = 0; j < kEntryUnroll; ++j)
         if (((pend >> j) & 1u) && is_pending(xv[j])) still |= 1u << j;
       pend = still;
-      if (pend && (((spins & 1023u) == 0 && *((volatile int*)&st->sweep_error)) || spins >= kSpinLimit)) {
+      if (pend && (((spins & 1023u) == 0 && *((volatile int*)&st->sweep_error)) || spins >= spin_limit)) {
         atomicExch(&st->sweep_error, 1);
 #pragma unroll
         for (int j = 0; j < kEntryUnroll; ++j)
@@ -544,7 +546,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(int ntasks, const Sweep
     for (int j = 0; j < kEntryUnroll; ++j)
       if (e0.id[j] >= 0) acc += e0.c[j] * xv[j];
     for (int k = e0.k0 + kEntryUnroll * gw; k < e0.k1; k += gw)
-      acc += __ldg(&coef[k]) * wait_value(&out[(size_t)__ldg(&idx[k]) * vs], st, poll_mode);
+      acc += __ldg(&coef[k]) * wait_value(&out[(size_t)__ldg(&idx[k]) * vs], st, poll_mode, spin_limit);
     __syncwarp();  // reconverge after the divergent waits before the shuffles
     acc = group_sum_w(acc, gw);
     if (e0.active && (lane & (gw - 1)) == 0) st_relaxed(&out[(size_t)e0.v * vs], kForward ? e0.a + acc : e0.a * e0.own + acc);

@@ -23,7 +23,8 @@ namespace acg {
 
 enum StopCode {
   kConverged = 0, kMaxits = 1, kStagX = 2, kStagR = 3, kStagRho = 4, kInf = 5, kStagP = 6, kMaxtime = 7,
-  kSweepTimeout = 100  // a bounded device wait of a sweep gave up (reported as an error)
+  kSweepTimeout = 100,  // a bounded device wait of a sweep gave up (reported as an error)
+  kBadInput = 101       // the right-hand side has a NaN or infinite entry (reported as an error)
 };
 
 struct LoopCtl {
@@ -291,6 +292,8 @@ __global__ void __launch_bounds__(kVecThreads) k_center(int n, double* __restric
       st->nr_true = 0.0;
       st->nr = 0.0;
       pcg_stop(st, kConverged, ctl);
+    } else if (!isfinite(st->nb)) {
+      pcg_stop(st, kBadInput, ctl);  // |b| sums every entry: a NaN or Inf shows here
     }
   }
 }

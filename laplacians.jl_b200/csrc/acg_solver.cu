@@ -107,6 +107,7 @@ struct SolverImpl {
   int ntasks_f = 0, ntasks_b = 0;
   int sweep_blocks[2] = {0, 0};    // co-resident grid of k_sweep per value type
   int poll_mode = 0;
+  unsigned spin_limit = kSpinLimit;  // polls before a sweep wait gives up
   DevBuf<SweepTask> tasks_f, tasks_b;
 
   DevBuf<int> perm, lvl_off_d;
@@ -308,7 +309,7 @@ void enqueue_syncfree(cudaStream_t s, const SolverImpl& S, const T* aux, const T
   cfg.numAttrs = 1;
   const SweepTask* tasks = (kForward ? S.tasks_f.p : S.tasks_b.p) + t0;
   ACG_CUDA(cudaLaunchKernelEx(&cfg, k_sweep<T, kForward>, t1 - t0, tasks, kForward ? A.fi : A.bi,
-                              kForward ? A.fc : A.bc, aux, sfwd, out, st, S.poll_mode, vs));
+                              kForward ? A.fc : A.bc, aux, sfwd, out, st, S.poll_mode, vs, S.spin_limit));
 }
 
 // The narrow tail of the DAG in one CTA.
@@ -571,6 +572,74 @@ std::vector<float> to_f32(const std::vector<T>& v) {
   std::vector<float> o(v.size());
   for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
   return o;
+}
+
+// Host-side checks of acg_create's inputs, run before any device work (so a
+// malformed factor is rejected with ACG_ERR_INVALID even where no GPU is
+// present): sizes and index bases; the adjacency's structure and weights
+// (finite, non-negative, no diagonal entries); the factor's structure (col a
+// set of distinct vertices, non-empty columns, colptr ending at F, rowval
+// naming only vertices eliminated later, i.e. an elimination order, and never
+// linking two graphs of a group); fval in [0, 1]; d finite and non-negative.
+// build_solver repeats the checks it depends on while it builds.
+void validate_inputs(int64_t n64, const int64_t* a_colptr, const int64_t* a_rowval, const double* a_nzval,
+                     const int64_t* col, int64_t ncol64, const int64_t* colptr, const int64_t* rowval,
+                     const double* fval, const double* d, int64_t F, int base, int64_t nseg,
+                     const int64_t* seg_off) {
+  if (n64 < 2 || n64 >= (int64_t)INT32_MAX) throw InputError("n must be in [2, 2^31-1)");
+  if (base != 0 && base != 1) throw InputError("index_base must be 0 or 1");
+  const int64_t n = n64;
+  if (nseg < 1 || nseg > n) throw InputError("graph count out of range");
+  if (ncol64 < 1 || ncol64 > n - 1) throw InputError("factor column count out of range");
+  std::vector<int> seg_of(n, 0);
+  if (seg_off) {
+    if (seg_off[0] != 0 || seg_off[nseg] != n64) throw InputError("graph offsets must start at 0 and end at n");
+    for (int64_t g = 0; g < nseg; ++g) {
+      if (seg_off[g + 1] - seg_off[g] < 2) throw InputError("every graph of a group needs at least 2 vertices");
+      for (int64_t v = seg_off[g]; v < seg_off[g + 1]; ++v) seg_of[v] = (int)g;
+    }
+  }
+  const int64_t abase = a_colptr[0];
+  if (abase != 0 && abase != 1) throw InputError("adjacency colptr[0] must be 0 or 1");
+  const int64_t m = a_colptr[n] - abase;
+  if (m < 0 || m + n >= (int64_t)INT32_MAX) throw InputError("adjacency too large for 32-bit indices");
+  for (int64_t c = 0; c < n; ++c) {
+    if (a_colptr[c + 1] < a_colptr[c]) throw InputError("adjacency colptr not monotone");
+    for (int64_t k = a_colptr[c] - abase; k < a_colptr[c + 1] - abase; ++k) {
+      const int64_t r = a_rowval[k] - abase;
+      if (r < 0 || r >= n) throw InputError("adjacency row index out of range");
+      if (r == c) throw InputError("adjacency matrix has a diagonal entry");
+      const double w = a_nzval[k];
+      if (!(w >= 0.0) || std::isinf(w)) throw InputError("Adjacency matrix can not have negative edge weights");
+    }
+  }
+  if (F < ncol64 || F >= (int64_t)INT32_MAX) throw InputError("factor size F out of range");
+  std::vector<int64_t> step(n, -1);
+  for (int64_t ii = 0; ii < ncol64; ++ii) {
+    const int64_t u = col[ii] - base;
+    if (u < 0 || u >= n) throw InputError("ldli.col entry out of range");
+    if (step[u] != -1) throw InputError("ldli.col repeats a vertex");
+    step[u] = ii;
+  }
+  for (int64_t v = 0; v < n; ++v)
+    if (step[v] == -1) step[v] = ncol64;  // roots come after every eliminated column
+  if (colptr[0] - base != 0) throw InputError("ldli.colptr[1] must point at the first entry");
+  for (int64_t ii = 0; ii < ncol64; ++ii)
+    if (colptr[ii + 1] <= colptr[ii]) throw InputError("ldli column " + std::to_string(ii + 1) + " is empty");
+  if (colptr[ncol64] - base != F) throw InputError("ldli.colptr[end] must equal F+1 (1-based)");
+  for (int64_t ii = 0; ii < ncol64; ++ii) {
+    const int64_t u = col[ii] - base;
+    for (int64_t e = colptr[ii] - base; e < colptr[ii + 1] - base; ++e) {
+      const int64_t j = rowval[e] - base;
+      if (j < 0 || j >= n) throw InputError("ldli.rowval entry out of range");
+      if (step[j] <= ii) throw InputError("ldli.rowval names a vertex eliminated earlier (not an elimination order)");
+      if (seg_of[j] != seg_of[u]) throw InputError("a factor column links two different graphs of the group");
+      const double f = fval[e];
+      if (!(f >= 0.0 && f <= 1.0)) throw InputError("ldli.fval entries must lie in [0, 1]");
+    }
+  }
+  for (int64_t v = 0; v < n; ++v)
+    if (!(d[v] >= 0.0) || std::isinf(d[v])) throw InputError("ldli.d must be finite and non-negative");
 }
 
 // Builds the device solver for one graph, or for the block-diagonal union of
@@ -969,6 +1038,18 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
         for (const auto& r : runs[l]) emit_level(tbb, r.first, r.second, outdeg, bptr, bheavy);
       for (int l = 0; l < nlev; ++l)
         for (const auto& r : runs[l]) emit_level(tfb, r.first, r.second, fdeg, fptr, fheavy);
+      // Testing only: blank one forward task record (it stores nothing), so
+      // the values of its vertices are never produced and the waits on them
+      // run out after spin_limit polls; the solve then reports
+      // ACG_ERR_TIMEOUT.  This is how the bounded waits are tested without
+      // faulting or hanging the GPU.
+      const int blank = opts ? opts->test_unproduced_task : 0;
+      if (blank > 0) {
+        if (blank > (int)tf.size() || blank > (int)tfb.size())
+          throw InputError("test_unproduced_task is beyond the forward task tables");
+        tf[blank - 1].cnt_heavy = 0;
+        tfb[blank - 1].cnt_heavy = 0;
+      }
       S.ntasks_bb = (int)tbb.size();
       S.tasks_bb.upload(tbb, S.stream);
       S.ntasks_fb = (int)tfb.size();
@@ -1005,6 +1086,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     S.sweep_blocks[1] = sms * std::max(1, std::min(cap, std::min(occ[2], occ[3])));
     S.sweep_mode = (opts && opts->sweep_lanes == 1 && nseg == 1) ? 1 : 0;
     if (opts && opts->poll_mode > 0) S.poll_mode = opts->poll_mode - 1;
+    if (opts && opts->spin_limit > 0) S.spin_limit = (unsigned)opts->spin_limit;
     S.batch_bps = (opts && opts->batch_blocks_per_sm > 0) ? opts->batch_blocks_per_sm : 0;
   }
   ACG_CUDA(cudaFuncSetAttribute(k_thin<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
@@ -1320,6 +1402,10 @@ int status_to_rc(int status) {
     set_last_error("a bounded wait of a sync-free LDLinv sweep gave up; the solve was abandoned");
     return ACG_ERR_TIMEOUT;
   }
+  if (status == kBadInput) {
+    set_last_error("the right-hand side has a NaN or infinite entry; x is left at zero");
+    return ACG_ERR_INVALID;
+  }
   return status;
 }
 
@@ -1354,7 +1440,7 @@ void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, T* sfwd, 
   cfg.numAttrs = 1;
   ACG_CUDA(cudaLaunchKernelEx(&cfg, kb_sweep<T, CPL, kForward>, kForward ? S.ntasks_fb : S.ntasks_bb,
                               (const SweepTask*)(kForward ? S.tasks_fb.p : S.tasks_bb.p), kForward ? A.fi : A.bi,
-                              kForward ? A.fc : A.bc, aux, (const T*)sfwd, out, mark, S.bsh));
+                              kForward ? A.fc : A.bc, aux, (const T*)sfwd, out, mark, S.bsh, S.spin_limit));
 }
 
 // Batched forward (s from r) and backward (y from s) sweeps, dense tail included.
@@ -2089,7 +2175,13 @@ int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, cons
     return ACG_ERR_INVALID;
   }
   *out = nullptr;
-  int rc = check_device();
+  int rc = guarded("acg_create", [&]() {
+    acg::validate_inputs(n, a_colptr, a_rowval, a_nzval, ldli_col, n - 1, ldli_colptr, ldli_rowval, ldli_fval,
+                         ldli_d, ldli_nnz, index_base, 1, nullptr);
+    return ACG_OK;
+  });
+  if (rc != ACG_OK) return rc;
+  rc = check_device();
   if (rc != ACG_OK) return rc;
   return guarded("acg_create", [&]() {
     std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
@@ -2249,7 +2341,13 @@ int acg_create_group(int64_t ngraphs, const int64_t* offsets, int64_t n, const i
     return ACG_ERR_INVALID;
   }
   *out = nullptr;
-  int rc = check_device();
+  int rc = guarded("acg_create_group", [&]() {
+    acg::validate_inputs(n, a_colptr, a_rowval, a_nzval, ldli_col, ncol, ldli_colptr, ldli_rowval, ldli_fval, ldli_d,
+                         ldli_nnz, index_base, ngraphs, offsets);
+    return ACG_OK;
+  });
+  if (rc != ACG_OK) return rc;
+  rc = check_device();
   if (rc != ACG_OK) return rc;
   return guarded("acg_create_group", [&]() {
     std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
@@ -2370,6 +2468,10 @@ int acg_ldlsolve_noalloc(acg_solver* h, const double* r_dev, double* y_dev, int 
                         " vertices; the fixed scratch array holds at most " + std::to_string(ACG_NOALLOC_MAX_N));
     return ACG_ERR_INVALID;
   }
+  if (h->impl.nseg > 1) {
+    acg::set_last_error("acg_ldlsolve_noalloc: needs a one-graph solver from acg_create, not a group solver");
+    return ACG_ERR_INVALID;
+  }
   if (!h->impl.noalloc_scratch) {
     acg::set_last_error("acg_ldlsolve_noalloc: scratch address was not resolved at acg_create");
     return ACG_ERR_INVALID;
@@ -2377,6 +2479,21 @@ int acg_ldlsolve_noalloc(acg_solver* h, const double* r_dev, double* y_dev, int 
   return guarded("acg_ldlsolve_noalloc", [&]() {
     acg::SolverImpl& S = h->impl;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // The factor, the solver's arrays and the scratch address all live on the
+    // solver's device; work enqueued on another device would read them as
+    // foreign addresses.  Refuse instead of switching devices behind the caller.
+    int cur = -1;
+    ACG_CUDA(cudaGetDevice(&cur));
+    if (cur != S.device)
+      throw acg::InputError("the current device is " + std::to_string(cur) + " but the solver lives on device " +
+                            std::to_string(S.device));
+    if (s) {
+      int sdev = -1;
+      ACG_CUDA(cudaStreamGetDevice(s, &sdev));
+      if (sdev != S.device)
+        throw acg::InputError("the stream belongs to device " + std::to_string(sdev) +
+                              " but the solver lives on device " + std::to_string(S.device));
+    }
     if (precision == 0) acg::ldlsolve_noalloc_impl<double>(S, s, r_dev, y_dev, S.noalloc_scratch);
     else acg::ldlsolve_noalloc_impl<float>(S, s, r_dev, y_dev, S.noalloc_scratch);
     ACG_CUDA(cudaGetLastError());

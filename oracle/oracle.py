@@ -40,7 +40,7 @@ def build(force: bool = False) -> Path:
     if LIB.exists() and not force and LIB.stat().st_mtime >= SRC.stat().st_mtime:
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    subprocess.run(["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fPIC", "-shared", str(SRC), "-o", str(tmp),
+    subprocess.run(["gcc", "-O3", "-std=c11", "-ffp-contract=off", "-fPIC", "-shared", str(SRC), "-o", str(tmp),
                     "-lm"], check=True)
     tmp.replace(LIB)
     return LIB
@@ -134,6 +134,49 @@ class OracleSolver:
         mi = (1 << 62) if maxits == float("inf") else int(maxits)
         rc = fn(ctypes.byref(self.prob), b, x, tol, mi, maxtime, self.stag_test, ctypes.byref(its), ctypes.byref(nr))
         return x, its.value, rc, nr.value
+
+
+def _magnitude_second(ev, upper):
+    """The reference's lower eigenvalue: upper minus the second-largest
+    magnitude eigenvalue of upper*I - G (src/approxChol.jl:1931-1933)."""
+    shifted = upper - ev
+    order = np.argsort(-np.abs(shifted), kind="stable")
+    return upper - shifted[order[1]]
+
+
+def cond_number(a, ldli):
+    """condNumber(a, ldli) (src/approxChol.jl:1880-1936): upper/lower of the
+    operator g(b) = D^-1/2 forward!(lap(a) * backward!(D^-1/2 b)), entries with
+    d = 0 zeroed.  The reference estimates the two eigenvalues with ARPACK's
+    eigs at tol 1e-2; here g is formed densely (n up to a few thousand) and its
+    eigenvalues are exact, with the same choice of upper and lower: upper is
+    the largest, lower = upper minus the second-largest magnitude of upper - g."""
+    n = ldli.n
+    L = OracleLap(a)
+    d = np.asarray(ldli.d, dtype=np.float64)
+    dis = np.where(d != 0, 1.0 / np.sqrt(np.where(d != 0, d, 1.0)), 0.0)
+    lib_ = lib()
+    g = np.empty((n, n))
+    for j in range(n):
+        y = np.zeros(n)
+        y[j] = dis[j]
+        lib_.oracle_backward(n, ldli.col, ldli.colptr, ldli.rowval, ldli.fval, y)
+        y = np.ascontiguousarray(L.mul(y))
+        lib_.oracle_forward(n, ldli.col, ldli.colptr, ldli.rowval, ldli.fval, y)
+        g[:, j] = y * dis
+    ev = np.linalg.eigvalsh(0.5 * (g + g.T))
+    upper = float(ev[-1])
+    return upper / float(_magnitude_second(ev, upper))
+
+
+def cond_number_of_operator(m):
+    """The same upper/lower for a dense operator m = P lap(a) given column by
+    column (P a preconditioner applied on a device): its eigenvalues are those
+    of g up to rounding (P L and D^-1/2 U' L U D^-1/2 share their nonzero
+    eigenvalues), so the two condition numbers agree."""
+    ev = np.sort(np.linalg.eigvals(np.asarray(m, dtype=np.float64)).real)
+    upper = float(ev[-1])
+    return upper / float(_magnitude_second(ev, upper))
 
 
 def exact_solve(a, b):
