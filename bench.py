@@ -267,7 +267,7 @@ def run_acgpu(args):
     a, ldli, factor_s = build_workload()
     n = a.shape[0]
     t = time.perf_counter()
-    dev = acgpu.DeviceLapSolver(a, ldli)
+    dev = acgpu.DeviceLapSolver(a, ldli, options=json.loads(args.options) if args.options else None)
     upload_s = time.perf_counter() - t
     L = lib()
     prec = 1 if args.precision == "mixed" else 0
@@ -448,6 +448,7 @@ def run_acgpu(args):
             "vs_baseline": None, "dtype": "f32 (SpMV, sweeps) / f64 (residual, dots, correction)"
             if prec == 1 else "f64", "data": "synthetic (seeded grid weights and Gaussian RHS)",
             "config": config(n, {"parallelism": f"replicas x{world}", "rhs_per_step": k,
+                                 "solver_options": json.loads(args.options) if args.options else {},
                                  "batching": f"{k} independent single-RHS solves per step in one batched launch",
                                  "pcg_iterations_mean": float(its.mean()), "refinements_mean": float(refs.mean()),
                                  "true_relres_max": float(res.max()), "factor_s": factor_s, "upload_s": upload_s,
@@ -837,6 +838,7 @@ def main():
     ap.add_argument("--impl", default="acgpu", choices=["acgpu", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg (and its oracle check)")
+    ap.add_argument("--options", default="", help="acg_options knobs as JSON (tuning), e.g. '{\"level_order\": 1}'")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the extra keys (FP64 arm, serving latency, 2M path+matchings graph)")
     ap.add_argument("--side", type=int, default=GRID_SIDE, help="grid side (100 = the benchmark workload)")

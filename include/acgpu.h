@@ -129,6 +129,9 @@ typedef struct {
   int sweep_stride;          /* 1 = one value per vertex in the one-vector sweep vectors;
                                 0 = one 32-byte sector per vertex (faster: values that
                                 different SMs write at once never share a sector)     */
+  int level_order;           /* vertex order inside a DAG level: 0 = by decreasing in-degree,
+                                1 = by the caller's vertex id (keeps the caller's locality
+                                for the mat-vec and the sweeps' gathers)               */
   int spin_limit;            /* polls of a pending value before a sweep wait gives up and
                                 the solve returns ACG_ERR_TIMEOUT (0 = 4,194,304, a few
                                 seconds)                                                */
@@ -183,6 +186,11 @@ typedef struct {
   double forward_sweep_ms, backward_sweep_ms;
   double dense_ms;          /* both dense tail products (forward + backward) */
   double forward_sweep_bytes, backward_sweep_bytes, dense_bytes;
+  /* the batched loop body's vector kernels, one call each (acg_time_kernels_batch
+     only; 0 otherwise): p.q and |p|_1, |q|_1; the x and r update; the sums of
+     y, y.r and r; the p update; and their algorithmic bytes */
+  double pq_ms, update_ms, yzr_ms, pupdate_ms;
+  double pq_bytes, update_bytes, yzr_bytes, pupdate_bytes;
 } acg_kernel_times;
 
 /* 0 if the current CUDA device is usable (sm_100), else an error code. */
@@ -259,9 +267,12 @@ int acg_create_group(int64_t ngraphs, const int64_t* offsets, int64_t n, const i
                      const int64_t* ldli_colptr, const int64_t* ldli_rowval, const double* ldli_fval,
                      const double* ldli_d, int64_t ldli_nnz, int index_base, const acg_options* opts,
                      acg_solver** out);
-/* One right-hand side per graph (b: n values of the union, host); info[ngraphs]. */
+/* One right-hand side per graph (b: n values of the union, host); info[ngraphs].
+ * precision 0: FP64 PCG per graph; 1: each graph's FP32 PCG inside its own FP64
+ * refinement on the true residual (as acg_solve's precision 1), all graphs in
+ * the same launches. */
 int acg_solve_group(acg_solver* h, const double* b, double* x, double tol, int64_t maxits, double maxtime,
-                    int stag_test, acg_solve_info* info);
+                    int stag_test, int precision, acg_solve_info* info);
 
 /* y = LDLsolver(ldli, r) (src/approxChol.jl:1347-1366) on the device; host arrays. */
 int acg_ldlsolve(acg_solver* h, const double* r, double* y, int precision);

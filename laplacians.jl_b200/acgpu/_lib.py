@@ -33,7 +33,8 @@ class AcgOptions(ctypes.Structure):
                 ("batch_bwd_heavy", ctypes.c_int), ("batch_fwd_heavy", ctypes.c_int),
                 ("batch_blocks_per_sm", ctypes.c_int), ("sweep_heavy", ctypes.c_int),
                 ("dense_tail", ctypes.c_int), ("sweep_stride", ctypes.c_int),
-                ("spin_limit", ctypes.c_int), ("test_unproduced_task", ctypes.c_int)]
+                ("level_order", ctypes.c_int), ("spin_limit", ctypes.c_int),
+                ("test_unproduced_task", ctypes.c_int)]
 
 
 class AcgStats(ctypes.Structure):
@@ -58,7 +59,10 @@ class AcgKernelTimes(ctypes.Structure):
                 ("forward_bytes", ctypes.c_double), ("backward_bytes", ctypes.c_double),
                 ("forward_sweep_ms", ctypes.c_double), ("backward_sweep_ms", ctypes.c_double),
                 ("dense_ms", ctypes.c_double), ("forward_sweep_bytes", ctypes.c_double),
-                ("backward_sweep_bytes", ctypes.c_double), ("dense_bytes", ctypes.c_double)]
+                ("backward_sweep_bytes", ctypes.c_double), ("dense_bytes", ctypes.c_double),
+                ("pq_ms", ctypes.c_double), ("update_ms", ctypes.c_double), ("yzr_ms", ctypes.c_double),
+                ("pupdate_ms", ctypes.c_double), ("pq_bytes", ctypes.c_double), ("update_bytes", ctypes.c_double),
+                ("yzr_bytes", ctypes.c_double), ("pupdate_bytes", ctypes.c_double)]
 
 
 # (name, restype, argtypes) for every entry point of include/acgpu.h
@@ -85,7 +89,7 @@ SIGNATURES = [
                                         i64p, i64p, f64p, f64p, ctypes.c_int64, ctypes.c_int,
                                         ctypes.POINTER(AcgOptions), ctypes.POINTER(ctypes.c_void_p)]),
     ("acg_solve_group", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_double, ctypes.c_int64, ctypes.c_double,
-                                       ctypes.c_int, ctypes.POINTER(AcgSolveInfo)]),
+                                       ctypes.c_int, ctypes.c_int, ctypes.POINTER(AcgSolveInfo)]),
     ("acg_destroy", None, [ctypes.c_void_p]),
     ("acg_solver_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AcgStats)]),
     ("acg_solve", ctypes.c_int, [ctypes.c_void_p, f64p, f64p, ctypes.c_int64, ctypes.c_int64, ctypes.c_double,

@@ -376,14 +376,14 @@ class GroupSolver:
     once).  Every graph must be connected and have at least 2 vertices."""
 
     def __init__(self, graphs, factors=None, *, tol=1e-6, maxits=1000, maxtime=math.inf, stag_test=5,
-                 options: dict | None = None):
+                 precision="fp64", options: dict | None = None):
         graphs = [_csc(a) for a in graphs]
         if factors is None:
             factors = [approx_chol(a) for a in graphs]
         sizes = [a.shape[0] for a in graphs]
         self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
         self.n = int(self.offsets[-1])
-        self.defaults = dict(tol=tol, maxits=maxits, maxtime=maxtime)
+        self.defaults = dict(tol=tol, maxits=maxits, maxtime=maxtime, precision=precision)
         self.stag_test = stag_test
         a = _csc(sp.block_diag(graphs, format="csc"))
         # union factor: columns of every graph in turn, vertex ids shifted (1-based)
@@ -412,19 +412,21 @@ class GroupSolver:
         self.ngraphs = len(graphs)
         self.last_info = []
 
-    def __call__(self, bs, tol=None, maxits=None, maxtime=None):
+    def __call__(self, bs, tol=None, maxits=None, maxtime=None, precision=None):
         """bs: one right-hand side per graph (list), or the union vector; returns
-        the same shape."""
+        the same shape.  precision "fp64" (default) or "mixed" (each graph's FP32
+        PCG inside its own FP64 refinement)."""
         d = self.defaults
         tol = d["tol"] if tol is None else tol
         maxits = d["maxits"] if maxits is None else maxits
         maxtime = d["maxtime"] if maxtime is None else maxtime
+        precision = d["precision"] if precision is None else precision
         as_list = isinstance(bs, (list, tuple))
         b = np.ascontiguousarray(np.concatenate(bs) if as_list else bs, dtype=np.float64)
         x = np.empty_like(b)
         infos = (AcgSolveInfo * self.ngraphs)()
         check(lib().acg_solve_group(self._h, b, x, float(tol), _maxits_int(maxits), float(maxtime), int(self.stag_test),
-                                    infos))
+                                    _PRECISIONS[precision], infos))
         self.last_info = list(infos)
         if as_list:
             return [x[self.offsets[g]:self.offsets[g + 1]] for g in range(self.ngraphs)]
@@ -473,36 +475,57 @@ class _DenseGroundedSolver:
         return x - x.mean()
 
 
-class _BlockSolver:
-    """`blockSolver` (src/solverInterface.jl:152-188): one solver per component."""
+class _GroupPart:
+    """Every component with at least 50 vertices of a disconnected graph,
+    solved together: one GroupSolver over their union, so each solve is one
+    launch for all of them (the reference solves them one after another in
+    blockSolver, src/solverInterface.jl:152-188)."""
 
-    def __init__(self, comps, solvers, defaults):
+    def __init__(self, graphs, factors, params, precision, options):
+        self.group = GroupSolver(graphs, factors, stag_test=params.stag_test, options=options)
+        self.precision = precision
+
+    def __call__(self, bs, tol, maxits, maxtime, precision=None):
+        xs = self.group(bs, tol=tol, maxits=maxits, maxtime=maxtime,
+                        precision=self.precision if precision is None else precision)
+        its = max(int(i.iterations) for i in self.group.last_info)
+        return xs, its
+
+
+class _BlockSolver:
+    """`blockSolver` (src/solverInterface.jl:152-188): the components of a
+    disconnected graph solved apart and assembled.  Components of fewer than 50
+    vertices (and singletons) are solved on the host as the reference does;
+    the large ones share one group launch per right-hand side."""
+
+    def __init__(self, comps, solvers, defaults, group=None, group_comps=()):
         self.comps = comps
         self.solvers = solvers
         self.defaults = defaults
+        self.group = group
+        self.group_comps = list(group_comps)
 
     def __call__(self, b, tol=None, maxits=None, maxtime=None, verbose=None, pcgIts=None, precision=None):
         d = self.defaults
-        kw = dict(tol=d["tol"] if tol is None else tol, maxits=d["maxits"] if maxits is None else maxits,
-                  maxtime=d["maxtime"] if maxtime is None else maxtime,
-                  verbose=d["verbose"] if verbose is None else verbose)
-        if precision is not None:
-            kw["precision"] = precision
+        tol = d["tol"] if tol is None else tol
+        maxits = d["maxits"] if maxits is None else maxits
+        maxtime = d["maxtime"] if maxtime is None else maxtime
         pcgIts = d["pcgIts"] if pcgIts is None else pcgIts
-        if pcgIts is not None and len(pcgIts) > 0:
-            pcgIts[0] = 0
-            tmp = [0]
-        else:
-            tmp = []
         b = np.asarray(b, dtype=np.float64)
         x = np.zeros(b.shape)
+        its = 0
         for ind, s in zip(self.comps, self.solvers):
-            if isinstance(s, DeviceLapSolver):
-                x[ind] = s(b[ind], pcgIts=tmp, **kw)
-            else:
-                x[ind] = s(b[ind])
-            if pcgIts is not None and len(pcgIts) > 0:
-                pcgIts[0] = max(pcgIts[0], tmp[0] if tmp else 0)
+            x[ind] = s(b[ind])
+        if self.group is not None:
+            cols = b.reshape(b.shape[0], -1)
+            xcols = x.reshape(b.shape[0], -1)
+            for c in range(cols.shape[1]):
+                xs, it = self.group([cols[ind, c] for ind in self.group_comps], tol, maxits, maxtime, precision)
+                for ind, xi in zip(self.group_comps, xs):
+                    xcols[ind, c] = xi
+                its = max(its, it)
+        if pcgIts is not None and len(pcgIts) > 0:
+            pcgIts[0] = its
         return x
 
 
@@ -544,24 +567,31 @@ def approxchol_lap(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False,
     if co.max() == 1:
         return approxchol_lap1(a, **kw)
     comps = vec_to_comps(co)
-    solvers = []
+    host_comps, solvers, big = [], [], []
     sizes = np.array([len(c) for c in comps])
     null_idx = np.where(sizes == 1)[0]
     if null_idx.size:
-        flat = np.concatenate([comps[i] for i in null_idx])
-        comps = [flat] + [c for i, c in enumerate(comps) if sizes[i] != 1]
+        host_comps.append(np.concatenate([comps[i] for i in null_idx]))
         solvers.append(null_solver)
-        rest = comps[1:]
-    else:
-        rest = comps
-    for ind in rest:
-        asub = a[ind][:, ind]
+    for i, ind in enumerate(comps):
+        if sizes[i] == 1:
+            continue
         if len(ind) < 50:
-            solvers.append(_DenseGroundedSolver(asub))
+            host_comps.append(ind)
+            solvers.append(_DenseGroundedSolver(a[ind][:, ind]))
         else:
-            solvers.append(approxchol_lap1(asub, **kw))
-    return _BlockSolver(comps, solvers, dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose,
-                                             pcgIts=pcgIts))
+            big.append(ind)
+    group = None
+    params = params or ApproxCholParams()
+    if big:
+        graphs = [_csc(a[ind][:, ind]) for ind in big]
+        t1 = time.time()
+        factors = [approx_chol(g, params) for g in graphs]
+        if verbose:
+            print(f"Factorization time for {len(big)} components: ", time.time() - t1)
+        group = _GroupPart(graphs, factors, params, precision, options)
+    return _BlockSolver(host_comps, solvers, dict(tol=tol, maxits=maxits, maxtime=maxtime, verbose=verbose,
+                                                  pcgIts=pcgIts), group=group, group_comps=big)
 
 
 def approxchol_lap2(a, *, tol=1e-6, maxits=1000, maxtime=math.inf, verbose=False, pcgIts=None,

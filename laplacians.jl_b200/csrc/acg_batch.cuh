@@ -783,6 +783,33 @@ __global__ void __launch_bounds__(kBVecThreads) kb_pupdate_z(int n, int kp, cons
   }
 }
 
+// Timing only (acg_time_kernels_batch): every column running, mid-solve, with
+// scalars that no stop test fires on (itcnt 1, tol 0, no maxits, no maxtime),
+// so each timed vector kernel does its full pass.
+__global__ void kb_timing_state(PcgState* st, BatchShared* bs, int kp) {
+  const int c = threadIdx.x;
+  if (c < kp) {
+    PcgState* s = &st[c];
+    s->tol = 0.0;
+    s->maxtime_s = 1e300;
+    s->maxits = 1ll << 62;
+    s->stag_test = 0;
+    s->nb = 1.0;
+    s->rho = s->best_rho = 1.0;
+    s->bestnr = 1.0;
+    s->itcnt = 1;
+    s->stag_count = 0;
+    s->done = 0;
+    s->xcur = 0;
+    s->xnext = 1;
+    s->xbest = 0;
+  }
+  if (c == 0) {
+    bs->all_done = 0;
+    bs->l1_due = 0;
+  }
+}
+
 // ---- set-up and wrap-up ------------------------------------------------------
 
 // bint[v*kp + c] = B[c*ldb + perm[v]] for c < k, 0 for padding; per-column mean.

@@ -216,10 +216,12 @@ __global__ void __launch_bounds__(kVecThreads) kg_gather_in(const int* __restric
 }
 
 // bm = b - mean; r = bm; x0 = 0; s, y pending; per-graph |b|, state reset.
+// outer = 1 starts a mixed-precision solve: the FP64 refinement state is reset
+// too, and a graph that stops here is done for the refinement loop as well.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) kg_center(double* __restrict__ bm, T* __restrict__ r, T* __restrict__ x0,
                                                          T* __restrict__ s_out, T* __restrict__ y_out, GroupArgs g,
-                                                         LoopCtl ctl, int vs) {
+                                                         LoopCtl ctl, int vs, int outer) {
   const SegChunk c = g.chunks[blockIdx.x];
   const double mu = g.st[c.seg].mean;
   const T pend = pending_value<T>();
@@ -251,12 +253,19 @@ __global__ void __launch_bounds__(kVecThreads) kg_center(double* __restrict__ bm
     s->xcur = 0;
     s->xbest = 0;
     s->xnext = 1;
+    s->scale = s->nb;
+    s->total_its = 0;
+    s->outer_its = 0;
+    s->outer_done = 0;
+    s->t_start = globaltimer_ns();
     if (s->nb == 0.0) {
       s->nr_true = 0.0;
       s->nr = 0.0;
+      s->outer_done = outer;
       mark_stop(s, kConverged);
       seg_stopped(g, ctl);
     } else if (!isfinite(s->nb)) {  // a NaN or Inf entry in this graph's right-hand side
+      s->outer_done = outer;
       mark_stop(s, kBadInput);
       seg_stopped(g, ctl);
     }
@@ -271,24 +280,158 @@ __global__ void __launch_bounds__(kVecThreads) kg_take_best(int n, const T* __re
   for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) xf[i] = (double)xb[i];
 }
 
-// per graph: |bm - L xf| / |bm| (FP64)
+// per graph: t = bm - L xf (FP64), |t| / |bm|.  In a refinement loop (rout
+// set) t is stored as the next inner right-hand side, |t| becomes the graph's
+// scale, and graphs whose refinement has ended are skipped (every chunk of
+// such a graph skips, so its reduction tickets stay balanced).
 __global__ void __launch_bounds__(kVecThreads) kg_true_residual(const int* __restrict__ ptr, const int* __restrict__ idx,
                                                                 const double* __restrict__ val,
                                                                 const double* __restrict__ xf,
-                                                                const double* __restrict__ bm, GroupArgs g) {
+                                                                const double* __restrict__ bm,
+                                                                double* __restrict__ rout, GroupArgs g) {
   const SegChunk c = g.chunks[blockIdx.x];
+  if (rout && g.st[c.seg].outer_done) return;
   double acc[1] = {0.0};
   for (int row = c.start + threadIdx.x; row < c.end; row += blockDim.x) {
     double s = 0.0;
     for (int k = __ldg(&ptr[row]); k < __ldg(&ptr[row + 1]); ++k) s += __ldg(&val[k]) * xf[__ldg(&idx[k])];
     const double t = bm[row] - s;
+    if (rout) rout[row] = t;
     acc[0] += t * t;
   }
   double tot[1];
   if (seg_reduce<1>(acc, c, g, 6, tot) && threadIdx.x == 0) {
     PcgState* s = &g.st[c.seg];
-    s->nr_true = s->nb64 > 0.0 ? sqrt(tot[0]) / s->nb64 : 0.0;
+    const double nt = sqrt(tot[0]);
+    s->nr_true = s->nb64 > 0.0 ? nt / s->nb64 : 0.0;
+    if (rout) s->scale = nt;
   }
+}
+
+// ---- mixed precision: FP32 PCG inside FP64 refinement, per graph -----------
+// The same refinement as one graph's (k_outer_prep .. k_outer_decide): each
+// graph keeps its FP64 x and residual, runs FP32 inner PCG on r64 / |r64| to
+// an adaptive tolerance, adds |r64| times the inner solution and recomputes
+// the true residual; graphs whose refinement has ended sit out the rest.
+
+// Start of a refinement step (one block): the graphs already finished count
+// as stopped for the inner loop, which is re-armed.
+__global__ void kg_outer_begin(GroupArgs g, LoopCtl inner_ctl) {
+  __shared__ int fin;
+  if (threadIdx.x == 0) fin = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int q = threadIdx.x; q < g.nseg; q += blockDim.x) mine += g.st[q].outer_done ? 1 : 0;
+  atomicAdd(&fin, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    g.gsh->stopped = fin;
+    g.gst->done = fin == g.nseg ? 1 : 0;
+    if (inner_ctl.use_handle) cudaGraphSetConditional(inner_ctl.handle, fin == g.nseg ? 0u : 1u);
+  }
+}
+
+// r_in = r64 / scale (FP32), x buffer 0 = 0, s and y pending; the graph's inner
+// PCG state reset (finished graphs are marked done for the inner loop).
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_outer_prep(const double* __restrict__ r64, T* __restrict__ rin,
+                                                             T* __restrict__ x0, T* __restrict__ s_out,
+                                                             T* __restrict__ y_out, GroupArgs g, LoopCtl inner_ctl,
+                                                             int vs) {
+  const SegChunk c = g.chunks[blockIdx.x];
+  PcgState* s = &g.st[c.seg];
+  const T pend = pending_value<T>();
+  if (s->outer_done) {
+    for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
+      s_out[(size_t)i * vs] = pend;
+      y_out[(size_t)i * vs] = pend;
+    }
+    if (threadIdx.x == 0) s->done = 1;  // every chunk writes the same value
+    return;
+  }
+  const double inv = 1.0 / s->scale;
+  double acc[2] = {0.0, 0.0};
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) {
+    const T v = (T)(r64[i] * inv);
+    rin[i] = v;
+    x0[i] = T(0);
+    s_out[(size_t)i * vs] = pend;
+    y_out[(size_t)i * vs] = pend;
+    acc[0] += (double)v * (double)v;
+    acc[1] += fabs((double)v);
+  }
+  double tot[2];
+  if (seg_reduce<2>(acc, c, g, 7, tot) && threadIdx.x == 0) {
+    s->nb = sqrt(tot[0]);
+    s->sum_abs_r = tot[1];
+    s->sum_abs_x = 0.0;
+    s->bestnr = 1.0;
+    s->nr = 1.0;
+    s->itcnt = 0;
+    s->stag_count = 0;
+    s->status = kMaxits;
+    s->done = 0;
+    s->xcur = 0;
+    s->xbest = 0;
+    s->xnext = 1;
+    s->tol = s->inner_tol;
+    if (s->nb == 0.0) {
+      mark_stop(s, kConverged);
+      seg_stopped(g, inner_ctl);
+    }
+  }
+}
+
+// x64 += scale * x_in[best] for the graphs still refining.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) kg_outer_correct(int n, const T* __restrict__ x3,
+                                                                double* __restrict__ x64, GroupArgs g) {
+  const SegChunk c = g.chunks[blockIdx.x];
+  const PcgState* s = &g.st[c.seg];
+  if (s->outer_done) return;
+  const T* xb = x3 + (size_t)s->xbest * n;
+  const double sc = s->scale;
+  for (int i = c.start + threadIdx.x; i < c.end; i += blockDim.x) x64[i] += sc * (double)xb[i];
+}
+
+// After the true residuals (one block): per graph, account its iterations and
+// decide, as k_outer_decide does for one graph, whether to refine again; the
+// refinement loop ends when no graph is left.
+__global__ void kg_outer_decide(GroupArgs g, LoopCtl outer_ctl) {
+  __shared__ int left;
+  if (threadIdx.x == 0) left = 0;
+  __syncthreads();
+  const bool timeout = g.gst->sweep_error != 0;
+  int mine = 0;
+  for (int q = threadIdx.x; q < g.nseg; q += blockDim.x) {
+    PcgState* st = &g.st[q];
+    if (st->outer_done) continue;
+    st->total_its += st->itcnt;
+    st->outer_its += 1;
+    const int inner_status = st->status;
+    const bool progressed = st->itcnt > 0 && st->bestnr < 1.0;
+    int stop = -1;
+    if (timeout || inner_status == kSweepTimeout) stop = kSweepTimeout;
+    else if (st->nr_true <= st->tol_user) stop = kConverged;
+    else if (st->total_its >= st->maxits_user) stop = kMaxits;
+    else if (st->outer_its >= st->max_outer) stop = kStagX;
+    else if (!progressed) stop = inner_status == kMaxits ? kStagRho : inner_status;
+    else if ((double)(globaltimer_ns() - st->t_start) * 1e-9 > st->maxtime_s) stop = kMaxtime;
+    if (stop >= 0) {
+      st->outer_done = 1;
+      st->status = stop;
+      continue;
+    }
+    double it = 0.5 * st->tol_user / st->nr_true;
+    if (it < st->min_inner_tol) it = st->min_inner_tol;
+    if (it > 0.25) it = 0.25;
+    st->inner_tol = it;
+    st->maxits = st->maxits_user - st->total_its;
+    ++mine;
+  }
+  atomicAdd(&left, mine);
+  __syncthreads();
+  if (threadIdx.x == 0 && left == 0 && outer_ctl.use_handle) cudaGraphSetConditional(outer_ctl.handle, 0u);
 }
 
 }  // namespace acg

@@ -136,7 +136,7 @@ struct SolverImpl {
   PcgState* gflags = nullptr;   // group flags (device)
   GroupShared* gsh = nullptr;
   PcgState* h_gstates = nullptr;
-  cudaGraphExec_t gexec = nullptr;
+  cudaGraphExec_t gexec = nullptr, gexec_mixed = nullptr;
 
   // batched solves: kp right-hand sides per launch (vertex-major n x kp blocks)
   int batch_kp = 0;  // capacity of the batch buffers
@@ -199,6 +199,7 @@ struct SolverImpl {
     if (bst) cudaFree(bst);
     if (bsh) cudaFree(bsh);
     if (gexec) cudaGraphExecDestroy(gexec);
+    if (gexec_mixed) cudaGraphExecDestroy(gexec_mixed);
     if (gstates) cudaFree(gstates);
     if (gflags) cudaFree(gflags);
     if (gsh) cudaFree(gsh);
@@ -722,9 +723,11 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   for (int64_t e = 0; e < F; ++e) indeg[rowval[e] - base]++;
   std::vector<int> perm(n), e2i(n);
   for (int v = 0; v < n; ++v) perm[v] = v;
+  const bool by_id = opts && opts->level_order == 1;
   std::sort(perm.begin(), perm.end(), [&](int x, int y) {
     if (seg_of[x] != seg_of[y]) return seg_of[x] < seg_of[y];
     if (lev[x] != lev[y]) return lev[x] < lev[y];
+    if (by_id) return x < y;
     if (indeg[x] != indeg[y]) return indeg[x] > indeg[y];
     return step[x] < step[y];
   });
@@ -1746,7 +1749,7 @@ cudaGraphExec_t build_group_graph(SolverImpl& S) {
   // to start are left incomplete by those blocks: clear them every solve
   ACG_CUDA(cudaMemsetAsync(S.seg_cnt.p, 0, sizeof(unsigned int) * 8 * S.nseg, s));
   kg_gather_in<<<nb, kVecThreads, 0, s>>>(S.perm.p, S.b_ext.p, S.bm.p, g);
-  kg_center<double><<<nb, kVecThreads, 0, s>>>(S.bm.p, S.r64.p, S.x3_64.p, S.s64.p, S.y64.p, g, ctl, S.vs64);
+  kg_center<double><<<nb, kVecThreads, 0, s>>>(S.bm.p, S.r64.p, S.x3_64.p, S.s64.p, S.y64.p, g, ctl, S.vs64, 0);
   enqueue_sweeps<double>(s, S, S.r64.p, S.s64.p, S.y64.p, S.gflags);
   kg_ysum<double><<<nb, kVecThreads, 0, s>>>(S.y64.p, g, ctl, S.vs64);
   kg_zdot<double><<<nb, kVecThreads, 0, s>>>(S.y64.p, S.r64.p, S.p64.p, g, kEps64, 1, ctl, S.vs64);
@@ -1766,7 +1769,72 @@ cudaGraphExec_t build_group_graph(SolverImpl& S) {
   end_into(s);
   begin_into(s, top, {wnode});
   kg_take_best<double><<<nb, kVecThreads, 0, s>>>(n, S.x3_64.p, S.xf.p, g);
-  kg_true_residual<<<nb, kVecThreads, 0, s>>>(S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.xf.p, S.bm.p, g);
+  kg_true_residual<<<nb, kVecThreads, 0, s>>>(S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.xf.p, S.bm.p, nullptr, g);
+  k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
+  end_into(s);
+  cudaGraphExec_t exec;
+  ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
+  cudaGraphDestroy(top);
+  return exec;
+}
+
+// Every graph's FP32 PCG inside its own FP64 refinement (the group form of
+// build_mixed_graph): an outer WHILE over refinement steps around an inner
+// WHILE over PCG iterations; graphs that finish refining sit out the rest.
+cudaGraphExec_t build_group_mixed_graph(SolverImpl& S) {
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  const int nb = S.nchunks;
+  const double eps32 = 1.1920928955078125e-07;
+  const GroupArgs g = group_args(S);
+  const TypedArrays<float> A = arrays_of<float>(S);
+  cudaGraph_t top;
+  ACG_CUDA(cudaGraphCreate(&top, 0));
+  cudaGraphConditionalHandle ho;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&ho, top, 1u, cudaGraphCondAssignDefault));
+  LoopCtl octl{ho, 1};
+  begin_into(s, top, {});
+  ACG_CUDA(cudaMemsetAsync(S.seg_cnt.p, 0, sizeof(unsigned int) * 8 * S.nseg, s));
+  kg_gather_in<<<nb, kVecThreads, 0, s>>>(S.perm.p, S.b_ext.p, S.bm.p, g);
+  // r64 = bm, x64 (xf) = 0, per-graph |b| and refinement state
+  kg_center<double><<<nb, kVecThreads, 0, s>>>(S.bm.p, S.r64.p, S.xf.p, S.s64.p, S.y64.p, g, octl, S.vs64, 1);
+  std::vector<cudaGraphNode_t> leaves = capture_leaves(s);
+  end_into(s);
+
+  cudaGraph_t obody;
+  cudaGraphNode_t onode = add_while(top, leaves, ho, &obody);
+  cudaGraphConditionalHandle hi;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&hi, obody, 1u, cudaGraphCondAssignDefault));
+  LoopCtl ictl{hi, 1};
+  begin_into(s, obody, {});
+  kg_outer_begin<<<1, 256, 0, s>>>(g, ictl);
+  kg_outer_prep<float><<<nb, kVecThreads, 0, s>>>(S.r64.p, S.r32.p, S.x3_32.p, S.s32.p, S.y32.p, g, ictl, S.vs32);
+  enqueue_sweeps<float>(s, S, S.r32.p, S.s32.p, S.y32.p, S.gflags);
+  kg_ysum<float><<<nb, kVecThreads, 0, s>>>(S.y32.p, g, ictl, S.vs32);
+  kg_zdot<float><<<nb, kVecThreads, 0, s>>>(S.y32.p, S.r32.p, S.p32.p, g, eps32, 2, ictl, S.vs32);
+  std::vector<cudaGraphNode_t> ol = capture_leaves(s);
+  end_into(s);
+
+  cudaGraph_t ibody;
+  cudaGraphNode_t inode = add_while(obody, ol, hi, &ibody);
+  begin_into(s, ibody, {});
+  kg_spmv<float, 8><<<kVecBlocks, kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, S.p32.p, S.q32.p, S.gflags);
+  kg_pq<float><<<nb, kVecThreads, 0, s>>>(S.p32.p, S.q32.p, g, eps32, ictl);
+  kg_update<float><<<nb, kVecThreads, 0, s>>>(n, S.x3_32.p, S.p32.p, S.q32.p, S.r32.p, S.s32.p, S.y32.p, g, ictl,
+                                              S.vs32);
+  enqueue_sweeps<float>(s, S, S.r32.p, S.s32.p, S.y32.p, S.gflags);
+  kg_ysum<float><<<nb, kVecThreads, 0, s>>>(S.y32.p, g, ictl, S.vs32);
+  kg_zdot<float><<<nb, kVecThreads, 0, s>>>(S.y32.p, S.r32.p, S.p32.p, g, eps32, 0, ictl, S.vs32);
+  kg_pupdate<float><<<nb, kVecThreads, 0, s>>>(S.y32.p, S.p32.p, g, S.vs32);
+  end_into(s);
+
+  begin_into(s, obody, {inode});
+  kg_outer_correct<float><<<nb, kVecThreads, 0, s>>>(n, S.x3_32.p, S.xf.p, g);
+  kg_true_residual<<<nb, kVecThreads, 0, s>>>(S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.xf.p, S.bm.p, S.r64.p, g);
+  kg_outer_decide<<<1, 256, 0, s>>>(g, octl);
+  end_into(s);
+
+  begin_into(s, top, {onode});
   k_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, S.perm.p, S.xf.p, S.x_ext.p);
   end_into(s);
   cudaGraphExec_t exec;
@@ -1776,11 +1844,12 @@ cudaGraphExec_t build_group_graph(SolverImpl& S) {
 }
 
 int solve_group(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, cudaMemcpyKind kout, double tol,
-                int64_t maxits, double maxtime, int stag_test, acg_solve_info* info) {
+                int64_t maxits, double maxtime, int stag_test, int precision, acg_solve_info* info) {
   cudaStream_t s = S.stream;
-  if (!S.gexec) {
+  cudaGraphExec_t& exec = precision == 0 ? S.gexec : S.gexec_mixed;
+  if (!exec) {
     std::lock_guard<std::recursive_mutex> glk(g_device_mu);
-    S.gexec = build_group_graph(S);
+    exec = precision == 0 ? build_group_graph(S) : build_group_mixed_graph(S);
   }
   PcgState* h = S.h_gstates;
   std::memset(h, 0, sizeof(PcgState) * S.nseg);
@@ -1790,6 +1859,11 @@ int solve_group(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, c
     h[g].maxits = maxits;
     h[g].stag_test = stag_test;
     h[g].nvert = S.seg_off[g + 1] - S.seg_off[g];
+    h[g].tol_user = tol;
+    h[g].maxits_user = maxits;
+    h[g].min_inner_tol = 1e-5;
+    h[g].max_outer = 40;
+    h[g].inner_tol = std::min(0.25, std::max(h[g].min_inner_tol, 0.5 * tol));
   }
   ACG_CUDA(cudaMemcpyAsync(S.gstates, h, sizeof(PcgState) * S.nseg, cudaMemcpyHostToDevice, s));
   ACG_CUDA(cudaMemcpyAsync(S.b_ext.p, b, sizeof(double) * S.n, kin, s));
@@ -1797,7 +1871,7 @@ int solve_group(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, c
   ACG_CUDA(cudaEventCreate(&e0));
   ACG_CUDA(cudaEventCreate(&e1));
   ACG_CUDA(cudaEventRecord(e0, s));
-  ACG_CUDA(cudaGraphLaunch(S.gexec, s));
+  ACG_CUDA(cudaGraphLaunch(exec, s));
   ACG_CUDA(cudaEventRecord(e1, s));
   ACG_CUDA(cudaMemcpyAsync(x, S.x_ext.p, sizeof(double) * S.n, kout, s));
   ACG_CUDA(cudaMemcpyAsync(h, S.gstates, sizeof(PcgState) * S.nseg, cudaMemcpyDeviceToHost, s));
@@ -1809,10 +1883,10 @@ int solve_group(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, c
   int worst = 0;
   for (int g = 0; g < S.nseg; ++g) {
     if (info) {
-      info[g].iterations = h[g].itcnt;
-      info[g].refinements = 0;
+      info[g].iterations = precision == 0 ? h[g].itcnt : h[g].total_its;
+      info[g].refinements = precision == 0 ? 0 : h[g].outer_its;
       info[g].relres = h[g].nr;
-      info[g].best_relres = h[g].bestnr;
+      info[g].best_relres = precision == 0 ? h[g].bestnr : h[g].nr_true;
       info[g].true_relres = h[g].nr_true;
       info[g].solve_ms = ms;
       info[g].status = h[g].status;
@@ -1874,7 +1948,7 @@ int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, 
 
 // Device time per call of the batched kernels for kp columns (see time_kernels_t).
 template <typename T, int CPL>
-void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T* y, T* p, T* q) {
+void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T* y, T* p, T* q, T* x3) {
   constexpr int kp = CPL * kBatchLanes;
   cudaStream_t s = S.stream;
   ACG_CUDA(cudaMemsetAsync(S.bsh, 0, sizeof(BatchShared), s));
@@ -1952,6 +2026,38 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
     enqueue_dense<T, CPL>(s, S, true, sv, (T*)nullptr, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
     enqueue_dense<T, CPL>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
   }) : 0.0;
+  // the loop body's vector kernels, each from the same running state (reset
+  // by kb_timing_state before every call; the reset is timed apart)
+  {
+    ACG_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * N, s));
+    ACG_CUDA(cudaMemsetAsync(q, 0, sizeof(T) * N, s));
+    ACG_CUDA(cudaMemsetAsync(x3, 0, sizeof(T) * 3 * N, s));
+    const double eps = sizeof(T) == 4 ? 1.1920928955078125e-07 : kEps64;
+    const LoopCtl none{0, 0};
+    auto reset = [&]() { kb_timing_state<<<1, 64, 0, s>>>(S.bst, S.bsh, kp); };
+    const double t_reset = time_graph(reset);
+    out->pq_ms = time_graph([&]() {
+      reset();
+      kb_pq<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(S.n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, none);
+    }) - t_reset;
+    out->update_ms = time_graph([&]() {
+      reset();
+      kb_update<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(S.n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, none);
+    }) - t_reset;
+    out->yzr_ms = time_graph([&]() {
+      reset();
+      kb_yzr<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(S.n, kp, y, r, S.bst, S.bsh, S.bpartials.p, eps, none);
+    }) - t_reset;
+    out->pupdate_ms = time_graph([&]() {
+      reset();
+      kb_pupdate_z<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(S.n, kp, y, p, S.bst, S.bsh, S.bpartials.p, eps, none);
+    }) - t_reset;
+    const double vec = (double)S.n * kp * sizeof(T);
+    out->pq_bytes = 2.0 * vec;       // p, q read
+    out->update_bytes = 6.0 * vec;   // x, p, q, r read; x', r written
+    out->yzr_bytes = 2.0 * vec;      // y, r read
+    out->pupdate_bytes = 3.0 * vec;  // y, p read; p written
+  }
   out->iteration_ms = 0.0;
   const int dense_launches = S.dt_K ? 2 : 0;
   // mat-vec, pq, update, two sweeps, kb_yzr, kb_pupdate_z and the dense products
@@ -1975,8 +2081,10 @@ void time_batch(SolverImpl& S, int precision, int kp, int reps, acg_kernel_times
   ensure_batch(S, std::max(kp, S.batch_kp));
   with_cpl(kp, [&](auto cpl) {
     constexpr int C = decltype(cpl)::value;
-    if (precision == 0) time_batch_t<double, C>(S, reps, out, S.br64.p, S.bs64.p, S.by64.p, S.bp64.p, S.bq64.p);
-    else time_batch_t<float, C>(S, reps, out, S.br32.p, S.bs32.p, S.by32.p, S.bp32.p, S.bq32.p);
+    if (precision == 0)
+      time_batch_t<double, C>(S, reps, out, S.br64.p, S.bs64.p, S.by64.p, S.bp64.p, S.bq64.p, S.bx3_64.p);
+    else
+      time_batch_t<float, C>(S, reps, out, S.br32.p, S.bs32.p, S.by32.p, S.bp32.p, S.bq32.p, S.bx3_32.p);
   });
 }
 
@@ -2367,15 +2475,15 @@ int acg_create_group(int64_t ngraphs, const int64_t* offsets, int64_t n, const i
 }
 
 int acg_solve_group(acg_solver* h, const double* b, double* x, double tol, int64_t maxits, double maxtime,
-                    int stag_test, acg_solve_info* info) {
-  if (!h || !b || !x || h->impl.nseg < 2) {
-    acg::set_last_error("acg_solve_group: bad arguments (needs a solver made by acg_create_group)");
+                    int stag_test, int precision, acg_solve_info* info) {
+  if (!h || !b || !x || h->impl.nseg < 2 || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_solve_group: bad arguments (needs a solver made by acg_create_group, precision 0 or 1)");
     return ACG_ERR_INVALID;
   }
   return guarded("acg_solve_group", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
     return acg::solve_group(h->impl, b, x, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol, maxits, maxtime,
-                            stag_test, info);
+                            stag_test, precision, info);
   });
 }
 
@@ -2511,6 +2619,7 @@ int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg
     acg::set_last_error("acg_time_kernels_batch: bad arguments");
     return ACG_ERR_INVALID;
   }
+  *out = acg_kernel_times{};
   return guarded("acg_time_kernels_batch", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
     std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
@@ -2524,6 +2633,7 @@ int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* o
     acg::set_last_error("acg_time_kernels: bad arguments");
     return ACG_ERR_INVALID;
   }
+  *out = acg_kernel_times{};
   return guarded("acg_time_kernels", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
     std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);

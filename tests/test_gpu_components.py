@@ -1,7 +1,8 @@
 """approxchol_lap on a disconnected graph follows lapWrapComponents
 (src/solverInterface.jl:212-275): singletons get zero, components with fewer
-than 50 vertices a direct solve, larger ones the GPU solver; x agrees with the
-exact solution per component, and pcgIts is the largest count over components."""
+than 50 vertices a direct solve, larger ones the GPU solver, all of the large
+ones together in one group launch; x agrees with the exact solution per
+component, and pcgIts is the largest count over components."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -47,6 +48,38 @@ def test_components_match_exact(gpu_ok):
     assert its[0] >= 1
     la = acgpu.lap(a)
     assert np.linalg.norm(la @ x - b) / np.linalg.norm(b) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_large_components_share_one_group_launch(gpu_ok, precision):
+    """Singletons, small components and four large ones: the large ones are one
+    GroupSolver (one launch per right-hand side), each agreeing with its exact
+    solve; several right-hand sides at once work column by column."""
+    parts = [G.grid2(15, weights="loguniform", seed=1), G.star_graph(9),
+             G.path_plus_matchings(400, seed=2), G.grid3(8, weights="loguniform", seed=3),
+             G.cycle_graph(30, np.linspace(0.5, 2, 30)), G.largest_component(G.random_geometric(900, seed=4))]
+    a = _union(parts, 3)
+    n = a.shape[0]
+    co = acgpu.components(a)
+    B = np.random.default_rng(1).standard_normal((n, 3))
+    for c in np.unique(co):
+        m = co == c
+        B[m] -= B[m].mean(axis=0)
+    acgpu.seed(8)
+    its = [0]
+    f = acgpu.approxchol_lap(a, tol=1e-10, pcgIts=its, precision=precision)
+    assert f.group is not None and f.group.group.ngraphs == 4
+    X = f(B)
+    assert its[0] >= 1
+    for col in range(3):
+        start = 0
+        for p in parts:
+            k = p.shape[0]
+            xe = O.exact_solve(p, B[start:start + k, col])
+            xs = X[start:start + k, col]
+            assert np.linalg.norm((xs - xs.mean()) - xe) <= 1e-7 * max(np.linalg.norm(xe), 1e-30)
+            start += k
+        assert np.all(X[start:, col] == 0)
 
 
 def test_negative_weight_error(gpu_ok):

@@ -70,3 +70,34 @@ def test_group_repeatable_and_reusable(group):
             assert info.status == 0 and info.iterations <= 2
         else:
             assert info.iterations == 4 and info.status == 1, (g, info.iterations, info.status)
+
+
+def test_group_mixed_precision_matches_each_graph_alone(group):
+    """Each graph's FP32 PCG inside its own FP64 refinement, all graphs in the
+    same launches: every graph reaches the true residual tolerance and agrees
+    with the same graph solved alone in mixed precision (x within 1e-6 of it,
+    mean removed) and with the exact solution."""
+    graphs, factors, gs = group
+    rng = np.random.default_rng(5)
+    bs = [rng.standard_normal(a.shape[0]) for a in graphs]
+    bs[5] = np.zeros(graphs[5].shape[0])
+    xs = gs(bs, tol=1e-9, maxits=2000, precision="mixed")
+    infos = gs.last_info
+    assert infos[5].status == 0 and np.all(xs[5] == 0)
+    for g, (a, f) in enumerate(zip(graphs, factors)):
+        if g == 5:
+            continue
+        b = bs[g] - bs[g].mean()
+        assert infos[g].status == 0, (g, infos[g].status)
+        assert O.relres(a, xs[g], b) <= 1e-9 * 1.01, (g, O.relres(a, xs[g], b))
+        assert infos[g].true_relres <= 1e-9 * 1.01
+        dev = acgpu.DeviceLapSolver(a, f)
+        x1 = dev(bs[g], tol=1e-9, maxits=2000, precision="mixed")
+        dev.close()
+        assert _rel(O.center(xs[g]), O.center(x1)) < 1e-6, g
+        xe = O.exact_solve(a, bs[g])
+        assert _rel(O.center(xs[g]), xe) < 1e-5, g
+    # repeatable
+    xs2 = gs(bs, tol=1e-9, maxits=2000, precision="mixed")
+    for a1, a2 in zip(xs, xs2):
+        assert np.array_equal(a1, a2)
