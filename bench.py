@@ -677,8 +677,8 @@ def serve_stream(pool, factors, nreq, rate, hbm_gb, seed=7):
     rhs_blocks = [np.random.default_rng(10_000 + r).standard_normal((pool[picks[r]][1].shape[0], int(ks[r])))
                   for r in range(nreq)]
     results = {}
-    for label, kw in (("batched_mixed", dict(precision="mixed", slots=4)),
-                      ("unbatched_fp64", dict(precision="fp64", slots=1, unbatched=True))):
+    for label, kw in (("batched_mixed", dict(precision="mixed", slots=64)),
+                      ("unbatched_fp64", dict(precision="fp64", unbatched=True))):
         server = SolveServer(hbm_budget=int(hbm_gb * (1 << 30)), **kw)
         for gid, a in pool:
             server.register(gid, a, ldli=factors[gid])
@@ -686,7 +686,6 @@ def serve_stream(pool, factors, nreq, rate, hbm_gb, seed=7):
             for gid, a in pool:  # warm: upload and capture every graph once
                 server.submit(gid, np.random.default_rng(1).standard_normal(a.shape[0]), tol=TOL).result()
             server.completed.clear()
-            server.launches = 0
             futs = []
             t0 = time.perf_counter()
             for r in range(nreq):

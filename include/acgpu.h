@@ -285,6 +285,44 @@ int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* o
  * (iteration_ms is not measured there). */
 int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg_kernel_times* out);
 
+/* ---- serving loop: continuous batching on the device -------------------- */
+/* The reference has no server: its closure solves one vector per call
+ * (src/approxChol.jl:1624).  A serving loop turns a one-graph solver's batched
+ * kernels into slots: one device-resident loop (a CUDA graph with a WHILE
+ * node) runs PCG iterations for every busy slot and, between iterations,
+ * admits waiting requests into free slots and hands finished solves back.
+ * Requests that arrive while others are on the GPU join the running loop as
+ * soon as a slot frees up; every right-hand side is its own PCG system with
+ * the reference's stop rules, so a result matches the same request solved
+ * alone up to the rounding of its first rho (summed in the loop body's form).
+ *   acg_serve_open: `slots` columns (rounded up to 8, 16, 32 or 64) in
+ *     `precision` 0 (FP64 PCG) or 1 (FP32 PCG inside FP64 refinement, each
+ *     column refining on its own schedule); `queue` more requests may wait
+ *     (0 = as many as slots).  Staging buffers for them are allocated here.
+ *     While the loop is open the solver's batched entry points return
+ *     ACG_ERR_BUSY; its one-vector entry points still work.
+ *   acg_serve_submit: nrhs right-hand sides (column-major, ldb >= n when
+ *     nrhs > 1), each its own solve; b is copied before the call returns; x
+ *     (same layout) is written by the time acg_serve_wait returns.  Blocks
+ *     while the queue is full.
+ *   acg_serve_poll: 1 when every column of the ticket has finished, else 0.
+ *   acg_serve_wait: blocks until then, fills info[nrhs], frees the ticket and
+ *     returns what acg_solve would have.
+ *   acg_serve_stats: launches of the loop so far (an idle loop ends and the
+ *     next request relaunches it) and right-hand sides finished.
+ *   acg_serve_close: waits for the loop to go idle and frees it; every
+ *     ticket must have been waited (else ACG_ERR_BUSY).  acg_destroy closes a
+ *     solver's open loop. */
+typedef struct acg_server acg_server;
+typedef struct acg_ticket acg_ticket;
+int acg_serve_open(acg_solver* h, int precision, int slots, int queue, acg_server** out);
+int acg_serve_submit(acg_server* s, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol,
+                     int64_t maxits, double maxtime, int stag_test, acg_ticket** out);
+int acg_serve_poll(acg_ticket* t);
+int acg_serve_wait(acg_ticket* t, acg_solve_info* info);
+int acg_serve_stats(acg_server* s, int64_t* launches, int64_t* completed);
+int acg_serve_close(acg_server* s);
+
 /* ---- allocation-free preconditioner application ------------------------ */
 /* No counterpart in the reference (its Julia LDLsolver allocates freely).
  * y_dev = LDLsolver(ldli, r_dev), as acg_ldlsolve computes it, for vectors

@@ -114,6 +114,16 @@ SIGNATURES = [
                                               ctypes.POINTER(AcgKernelTimes)]),
     ("acg_ldlsolve_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                             ctypes.c_void_p]),
+    ("acg_serve_open", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_void_p)]),
+    ("acg_serve_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                        ctypes.c_int64, ctypes.c_double, ctypes.c_int64, ctypes.c_double, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    ("acg_serve_poll", ctypes.c_int, [ctypes.c_void_p]),
+    ("acg_serve_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AcgSolveInfo)]),
+    ("acg_serve_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64),
+                                       ctypes.POINTER(ctypes.c_int64)]),
+    ("acg_serve_close", ctypes.c_int, [ctypes.c_void_p]),
 ]
 
 _lib = None

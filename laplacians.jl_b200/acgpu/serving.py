@@ -1,18 +1,24 @@
 """Continuous-batching solve server on one GPU.
 
-Requests name a registered graph and carry 1..64 right-hand sides.  The
-server keeps one device solver per graph (factor uploaded once, cached on the
-device, evicted least-recently-used when a new graph would exceed the HBM
-budget), a queue of pending requests per graph, and `slots` worker threads.
-A free worker takes the graph whose oldest pending request is oldest, merges
-that graph's pending requests (up to 64 right-hand sides) into one batched
-launch on that solver's own CUDA stream, and completes their futures.  Work
-of different graphs therefore overlaps on the device, and requests that
-arrive while a graph's launch is running join its next launch.
+Requests name a registered graph and carry one or more right-hand sides.
+Every graph that has work is resident on the device: its solver (lap(a) and
+the LDLinv factor, uploaded once) and a device-resident serving loop
+(ServeLoop, acg_serve_* in include/acgpu.h) whose slots are the batched
+solver's columns.  A request's right-hand sides are handed to the loop as
+soon as they arrive; the loop admits them into free slots between PCG
+iterations while other solves are running, and hands each solve back the
+moment it stops.  So requests that arrive while others are on the GPU join
+the running launch, and nothing waits for a batch to fill or to drain.
 
-Every right-hand side stays its own PCG system inside a batch, so a result is
-the same as the request solved alone up to the rounding of the per-column
-reductions (the batched tests bound the difference).
+Residency is bounded by an HBM budget: a graph is uploaded when its first
+request arrives (outside the server's lock, so requests on resident graphs
+are not held up), and when the budget would be exceeded the least recently
+used graphs with no work in flight are evicted.  Different graphs have their
+own loops on their own CUDA streams; their kernels interleave on the device.
+
+Every right-hand side stays its own PCG system, so a result is that of the
+same request solved alone up to rounding (tests/test_gpu_serve_loop.py and
+tests/test_gpu_serving.py hold it to the batched tests' tolerances).
 
 The reference has no server: its closure solves one vector per call
 (src/approxChol.jl:1624); this module is the serving layer around it.
@@ -27,7 +33,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .solvers import DeviceLapSolver, approx_chol, seed as rng_seed
+from .solvers import DeviceLapSolver, ServeLoop, approx_chol, seed as rng_seed
 
 __all__ = ["SolveServer", "Request", "AdmissionError"]
 
@@ -45,6 +51,7 @@ class Request:
     future: Future = field(default_factory=Future)
     t_start: float = 0.0
     t_done: float = 0.0
+    ticket: object = None
 
 
 class _GraphEntry:
@@ -53,8 +60,10 @@ class _GraphEntry:
         self.a = a
         self.ldli = ldli
         self.solver: DeviceLapSolver | None = None
+        self.loop: ServeLoop | None = None
         self.bytes = 0
-        self.busy = False
+        self.loading = False
+        self.inflight = 0
         self.last_used = 0.0
         self.queue: collections.deque[Request] = collections.deque()
 
@@ -62,26 +71,30 @@ class _GraphEntry:
 class SolveServer:
     """Serve Laplacian solves with device-resident factors and continuous batching.
 
-    hbm_budget: bytes of device memory the cached solvers may hold together.
-    slots: concurrent launches (worker threads, one CUDA stream per solver).
+    hbm_budget: bytes of device memory the resident graphs may hold together.
     precision: "mixed" (FP32 PCG in FP64 refinement) or "fp64".
+    slots: columns of each graph's serving loop (8, 16, 32 or 64).
+    queue: requests that may wait in a loop's ring beside its busy slots.
+    unbatched: the baseline instead: one request at a time, one right-hand
+      side per solve, through the plain solve entry.
     """
 
-    def __init__(self, hbm_budget: int, slots: int = 4, precision: str = "mixed", max_batch: int = 64,
-                 maxits: int = 2000, unbatched: bool = False):
-        self.unbatched = bool(unbatched)  # baseline: one request per launch, one right-hand side per solve
+    def __init__(self, hbm_budget: int, slots: int = 64, precision: str = "mixed", maxits: int = 2000,
+                 unbatched: bool = False, queue: int = 64):
+        self.unbatched = bool(unbatched)
         self.hbm_budget = int(hbm_budget)
         self.slots = int(slots)
+        self.queue = int(queue)
         self.precision = precision
-        self.max_batch = int(max_batch)
         self.maxits = maxits
         self._graphs: dict[object, _GraphEntry] = {}
         self._cv = threading.Condition()
         self._stop = False
         self._resident = 0
-        self._workers: list[threading.Thread] = []
+        self._threads: list[threading.Thread] = []
+        self._pending: list[Request] = []  # handed to a loop, not yet finished
         self.completed: list[Request] = []
-        self.launches = 0
+        self.uploads = 0
 
     # ---- graphs -------------------------------------------------------------
     def register(self, gid, a, ldli=None, seed: int | None = None):
@@ -93,42 +106,66 @@ class SolveServer:
         with self._cv:
             self._graphs[gid] = _GraphEntry(gid, a, ldli)
 
-    def _ensure_resident(self, e: _GraphEntry) -> bool:
-        """Called with the lock held.  Uploads e's solver if it is not on the
-        device, evicting idle solvers (least recently used first, those with
-        no queued work before those with some).  False when it cannot fit now
-        because the other solvers are busy."""
-        if e.solver is not None:
-            return True
-        est = self._estimate_bytes(e)
-        if est > self.hbm_budget:
-            raise AdmissionError(f"graph {e.gid!r} needs ~{est} bytes, budget {self.hbm_budget}")
-        if self._resident + est > self.hbm_budget:
-            idle = [g for g in self._graphs.values() if g.solver is not None and not g.busy and g is not e]
-            idle.sort(key=lambda g: (len(g.queue) > 0, g.last_used))
-            freeable = sum(g.bytes for g in idle)
-            if self._resident - freeable + est > self.hbm_budget:
-                return False
-            for victim in idle:
-                if self._resident + est <= self.hbm_budget:
-                    break
-                victim.solver.close()
-                victim.solver = None
-                self._resident -= victim.bytes
-                victim.bytes = 0
-        e.solver = DeviceLapSolver(e.a, e.ldli)
-        e.bytes = est
-        self._resident += est
-        return True
-
     def _estimate_bytes(self, e: _GraphEntry) -> int:
         n = e.a.shape[0]
         nnz_l = e.a.nnz + n
         F = e.ldli.nnz
         structure = nnz_l * 16 + 2 * F * 16 + n * 64
         vectors = n * 8 * 30
-        batch = n * self.max_batch * (9 * 8 + 3 * 8 + 8 * 4)
-        return int(structure + vectors + batch)
+        batch = n * self.slots * (9 * 8 + 3 * 8 + 8 * 4)
+        staging = 0 if self.unbatched else n * 8 * 2 * (self.slots + self.queue)
+        return int(structure + vectors + batch + staging)
+
+    def _reserve(self, e: _GraphEntry) -> bool:
+        """With the lock held: reserve e's bytes, evicting idle graphs (least
+        recently used first).  False when it cannot fit now."""
+        est = self._estimate_bytes(e)
+        if est > self.hbm_budget:
+            raise AdmissionError(f"graph {e.gid!r} needs ~{est} bytes, budget {self.hbm_budget}")
+        if self._resident + est > self.hbm_budget:
+            idle = [g for g in self._graphs.values()
+                    if g.solver is not None and not g.loading and g.inflight == 0 and not g.queue and g is not e]
+            idle.sort(key=lambda g: g.last_used)
+            if self._resident - sum(g.bytes for g in idle) + est > self.hbm_budget:
+                return False
+            for victim in idle:
+                if self._resident + est <= self.hbm_budget:
+                    break
+                self._evict(victim)
+        e.bytes = est
+        self._resident += est
+        return True
+
+    def _evict(self, g: _GraphEntry):
+        if g.loop is not None:
+            g.loop.close()
+            g.loop = None
+        g.solver.close()
+        g.solver = None
+        self._resident -= g.bytes
+        g.bytes = 0
+
+    def _load(self, e: _GraphEntry):
+        """Upload e outside the lock; its queued requests go out afterwards."""
+        err = None
+        solver = loop = None
+        try:
+            solver = DeviceLapSolver(e.a, e.ldli)
+            if not self.unbatched:
+                loop = ServeLoop(solver, precision=self.precision, slots=self.slots, queue=self.queue)
+        except Exception as exc:  # noqa: BLE001 - forwarded to the waiting callers
+            err = exc
+        with self._cv:
+            e.loading = False
+            if err is not None:
+                self._resident -= e.bytes
+                e.bytes = 0
+                while e.queue:
+                    e.queue.popleft().future.set_exception(err)
+            else:
+                e.solver, e.loop = solver, loop
+                self.uploads += 1
+            self._cv.notify_all()
 
     # ---- requests -----------------------------------------------------------
     def submit(self, gid, B, tol: float = 1e-8) -> Future:
@@ -139,19 +176,18 @@ class SolveServer:
         with self._cv:
             if gid not in self._graphs:
                 raise KeyError(f"graph {gid!r} not registered")
-            if B.shape[1] > self.max_batch:
-                raise ValueError(f"at most {self.max_batch} right-hand sides per request")
             self._graphs[gid].queue.append(req)
-            self._cv.notify()
+            self._cv.notify_all()
         return req.future
 
-    # ---- workers ------------------------------------------------------------
+    # ---- threads ------------------------------------------------------------
     def start(self):
         self._stop = False
-        for i in range(self.slots):
-            t = threading.Thread(target=self._worker, name=f"acgpu-slot-{i}", daemon=True)
+        targets = [self._dispatch_unbatched] if self.unbatched else [self._dispatch, self._complete]
+        for f in targets:
+            t = threading.Thread(target=f, name=f"acgpu-{f.__name__}", daemon=True)
             t.start()
-            self._workers.append(t)
+            self._threads.append(t)
         return self
 
     def stop(self, wait: bool = True):
@@ -159,16 +195,15 @@ class SolveServer:
             self._stop = True
             self._cv.notify_all()
         if wait:
-            for t in self._workers:
+            for t in self._threads:
                 t.join()
-        self._workers.clear()
+        self._threads.clear()
 
     def close(self):
         self.stop()
         for e in self._graphs.values():
             if e.solver is not None:
-                e.solver.close()
-                e.solver = None
+                self._evict(e)
         self._resident = 0
 
     def __enter__(self):
@@ -177,79 +212,127 @@ class SolveServer:
     def __exit__(self, *exc):
         self.close()
 
-    def _next_batch(self):
-        """With the lock held: pick a graph and the requests of its next launch.
-        Graphs are tried in order of their oldest pending request; one that
-        cannot be made resident now is skipped for a resident one."""
-        cands = [e for e in self._graphs.values() if not e.busy and e.queue]
-        cands.sort(key=lambda e: e.queue[0].t_submit)
-        for best in cands:
-            try:
-                if not self._ensure_resident(best):
-                    continue
-            except AdmissionError as exc:
-                while best.queue:
-                    best.queue.popleft().future.set_exception(exc)
-                continue
-            reqs, cols = [], 0
-            while best.queue and cols + best.queue[0].B.shape[1] <= self.max_batch:
-                r = best.queue.popleft()
-                reqs.append(r)
-                cols += r.B.shape[1]
-                if self.unbatched:
-                    break
-            best.busy = True
-            return best, reqs
-        return None, None
+    def _idle(self):
+        return not any(e.queue or e.loading for e in self._graphs.values()) and not self._pending
 
-    def _worker(self):
+    def _dispatch(self):
+        """Hand queued requests to their graphs' loops, uploading graphs as needed."""
+        while True:
+            load = None
+            with self._cv:
+                while True:
+                    if self._stop and self._idle():
+                        return
+                    ready = [e for e in self._graphs.values() if e.queue and e.loop is not None]
+                    waiting = [e for e in self._graphs.values() if e.queue and e.solver is None and not e.loading]
+                    if ready or waiting:
+                        break
+                    self._cv.wait(timeout=0.05)
+                for e in ready:
+                    while e.queue:
+                        r = e.queue.popleft()
+                        r.t_start = time.perf_counter()
+                        try:
+                            r.ticket = e.loop.submit(r.B, tol=r.tol, maxits=self.maxits)
+                        except Exception as exc:  # noqa: BLE001
+                            r.future.set_exception(exc)
+                            continue
+                        e.inflight += 1
+                        self._pending.append(r)
+                        self._cv.notify_all()
+                waiting.sort(key=lambda e: e.queue[0].t_submit)
+                for e in waiting:
+                    try:
+                        if self._reserve(e):
+                            e.loading = True
+                            load = e
+                            break
+                    except AdmissionError as exc:
+                        while e.queue:
+                            e.queue.popleft().future.set_exception(exc)
+                if load is None and not ready:
+                    # nothing fits until resident graphs finish their work
+                    self._cv.wait(timeout=0.01)
+            if load is not None:
+                self._load(load)
+
+    def _complete(self):
+        """Finish the requests whose solves have all stopped."""
+        while True:
+            with self._cv:
+                while not self._pending:
+                    if self._stop and self._idle():
+                        return
+                    self._cv.wait(timeout=0.05)
+                pending = list(self._pending)
+            finished = [r for r in pending if r.ticket.done()]
+            if not finished:
+                time.sleep(5e-5)
+                continue
+            for r in finished:
+                try:
+                    X = r.ticket.wait()
+                    res, exc = (X.reshape(r.B.shape).copy(), list(r.ticket.info)), None
+                except Exception as e:  # noqa: BLE001
+                    res, exc = None, e
+                r.t_done = time.perf_counter()
+                with self._cv:
+                    self._pending.remove(r)
+                    g = self._graphs[r.gid]
+                    g.inflight -= 1
+                    g.last_used = r.t_done
+                    self.completed.append(r)
+                    self._cv.notify_all()
+                if exc is None:
+                    r.future.set_result(res)
+                else:
+                    r.future.set_exception(exc)
+
+    def _dispatch_unbatched(self):
+        """The baseline: requests one at a time in arrival order, one right-hand
+        side per solve."""
         while True:
             with self._cv:
                 while True:
+                    cands = [e for e in self._graphs.values() if e.queue]
+                    if cands:
+                        break
                     if self._stop:
                         return
-                    e, reqs = self._next_batch()
-                    if e is not None:
-                        break
                     self._cv.wait(timeout=0.05)
+                e = min(cands, key=lambda g: g.queue[0].t_submit)
+                r = e.queue.popleft()
+                if e.solver is None:
+                    try:
+                        fits = self._reserve(e)
+                        if not fits:  # nothing runs meanwhile: every other graph is idle
+                            for g in self._graphs.values():
+                                if g.solver is not None and g is not e:
+                                    self._evict(g)
+                            fits = self._reserve(e)
+                    except AdmissionError as exc:
+                        r.future.set_exception(exc)
+                        continue
+                    e.loading = fits
+            if e.loading:
+                self._load(e)
+            r.t_start = time.perf_counter()
             try:
-                self._run(e, reqs)
-            finally:
-                with self._cv:
-                    e.busy = False
-                    e.last_used = time.perf_counter()
-                    self._cv.notify_all()
-
-    def _run(self, e: _GraphEntry, reqs: list[Request]):
-        t0 = time.perf_counter()
-        B = np.concatenate([r.B for r in reqs], axis=1)
-        tol = min(r.tol for r in reqs)
-        try:
-            if self.unbatched:
                 cols, infos = [], []
-                for c in range(B.shape[1]):
-                    cols.append(e.solver(B[:, c], tol=tol, maxits=self.maxits, precision=self.precision))
+                for c in range(r.B.shape[1]):
+                    cols.append(e.solver(r.B[:, c], tol=r.tol, maxits=self.maxits, precision=self.precision))
                     infos += list(e.solver.last_info)
-                X = np.stack(cols, axis=1)
-            else:
-                X = e.solver(B, tol=tol, maxits=self.maxits, precision=self.precision)
-                infos = list(e.solver.last_info)
-        except Exception as exc:  # noqa: BLE001 - forwarded to every waiting caller
-            for r in reqs:
-                r.future.set_exception(exc)
-            return
-        X = X.reshape(B.shape)
-        t1 = time.perf_counter()
-        c = 0
-        with self._cv:
-            self.launches += 1
-        for r in reqs:
-            k = r.B.shape[1]
-            r.t_start, r.t_done = t0, t1
-            r.future.set_result((X[:, c:c + k].copy(), infos[c:c + k]))
-            c += k
+                res, exc = (np.stack(cols, axis=1), infos), None
+            except Exception as ex:  # noqa: BLE001
+                res, exc = None, ex
+            r.t_done = time.perf_counter()
             with self._cv:
+                e.last_used = r.t_done
                 self.completed.append(r)
+            if exc is None:
+                r.future.set_result(res)
+            else:
+                r.future.set_exception(exc)
 
     # ---- statistics -------------------------------------------------------------
     def latency_stats(self):
@@ -258,6 +341,7 @@ class SolveServer:
         if not len(lat):
             return {}
         span = max(r.t_done for r in self.completed) - min(r.t_submit for r in self.completed)
+        launches = sum(e.loop.stats()["launches"] for e in self._graphs.values() if e.loop is not None)
         return {"requests": len(lat), "solves": cols, "solves_per_s": cols / span if span > 0 else None,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                "mean_ms": float(lat.mean() * 1e3), "launches": self.launches}
+                "mean_ms": float(lat.mean() * 1e3), "loop_launches": launches, "uploads": self.uploads}

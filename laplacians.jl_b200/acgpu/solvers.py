@@ -33,6 +33,7 @@ from ._lib import AcgOptions, AcgSolveInfo, AcgStats, check, lib
 __all__ = [
     "ApproxCholParams", "LDLinv", "approxchol_lap", "approxchol_lap1", "lap", "seed", "rng_state",
     "set_rng_state", "approx_chol", "components", "vec_to_comps", "DeviceLapSolver", "GroupSolver", "null_solver",
+    "ServeLoop", "Ticket",
 ]
 
 _PRECISIONS = {"fp64": 0, "mixed": 1}
@@ -367,6 +368,76 @@ class AsyncSolve:
         if getattr(self, "_req", None) is not None:
             self._lib.acg_wait(self._req, None)
             self._req = None
+
+
+class ServeLoop:
+    """A device-resident serving loop on one solver (acg_serve_open): requests
+    of one or more right-hand sides join the running loop as slots free up,
+    and every right-hand side is its own PCG system with the reference's stop
+    rules.  submit() returns a Ticket at once; Ticket.wait() gives x."""
+
+    def __init__(self, solver: DeviceLapSolver, precision="mixed", slots=64, queue=0):
+        h = ctypes.c_void_p()
+        check(lib().acg_serve_open(solver._h, _PRECISIONS[precision], int(slots), int(queue), ctypes.byref(h)))
+        self._h = h
+        self._lib = lib()
+        self.solver = solver
+        self.n = solver.n
+        self.precision = precision
+
+    def submit(self, b, tol=1e-8, maxits=2000, maxtime=math.inf, stag_test=None) -> "Ticket":
+        b = np.asarray(b, dtype=np.float64)
+        if b.shape[0] != self.n:
+            raise ValueError(f"rhs has {b.shape[0]} rows, solver has {self.n}")
+        cols = b.reshape(self.n, -1)
+        B = np.ascontiguousarray(cols.T)
+        X = np.empty_like(B)
+        t = ctypes.c_void_p()
+        st = self.solver.params.stag_test if stag_test is None else stag_test
+        check(self._lib.acg_serve_submit(self._h, B.ctypes.data, X.ctypes.data, B.shape[0], self.n, float(tol),
+                                         _maxits_int(maxits), float(maxtime), int(st), ctypes.byref(t)))
+        return Ticket(self, t, X, b.shape)
+
+    def stats(self) -> dict:
+        """Loop launches so far and right-hand sides finished."""
+        la, co = ctypes.c_int64(), ctypes.c_int64()
+        check(self._lib.acg_serve_stats(self._h, ctypes.byref(la), ctypes.byref(co)))
+        return {"launches": la.value, "completed": co.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            check(self._lib.acg_serve_close(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Ticket:
+    """A request submitted to a ServeLoop; holds its x block until wait()."""
+
+    def __init__(self, loop, t, X, shape):
+        self._loop, self._t, self._X, self._shape = loop, t, X, shape
+        self.info: list[AcgSolveInfo] = []
+        self.rc = None
+
+    def done(self) -> bool:
+        if self._t is None:
+            return True
+        return check(self._loop._lib.acg_serve_poll(self._t)) == 1
+
+    def wait(self):
+        if self._t is not None:
+            k = self._X.shape[0]
+            infos = (AcgSolveInfo * k)()
+            t, self._t = self._t, None
+            rc = self._loop._lib.acg_serve_wait(t, infos)
+            self.info = list(infos)
+            self.rc = check(rc)
+        return self._X.T.reshape(self._shape)
 
 
 class GroupSolver:

@@ -723,7 +723,9 @@ __global__ void __launch_bounds__(kBVecThreads) kb_yzr(int n, int kp, const T* _
       const double mu = tot[0] / (double)n;
       st[c].mean = mu;
       if (bs->sweep_error && !st[c].done) mark_stop(&st[c], kSweepTimeout);
-      if (!st[c].done && !pcg_scalar_rho(&st[c], tot[1] - mu * tot[2])) {
+      if (!st[c].done && st[c].entering) {
+        pcg_scalar_enter(&st[c], tot[1] - mu * tot[2]);
+      } else if (!st[c].done && !pcg_scalar_rho(&st[c], tot[1] - mu * tot[2])) {
         if (st[c].itcnt % 10 == 0)
           deferred = true;
         else
@@ -775,7 +777,7 @@ __global__ void __launch_bounds__(kBVecThreads) kb_pupdate_z(int n, int kp, cons
   double tot[1];
   if (batch_reduce<1>(acc, kp, partials, &bs->counter[9], tot)) {
     const int cc = threadIdx.x;
-    if (cc < kp && !st[cc].done && st[cc].itcnt % 10 == 0) {
+    if (cc < kp && !st[cc].done && st[cc].itcnt > 0 && st[cc].itcnt % 10 == 0) {
       st[cc].sum_abs_z = tot[0];
       pcg_scalar_tail(&st[cc], eps);
     }
@@ -913,7 +915,9 @@ __global__ void __launch_bounds__(kVecThreads) kb_true_residual(int n, const int
                                                                 const double* __restrict__ val,
                                                                 const double* __restrict__ x,
                                                                 const double* __restrict__ bm, double* __restrict__ rout,
-                                                                PcgState* st, BatchShared* bs, double* partials) {
+                                                                PcgState* st, BatchShared* bs, double* partials,
+                                                                const int* gate = nullptr) {
+  if (gate && !*gate) return;  // serving loop: only on ticks where some column needs it
   constexpr int kp = CPL * kBatchLanes;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int gl = gt & 7;

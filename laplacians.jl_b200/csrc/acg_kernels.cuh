@@ -61,6 +61,8 @@ struct PcgState {
   int max_outer;
   int sweep_error;             // a bounded wait of a sync-free sweep gave up
   long long nvert;             // vertices of this system (graphs of a group)
+  int entering;                // joined a running serving loop: this pass is its pre-loop step
+  int pad1;
   unsigned int counter[16];    // last-block tickets of the reducing kernels
 };
 

@@ -58,6 +58,10 @@ __device__ __forceinline__ bool mark_stop(PcgState* st, int code) {
 // after q = L p: alpha and the first two L1 stagnation tests (src/pcg.jl:288-338)
 __device__ __forceinline__ bool pcg_scalar_pq(PcgState* st, double pq, double sum_abs_p, double sum_abs_q,
                                               double eps) {
+  if (st->entering) {  // no step yet: x and r stay, the sweeps then give z = pre(r)
+    st->alpha = 0.0;
+    return false;
+  }
   st->itcnt += 1;
   st->sum_abs_p = sum_abs_p;
   st->sum_abs_q = sum_abs_q;
@@ -72,6 +76,7 @@ __device__ __forceinline__ bool pcg_scalar_pq(PcgState* st, double pq, double su
 
 // after x += alpha p, r -= alpha q: |r|/|b|, bestx, convergence (src/pcg.jl:348-361)
 __device__ __forceinline__ bool pcg_scalar_update(PcgState* st, double rr, double sum_abs_x, double sum_abs_r) {
+  if (st->entering) return false;
   const double nr = sqrt(rr) / st->nb;
   st->nr = nr;
   st->sum_abs_x = sum_abs_x;
@@ -115,6 +120,19 @@ __device__ __forceinline__ bool pcg_scalar_tail(PcgState* st, double eps) {
   if (st->itcnt % 10 == 0 && st->beta * st->sum_abs_p < eps * st->sum_abs_z) return mark_stop(st, kStagP);
   const double el = (double)(globaltimer_ns() - st->t_start) * 1e-9;
   if (el > st->maxtime_s) return mark_stop(st, kMaxtime);
+  if (st->itcnt >= st->maxits) return mark_stop(st, kMaxits);
+  return false;
+}
+
+// The pre-loop step of a system that joined a running serving loop, taken in
+// the loop body once its z = pre(r) is known: rho = best_rho = z.r, beta = 0
+// (so p = z), as pcg_scalar_zdot's init branch (src/pcg.jl:271-286).
+__device__ __forceinline__ bool pcg_scalar_enter(PcgState* st, double zr) {
+  st->entering = 0;
+  st->rho = zr;
+  st->best_rho = zr;
+  st->stag_count = 0;
+  st->beta = 0.0;
   if (st->itcnt >= st->maxits) return mark_stop(st, kMaxits);
   return false;
 }

@@ -5,7 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -20,6 +22,7 @@
 #include "acg_batch.cuh"
 #include "acg_dense.cuh"
 #include "acg_group.cuh"
+#include "acg_serve.cuh"
 
 namespace acg {
 
@@ -176,6 +179,8 @@ struct SolverImpl {
     acg_request* owner = nullptr;  // request whose results are not yet collected
   };
   bool async_on = false;
+  bool serving = false;  // a serving loop (acg_serve_open) owns the batch buffers
+  acg_server* server = nullptr;
   cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
   AsyncSlot slots[2];
   int next_slot = 0;
@@ -2218,6 +2223,183 @@ int submit_async(acg_solver* h, const double* B, double* X, int k, int64_t ld, d
   return ACG_OK;
 }
 
+// ============================================================================
+// Serving loop (acg_serve_*): continuous batching in one device-resident loop
+// ============================================================================
+
+// The loop graph: WHILE(any slot busy or a request waiting) { one tick }, see
+// acg_serve.cuh.  The iteration kernels get no loop handle: a tick whose
+// columns all stopped skips the rest of its iteration, and only ks_admit ends
+// the loop.
+template <int CPL>
+cudaGraphExec_t build_serve_graph(SolverImpl& S, int precision, ServeRing* ring, ServeRequest* reqs,
+                                  ServeSlots* sl) {
+  constexpr int kp = CPL * kBatchLanes;
+  cudaStream_t s = S.stream;
+  const int n = S.n;
+  const double eps32 = 1.1920928955078125e-07;
+  const int mixed = precision == 1;
+  cudaGraph_t top;
+  ACG_CUDA(cudaGraphCreate(&top, 0));
+  cudaGraphConditionalHandle h;
+  ACG_CUDA(cudaGraphConditionalHandleCreate(&h, top, 1u, cudaGraphCondAssignDefault));
+  const LoopCtl ctl{h, 1};
+  const LoopCtl none{0, 0};
+  cudaGraph_t body;
+  add_while(top, {}, h, &body);
+  begin_into(s, body, {});
+  ks_admit<<<1, kMaxBatch, 0, s>>>(ring, reqs, sl, S.bst, S.bsh, kp, ctl);
+  ks_gather<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, ring, reqs, sl, S.bbm.p, S.bst, S.bsh, S.bpartials.p);
+  if (mixed) {
+    ks_center<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, S.br32.p, S.bx3_32.p, S.bxf.p,
+                                                        S.bp32.p, sl, S.bst, S.bsh, S.bpartials.p, 1);
+    ks_inner_start<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.br64.p, S.br32.p, S.bx3_32.p, S.bp32.p, sl,
+                                                             S.bst, S.bsh, S.bpartials.p);
+    ks_park<<<1, kMaxBatch, 0, s>>>(sl, S.bst, kp);
+    enqueue_biteration<float, CPL>(s, S, S.br32.p, S.bs32.p, S.by32.p, S.bp32.p, S.bq32.p, S.bx3_32.p, eps32, none);
+    ks_after_iteration<<<1, kMaxBatch, 0, s>>>(sl, S.bst, kp, 1);
+    ks_outer_correct<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bx3_32.p, S.bxf.p, sl, S.bst);
+    kb_true_residual<CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.bxf.p, S.bbm.p,
+                                                             S.br64.p, S.bst, S.bsh, S.bpartials.p, &sl->any_refine);
+    ks_outer_decide<<<1, kMaxBatch, 0, s>>>(sl, S.bst, S.bsh, kp);
+  } else {
+    ks_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, S.br64.p, S.bx3_64.p, S.bxf.p,
+                                                         S.bp64.p, sl, S.bst, S.bsh, S.bpartials.p, 0);
+    ks_park<<<1, kMaxBatch, 0, s>>>(sl, S.bst, kp);
+    enqueue_biteration<double, CPL>(s, S, S.br64.p, S.bs64.p, S.by64.p, S.bp64.p, S.bq64.p, S.bx3_64.p, kEps64,
+                                    none);
+    ks_after_iteration<<<1, kMaxBatch, 0, s>>>(sl, S.bst, kp, 0);
+    ks_take_best<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bx3_64.p, S.bxf.p, sl, S.bst);
+    kb_true_residual<CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.bxf.p, S.bbm.p,
+                                                             nullptr, S.bst, S.bsh, S.bpartials.p, &sl->any_end);
+  }
+  ks_scatter<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, ring, reqs, sl);
+  ks_finish<<<1, kMaxBatch, 0, s>>>(ring, reqs, sl, S.bst, kp, mixed);
+  end_into(s);
+  cudaGraphExec_t exec;
+  ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
+  cudaGraphDestroy(top);
+  return exec;
+}
+
+}  // namespace
+}  // namespace acg
+
+// A request of acg_serve_submit: nrhs single-right-hand-side solves.
+struct acg_ticket {
+  struct acg_server* srv = nullptr;
+  int k = 0;
+  double* x = nullptr;
+  int64_t ldx = 0;
+  int remaining = 0;
+  int rc = ACG_OK;
+  std::vector<acg_solve_info> info;
+};
+
+struct acg_server {
+  acg_solver* h = nullptr;
+  int precision = 0, kp = 0, capacity = 0;
+  acg::ServeRing* ring_h = nullptr;
+  acg::ServeRing* ring_d = nullptr;
+  acg::ServeRequest* reqs_h = nullptr;
+  acg::ServeRequest* reqs_d = nullptr;
+  acg::ServeSlots* slots = nullptr;
+  std::vector<double*> bstage, xstage;            // device staging per ring entry
+  std::vector<std::pair<acg_ticket*, int>> owner;  // per ring entry: (ticket, column) in flight
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t loop_stream = nullptr, in_stream = nullptr, out_stream = nullptr;
+  cudaEvent_t loop_done = nullptr;
+  std::thread manager;
+  std::mutex mu;
+  std::condition_variable cv;
+  bool closing = false, launched = false;
+  unsigned long long published = 0;
+  int err = ACG_OK;
+  std::string err_msg;
+  int device = 0;
+  int outstanding = 0;                  // tickets submitted and not yet waited
+  int64_t launches = 0, completed = 0;  // loop launches, right-hand sides finished
+};
+
+namespace acg {
+namespace {
+
+// Ends the ring entry e's request column: x to the caller, info, entry freed.
+// Called by the manager thread with srv->mu held.
+void serve_complete(acg_server* srv, int e) {
+  acg_ticket* t = srv->owner[e].first;
+  const int c = srv->owner[e].second;
+  const ServeRequest& r = srv->reqs_h[e];
+  const int n = srv->h->impl.n;
+  cudaError_t ce = cudaMemcpyAsync(t->x + (size_t)c * t->ldx, srv->xstage[e], sizeof(double) * n,
+                                   cudaMemcpyDeviceToHost, srv->out_stream);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(srv->out_stream);
+  acg_solve_info& in = t->info[c];
+  in.iterations = r.iterations;
+  in.refinements = r.refinements;
+  in.relres = r.relres;
+  in.best_relres = r.true_relres;
+  in.true_relres = r.true_relres;
+  in.solve_ms = r.solve_ms;
+  in.status = r.status;
+  in.levels = srv->h->impl.nlev;
+  const int rc = ce == cudaSuccess ? status_to_rc(r.status) : ACG_ERR_CUDA;
+  if (ce != cudaSuccess) cudaGetLastError();
+  if (rc < 0) t->rc = t->rc < 0 ? t->rc : rc;
+  else if (t->rc >= 0) t->rc = std::max(t->rc, rc);
+  srv->owner[e] = {nullptr, 0};
+  t->remaining -= 1;
+  srv->completed += 1;
+}
+
+// The server's host thread: hands finished solves back, and launches the loop
+// graph whenever requests wait and it is not running.  A request published
+// just as the loop decided to end is seen here after the launch completes.
+void serve_manager(acg_server* srv) {
+  cudaSetDevice(srv->device);
+  std::unique_lock<std::mutex> lk(srv->mu);
+  while (true) {
+    bool progress = false;
+    for (int e = 0; e < srv->capacity; ++e)
+      if (srv->owner[e].first && *(volatile int*)&srv->reqs_h[e].done) {
+        serve_complete(srv, e);
+        progress = true;
+      }
+    if (progress) srv->cv.notify_all();
+    if (srv->launched && cudaEventQuery(srv->loop_done) == cudaSuccess) {
+      srv->launched = false;
+      progress = true;
+    }
+    const unsigned long long head = *(volatile unsigned long long*)&srv->ring_h->head;
+    if (!srv->launched && srv->published > head && srv->err == ACG_OK) {
+      *(volatile int*)&srv->ring_h->running = 1;
+      cudaError_t ce = cudaGraphLaunch(srv->exec, srv->loop_stream);
+      if (ce == cudaSuccess) ce = cudaEventRecord(srv->loop_done, srv->loop_stream);
+      if (ce != cudaSuccess) {
+        cudaGetLastError();
+        srv->err = ACG_ERR_CUDA;
+        srv->err_msg = std::string("serving loop launch: ") + cudaGetErrorString(ce);
+        srv->cv.notify_all();
+      } else {
+        srv->launched = true;
+        srv->launches += 1;
+      }
+      continue;
+    }
+    bool busy = false;
+    for (int e = 0; e < srv->capacity && !busy; ++e) busy = srv->owner[e].first != nullptr;
+    if (srv->closing && !busy && !srv->launched) break;
+    if (srv->launched || busy) {
+      // the loop runs: poll the done flags
+      lk.unlock();
+      std::this_thread::sleep_for(std::chrono::microseconds(progress ? 0 : 20));
+      lk.lock();
+    } else {
+      srv->cv.wait(lk);
+    }
+  }
+}
+
 }  // namespace
 }  // namespace acg
 
@@ -2312,6 +2494,7 @@ int acg_create(int64_t n, const int64_t* a_colptr, const int64_t* a_rowval, cons
 
 void acg_destroy(acg_solver* h) {
   if (!h) return;
+  if (h->impl.server) acg_serve_close(h->impl.server);
   std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
   {
     std::lock_guard<std::mutex> lk(h->impl.mu);
@@ -2368,6 +2551,10 @@ int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t l
   }
   return guarded("acg_solve", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
+    if (h->impl.serving && nrhs > 1) {
+      acg::set_last_error("acg_solve: the solver's batch buffers belong to its serving loop");
+      return ACG_ERR_BUSY;
+    }
     int worst = ACG_OK;
     if (nrhs == 1)
       return acg::solve_column(h->impl, b, x, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol, maxits, maxtime,
@@ -2387,6 +2574,10 @@ int acg_solve(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t l
 int acg_solve_async(acg_solver* h, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol,
                     int64_t maxits, double maxtime, int stag_test, int precision, acg_request** out) {
   if (out) *out = nullptr;
+  if (h && h->impl.serving) {
+    acg::set_last_error("acg_solve_async: the solver's batch buffers belong to its serving loop");
+    return ACG_ERR_BUSY;
+  }
   if (!h || !b || !x || !out || nrhs < 1 || nrhs > acg::kMaxBatch || ldb < h->impl.n ||
       (precision != 0 && precision != 1) || h->impl.nseg > 1) {
     acg::set_last_error("acg_solve_async: bad arguments (1 <= nrhs <= 64, ldb >= n, one graph)");
@@ -2509,6 +2700,10 @@ int acg_solve_batch_device(acg_solver* h, const double* b_dev, double* x_dev, in
   }
   return guarded("acg_solve_batch_device", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
+    if (h->impl.serving) {
+      acg::set_last_error("acg_solve_batch_device: the solver's batch buffers belong to its serving loop");
+      return ACG_ERR_BUSY;
+    }
     ACG_CUDA(cudaDeviceSynchronize());
     int worst = ACG_OK;
     for (int64_t c0 = 0; c0 < nrhs; c0 += acg::kMaxBatch) {
@@ -2622,6 +2817,10 @@ int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg
   *out = acg_kernel_times{};
   return guarded("acg_time_kernels_batch", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
+    if (h->impl.serving) {
+      acg::set_last_error("acg_time_kernels_batch: the solver's batch buffers belong to its serving loop");
+      return ACG_ERR_BUSY;
+    }
     std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
     acg::time_batch(h->impl, precision, acg::round_kp(nrhs), reps, out);
     return ACG_OK;
@@ -2641,6 +2840,206 @@ int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* o
     acg::time_kernels(S, precision, reps, out);
     return ACG_OK;
   });
+}
+
+// ---- serving loop -------------------------------------------------------------
+
+int acg_serve_open(acg_solver* h, int precision, int slots, int queue, acg_server** out) {
+  if (out) *out = nullptr;
+  if (!h || !out || (precision != 0 && precision != 1) || slots < 1 || slots > acg::kMaxBatch || queue < 0 ||
+      h->impl.nseg > 1) {
+    acg::set_last_error("acg_serve_open: bad arguments (one-graph solver, precision 0 or 1, 1 <= slots <= 64)");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_serve_open", [&]() {
+    acg::SolverImpl& S = h->impl;
+    std::lock_guard<std::mutex> lk(S.mu);
+    std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
+    if (S.serving) throw acg::InputError("the solver already has a serving loop");
+    ACG_CUDA(cudaSetDevice(S.device));
+    acg::drain_async(S);
+    auto srv = std::make_unique<acg_server>();
+    srv->h = h;
+    srv->precision = precision;
+    srv->device = S.device;
+    srv->kp = acg::round_kp(slots);
+    srv->capacity = srv->kp + (queue > 0 ? queue : srv->kp);
+    acg::ensure_batch(S, std::max(srv->kp, S.batch_kp));
+    const size_t ring_bytes = sizeof(acg::ServeRing);
+    const size_t reqs_bytes = sizeof(acg::ServeRequest) * srv->capacity;
+    ACG_CUDA(cudaHostAlloc(&srv->ring_h, ring_bytes, cudaHostAllocMapped));
+    ACG_CUDA(cudaHostAlloc(&srv->reqs_h, reqs_bytes, cudaHostAllocMapped));
+    std::memset(srv->ring_h, 0, ring_bytes);
+    std::memset(srv->reqs_h, 0, reqs_bytes);
+    srv->ring_h->capacity = srv->capacity;
+    ACG_CUDA(cudaHostGetDevicePointer((void**)&srv->ring_d, srv->ring_h, 0));
+    ACG_CUDA(cudaHostGetDevicePointer((void**)&srv->reqs_d, srv->reqs_h, 0));
+    ACG_CUDA(cudaMalloc(&srv->slots, sizeof(acg::ServeSlots)));
+    ACG_CUDA(cudaMemset(srv->slots, 0, sizeof(acg::ServeSlots)));
+    srv->bstage.assign(srv->capacity, nullptr);
+    srv->xstage.assign(srv->capacity, nullptr);
+    srv->owner.assign(srv->capacity, {nullptr, 0});
+    for (int e = 0; e < srv->capacity; ++e) {
+      if (cudaMalloc(&srv->bstage[e], sizeof(double) * S.n) != cudaSuccess ||
+          cudaMalloc(&srv->xstage[e], sizeof(double) * S.n) != cudaSuccess) {
+        cudaGetLastError();
+        for (int f = 0; f <= e; ++f) {
+          if (srv->bstage[f]) cudaFree(srv->bstage[f]);
+          if (srv->xstage[f]) cudaFree(srv->xstage[f]);
+        }
+        cudaFree(srv->slots);
+        cudaFreeHost(srv->ring_h);
+        cudaFreeHost(srv->reqs_h);
+        throw acg::DeviceNoMem("serving staging buffers");
+      }
+    }
+    // every slot free and stopped; the batch flags clear
+    std::vector<acg::PcgState> st0(acg::kMaxBatch);
+    std::memset(st0.data(), 0, sizeof(acg::PcgState) * acg::kMaxBatch);
+    for (auto& x : st0) x.done = 1;
+    ACG_CUDA(cudaMemcpy(S.bst, st0.data(), sizeof(acg::PcgState) * acg::kMaxBatch, cudaMemcpyHostToDevice));
+    ACG_CUDA(cudaMemset(S.bsh, 0, sizeof(acg::BatchShared)));
+    acg::with_cpl(srv->kp, [&](auto cpl) {
+      constexpr int C = decltype(cpl)::value;
+      srv->exec = acg::build_serve_graph<C>(S, precision, srv->ring_d, srv->reqs_d, srv->slots);
+    });
+    ACG_CUDA(cudaStreamCreateWithFlags(&srv->loop_stream, cudaStreamNonBlocking));
+    ACG_CUDA(cudaStreamCreateWithFlags(&srv->in_stream, cudaStreamNonBlocking));
+    ACG_CUDA(cudaStreamCreateWithFlags(&srv->out_stream, cudaStreamNonBlocking));
+    ACG_CUDA(cudaEventCreateWithFlags(&srv->loop_done, cudaEventDisableTiming));
+    ACG_CUDA(cudaStreamSynchronize(S.stream));
+    S.serving = true;
+    S.server = srv.get();
+    acg_server* raw = srv.get();
+    raw->manager = std::thread(acg::serve_manager, raw);
+    *out = srv.release();
+    return ACG_OK;
+  });
+}
+
+int acg_serve_submit(acg_server* srv, const double* b, double* x, int64_t nrhs, int64_t ldb, double tol,
+                     int64_t maxits, double maxtime, int stag_test, acg_ticket** out) {
+  if (out) *out = nullptr;
+  if (!srv || !b || !x || !out || nrhs < 1 || (nrhs > 1 && ldb < srv->h->impl.n)) {
+    acg::set_last_error("acg_serve_submit: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_serve_submit", [&]() {
+    const int n = srv->h->impl.n;
+    auto t = std::make_unique<acg_ticket>();
+    t->srv = srv;
+    t->k = (int)nrhs;
+    t->x = x;
+    t->ldx = nrhs > 1 ? ldb : n;
+    t->remaining = (int)nrhs;
+    t->info.assign((size_t)nrhs, acg_solve_info{});
+    std::unique_lock<std::mutex> lk(srv->mu);
+    if (srv->closing) throw acg::InputError("the serving loop is closing");
+    for (int64_t c = 0; c < nrhs; ++c) {
+      const int e = (int)(srv->published % (unsigned long long)srv->capacity);
+      // the entry is reused once its previous request has been completed
+      srv->cv.wait(lk, [&]() { return srv->owner[e].first == nullptr || srv->err != ACG_OK; });
+      if (srv->err != ACG_OK) throw acg::CudaError(srv->err_msg);
+      ACG_CUDA(cudaMemcpyAsync(srv->bstage[e], b + (size_t)c * (nrhs > 1 ? ldb : n), sizeof(double) * n,
+                               cudaMemcpyHostToDevice, srv->in_stream));
+      ACG_CUDA(cudaStreamSynchronize(srv->in_stream));
+      acg::ServeRequest& r = srv->reqs_h[e];
+      r.b = srv->bstage[e];
+      r.x = srv->xstage[e];
+      r.tol = tol;
+      r.maxtime = maxtime;
+      r.maxits = maxits;
+      r.stag_test = stag_test;
+      r.done = 0;
+      srv->owner[e] = {t.get(), (int)c};
+      std::atomic_thread_fence(std::memory_order_seq_cst);
+      srv->published += 1;
+      *(volatile unsigned long long*)&srv->ring_h->tail = srv->published;
+      srv->cv.notify_all();
+    }
+    srv->outstanding += 1;
+    *out = t.release();
+    return ACG_OK;
+  });
+}
+
+int acg_serve_poll(acg_ticket* t) {
+  if (!t || !t->srv) {
+    acg::set_last_error("acg_serve_poll: null ticket");
+    return ACG_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(t->srv->mu);
+  if (t->srv->err != ACG_OK) {
+    acg::set_last_error(t->srv->err_msg);
+    return t->srv->err;
+  }
+  return t->remaining == 0 ? 1 : 0;
+}
+
+int acg_serve_wait(acg_ticket* t, acg_solve_info* info) {
+  if (!t || !t->srv) {
+    acg::set_last_error("acg_serve_wait: null ticket");
+    return ACG_ERR_INVALID;
+  }
+  std::unique_ptr<acg_ticket> own(t);
+  acg_server* srv = t->srv;
+  std::unique_lock<std::mutex> lk(srv->mu);
+  srv->cv.wait(lk, [&]() { return t->remaining == 0 || srv->err != ACG_OK; });
+  srv->outstanding -= 1;
+  if (t->remaining != 0) {
+    acg::set_last_error(srv->err_msg);
+    return srv->err;
+  }
+  if (info) std::memcpy(info, t->info.data(), sizeof(acg_solve_info) * t->k);
+  if (t->rc < 0) acg::set_last_error("acg_serve_wait: a right-hand side failed (see its status)");
+  return t->rc;
+}
+
+int acg_serve_stats(acg_server* srv, int64_t* launches, int64_t* completed) {
+  if (!srv) {
+    acg::set_last_error("acg_serve_stats: null server");
+    return ACG_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(srv->mu);
+  if (launches) *launches = srv->launches;
+  if (completed) *completed = srv->completed;
+  return ACG_OK;
+}
+
+int acg_serve_close(acg_server* srv) {
+  if (!srv) return ACG_OK;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->outstanding > 0) {
+      acg::set_last_error("acg_serve_close: " + std::to_string(srv->outstanding) + " tickets not yet waited");
+      return ACG_ERR_BUSY;
+    }
+    srv->closing = true;  // requests already published are still served
+    srv->cv.notify_all();
+  }
+  if (srv->manager.joinable()) srv->manager.join();
+  acg::SolverImpl& S = srv->h->impl;
+  const int rc = srv->err;
+  {
+    std::lock_guard<std::mutex> lk(S.mu);
+    cudaStreamSynchronize(srv->loop_stream);
+    if (srv->exec) cudaGraphExecDestroy(srv->exec);
+    for (int e = 0; e < srv->capacity; ++e) {
+      cudaFree(srv->bstage[e]);
+      cudaFree(srv->xstage[e]);
+    }
+    cudaFree(srv->slots);
+    cudaFreeHost(srv->ring_h);
+    cudaFreeHost(srv->reqs_h);
+    cudaEventDestroy(srv->loop_done);
+    cudaStreamDestroy(srv->loop_stream);
+    cudaStreamDestroy(srv->in_stream);
+    cudaStreamDestroy(srv->out_stream);
+    S.serving = false;
+    S.server = nullptr;
+  }
+  delete srv;
+  return rc;
 }
 
 }  // extern "C"
