@@ -589,58 +589,84 @@ def run_grid3_64rhs(args):
 def run_many_graphs(args):
     """256 graphs in one launch: half 2D grids with side uniform in [32, 256],
     half random geometric graphs (n uniform in [1e3, 1e5], mean degree 8,
-    weights 1/distance, largest component); one right-hand side each; FP64 to
-    tol 1e-8.  Against the same graphs solved one after another."""
+    weights 1/distance), one right-hand side each, tol 1e-8.  A random
+    geometric graph may be disconnected: as approxchol_lap does
+    (lapWrapComponents, src/solverInterface.jl:212-275), each component of at
+    least 50 vertices is its own PCG system in the one group launch, smaller
+    ones are solved on the host and singletons get zero.  FP64 and mixed
+    precision, against the same graphs solved one after another."""
     import acgpu
     from acgpu import generators as G
+    from acgpu.solvers import _DenseGroundedSolver
     rng = np.random.default_rng(44)
     graphs = []
     for i in range(args.group_graphs):
-        s = int(rng.integers(1 << 30))
+        s_ = int(rng.integers(1 << 30))
         if i % 2 == 0:
-            graphs.append(G.grid2(int(rng.integers(32, 257)), weights="loguniform", seed=s))
+            graphs.append(G.grid2(int(rng.integers(32, 257)), weights="loguniform", seed=s_))
         else:
-            graphs.append(G.largest_component(G.random_geometric(int(rng.integers(1000, 100001)), seed=s)))
+            graphs.append(G.random_geometric(int(rng.integers(1000, 100001)), seed=s_))
+    # split every graph into components: members of the group, host solves, singletons
+    members, small, nsingle = [], [], 0
+    for gi, a in enumerate(graphs):
+        co = acgpu.components(a)
+        for ind in acgpu.vec_to_comps(co):
+            if len(ind) == 1:
+                nsingle += 1
+            elif len(ind) < 50:
+                small.append((gi, ind))
+            else:
+                members.append((gi, ind))
+    comp_graphs = [acgpu.solvers._csc(graphs[gi][ind][:, ind]) for gi, ind in members]
     t = time.perf_counter()
     factors = []
-    for i, a in enumerate(graphs):
+    for i, a in enumerate(comp_graphs):
         acgpu.seed(500 + i)
         factors.append(acgpu.approx_chol(a))
     factor_s = time.perf_counter() - t
     t = time.perf_counter()
-    gs = acgpu.GroupSolver(graphs, factors)
+    gs = acgpu.GroupSolver(comp_graphs, factors)
     upload_s = time.perf_counter() - t
+    small_solvers = [_DenseGroundedSolver(graphs[gi][ind][:, ind]) for gi, ind in small]
     bs = [rhs(a.shape[0], 900 + i) for i, a in enumerate(graphs)]
-    times = []
-    for rep in range(3):
-        t = time.perf_counter()
-        xs = gs(bs, tol=TOL, maxits=MAXITS)
-        times.append(time.perf_counter() - t)
-    infos = gs.last_info
-    st = gs.stats()
+    # per component: b restricted and centred (the solvable part, as blockSolver solves it)
+    comp_b = [bs[gi][ind] - bs[gi][ind].mean() for gi, ind in members]
+    small_b = [bs[gi][ind] - bs[gi][ind].mean() for gi, ind in small]
+    out = {"workload": f"{len(graphs)} graphs in one launch (2D grids side U[32,256], RGG n U[1e3,1e5] with all "
+                       "their components), 1 RHS each, tol 1e-8",
+           "n_total": int(sum(a.shape[0] for a in graphs)), "group_members": len(members),
+           "host_small_components": len(small), "singletons": nsingle, "factor_s": factor_s, "upload_s": upload_s}
+    for prec in ("fp64", "mixed"):
+        times = []
+        for rep in range(3):
+            t = time.perf_counter()
+            xs = gs(comp_b, tol=TOL, maxits=MAXITS, precision=prec)
+            for sv, b in zip(small_solvers, small_b):
+                sv(b)
+            times.append(time.perf_counter() - t)
+        infos = gs.last_info
+        out[prec] = {"group_ms": 1e3 * min(times), "graphs_per_s": len(graphs) / min(times),
+                     "its_max": max(i.iterations for i in infos),
+                     "true_relres_max": max(i.true_relres for i in infos),
+                     "all_converged": all(i.status == 0 for i in infos)}
+    out["levels_max"] = gs.stats()["levels"]
     seq = []
-    for a, f, b in zip(graphs, factors, bs):
+    for a, f, b in zip(comp_graphs, factors, comp_b):
         dev = acgpu.DeviceLapSolver(a, f)
         dev(b, tol=TOL, maxits=MAXITS)
         dev(b, tol=TOL, maxits=MAXITS)
         seq.append(dev.last_info[0].solve_ms)
         dev.close()
-    out = {"workload": f"{len(graphs)} graphs in one launch (2D grids side U[32,256], RGG n U[1e3,1e5]), "
-                       "1 RHS each, tol 1e-8, fp64",
-           "n_total": int(sum(a.shape[0] for a in graphs)), "levels_max": st["levels"], "factor_s": factor_s,
-           "upload_s": upload_s, "group_ms": 1e3 * min(times), "group_solves_per_s": len(graphs) / min(times),
-           "its_max": max(i.iterations for i in infos), "true_relres_max": max(i.true_relres for i in infos),
-           "all_converged": all(i.status == 0 for i in infos),
-           "sequential_ms": float(sum(seq)), "sequential_solves_per_s": 1e3 * len(graphs) / float(sum(seq)),
-           "speedup": float(sum(seq)) / (1e3 * min(times))}
+    out["sequential_fp64_ms"] = float(sum(seq))
+    out["speedup_fp64"] = float(sum(seq)) / out["fp64"]["group_ms"]
     print(json.dumps(out), flush=True)
     gs.close()
 
 
 def serving_graph_pool(count, seed):
     """Graphs for the serving stream: 2D/3D grids, path + random matchings and
-    random geometric graphs (largest component), n log-uniform in [1e3, 1e6],
-    lognormal(0, 1) weights."""
+    random geometric graphs (whole, components and all), n log-uniform in
+    [1e3, 1e6], lognormal(0, 1) weights."""
     from acgpu import generators as G
     rng = np.random.default_rng(seed)
     fams = ["grid2", "grid3", "matchings", "rgg"]
@@ -658,7 +684,8 @@ def serving_graph_pool(count, seed):
         elif fam == "matchings":
             a = G.path_plus_matchings(max(4, n - n % 2), k=4, sigma=1.0, seed=s)
         else:
-            a = G.largest_component(G.random_geometric(n, seed=s, weights="lognormal:1"))
+            # the whole graph: a disconnected one is served per component
+            a = G.random_geometric(n, seed=s, weights="lognormal:1")
         pool.append((f"{fam}-{a.shape[0]}", a))
     return pool
 
@@ -680,8 +707,8 @@ def serve_stream(pool, factors, nreq, rate, hbm_gb, seed=7):
     for label, kw in (("batched_mixed", dict(precision="mixed", slots=64)),
                       ("unbatched_fp64", dict(precision="fp64", unbatched=True))):
         server = SolveServer(hbm_budget=int(hbm_gb * (1 << 30)), **kw)
-        for gid, a in pool:
-            server.register(gid, a, ldli=factors[gid])
+        for i, (gid, a) in enumerate(pool):
+            server.register(gid, a, ldli=factors[gid], seed=None if factors[gid] is not None else 3000 + i)
         with server:
             for gid, a in pool:  # warm: upload and capture every graph once
                 server.submit(gid, np.random.default_rng(1).standard_normal(a.shape[0]), tol=TOL).result()
@@ -706,12 +733,14 @@ def serve_stream(pool, factors, nreq, rate, hbm_gb, seed=7):
 
 
 def factor_pool(pool, seed0):
+    """Host factors of the pool's connected graphs (a disconnected graph is
+    factored per component when the server registers it: None here)."""
     import acgpu
     factors = {}
     t = time.perf_counter()
     for i, (gid, a) in enumerate(pool):
         acgpu.seed(seed0 + i)
-        factors[gid] = acgpu.approx_chol(a)
+        factors[gid] = acgpu.approx_chol(a) if acgpu.components(a).max() == 1 else None
     return factors, time.perf_counter() - t
 
 

@@ -33,7 +33,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .solvers import DeviceLapSolver, ServeLoop, approx_chol, seed as rng_seed
+from .solvers import (DeviceLapSolver, ServeLoop, _csc, _DenseGroundedSolver, approx_chol, components,
+                      seed as rng_seed, vec_to_comps)
 
 __all__ = ["SolveServer", "Request", "AdmissionError"]
 
@@ -52,6 +53,7 @@ class Request:
     t_start: float = 0.0
     t_done: float = 0.0
     ticket: object = None
+    internal: bool = False  # one component's part of a request on a disconnected graph
 
 
 class _GraphEntry:
@@ -66,6 +68,17 @@ class _GraphEntry:
         self.inflight = 0
         self.last_used = 0.0
         self.queue: collections.deque[Request] = collections.deque()
+
+
+class _Composite:
+    """A disconnected graph (lapWrapComponents, src/solverInterface.jl:212-275):
+    components of at least 50 vertices are graphs of their own in the server
+    (keys (gid, k)), smaller ones are solved on the host, singletons get 0."""
+
+    def __init__(self, n, big, small):
+        self.n = n
+        self.big = big        # [(index array, sub-gid)]
+        self.small = small    # [(index array, host solver)]
 
 
 class SolveServer:
@@ -93,15 +106,37 @@ class SolveServer:
         self._resident = 0
         self._threads: list[threading.Thread] = []
         self._pending: list[Request] = []  # handed to a loop, not yet finished
+        self._composites: dict[object, _Composite] = {}
         self.completed: list[Request] = []
         self.uploads = 0
 
     # ---- graphs -------------------------------------------------------------
     def register(self, gid, a, ldli=None, seed: int | None = None):
-        """Add a graph (host factor built now, device upload on first use)."""
+        """Add a graph (host factor built now, device upload on first use).  A
+        disconnected graph is split into its components, as approxchol_lap does;
+        its factor is then built here per component (ldli must be None)."""
+        a = _csc(a)
+        if seed is not None and ldli is None:
+            rng_seed(seed)
+        co = components(a)
+        if co.max() > 1:
+            if ldli is not None:
+                raise ValueError("a disconnected graph is factored per component: pass ldli=None")
+            big, small = [], []
+            for k, ind in enumerate(vec_to_comps(co)):
+                if len(ind) == 1:
+                    continue
+                sub = _csc(a[ind][:, ind])
+                if len(ind) < 50:
+                    small.append((ind, _DenseGroundedSolver(sub)))
+                else:
+                    big.append((ind, (gid, k)))
+                    with self._cv:
+                        self._graphs[(gid, k)] = _GraphEntry((gid, k), sub, approx_chol(sub))
+            with self._cv:
+                self._composites[gid] = _Composite(a.shape[0], big, small)
+            return
         if ldli is None:
-            if seed is not None:
-                rng_seed(seed)
             ldli = approx_chol(a)
         with self._cv:
             self._graphs[gid] = _GraphEntry(gid, a, ldli)
@@ -172,13 +207,63 @@ class SolveServer:
         B = np.asarray(B, dtype=np.float64)
         if B.ndim == 1:
             B = B[:, None]
-        req = Request(gid, B, tol, time.perf_counter())
+        if gid in self._composites:
+            return self._submit_composite(gid, self._composites[gid], B, tol)
+        return self._submit_one(gid, B, tol).future
+
+    def _submit_one(self, gid, B, tol, internal=False) -> Request:
+        req = Request(gid, B, tol, time.perf_counter(), internal=internal)
         with self._cv:
             if gid not in self._graphs:
                 raise KeyError(f"graph {gid!r} not registered")
             self._graphs[gid].queue.append(req)
             self._cv.notify_all()
-        return req.future
+        return req
+
+    def _submit_composite(self, gid, comp: _Composite, B, tol) -> Future:
+        """One request on a disconnected graph: each large component's rows go
+        to that component's loop; the result is assembled when all are back."""
+        top = Request(gid, B, tol, time.perf_counter())
+        parts = [(ind, self._submit_one(sub, np.ascontiguousarray(B[ind]), tol, internal=True))
+                 for ind, sub in comp.big]
+        X = np.zeros(B.shape)
+        for ind, solver in comp.small:
+            for c in range(B.shape[1]):
+                X[ind, c] = solver(B[ind, c])
+        left = [len(parts)]
+        lock = threading.Lock()
+
+        def one_done(_):
+            with lock:
+                left[0] -= 1
+                if left[0]:
+                    return
+            infos, exc = [], None
+            for ind, r in parts:
+                try:
+                    Xi, inf = r.future.result()
+                    X[ind] = Xi
+                    infos.append(inf)
+                except Exception as e:  # noqa: BLE001
+                    exc = e
+            top.t_done = time.perf_counter()
+            with self._cv:
+                self.completed.append(top)
+            if exc is not None:
+                top.future.set_exception(exc)
+            else:
+                # per column: the component with the most iterations
+                cols = [max((inf[c] for inf in infos), key=lambda i: i.iterations) for c in range(B.shape[1])]
+                top.future.set_result((X, cols))
+
+        if not parts:
+            top.t_done = time.perf_counter()
+            with self._cv:
+                self.completed.append(top)
+            top.future.set_result((X, []))
+        for _, r in parts:
+            r.future.add_done_callback(one_done)
+        return top.future
 
     # ---- threads ------------------------------------------------------------
     def start(self):
@@ -336,11 +421,12 @@ class SolveServer:
 
     # ---- statistics -------------------------------------------------------------
     def latency_stats(self):
-        lat = np.array([r.t_done - r.t_submit for r in self.completed])
-        cols = sum(r.B.shape[1] for r in self.completed)
+        done = [r for r in self.completed if not r.internal]
+        lat = np.array([r.t_done - r.t_submit for r in done])
+        cols = sum(r.B.shape[1] for r in done)
         if not len(lat):
             return {}
-        span = max(r.t_done for r in self.completed) - min(r.t_submit for r in self.completed)
+        span = max(r.t_done for r in done) - min(r.t_submit for r in done)
         launches = sum(e.loop.stats()["launches"] for e in self._graphs.values() if e.loop is not None)
         return {"requests": len(lat), "solves": cols, "solves_per_s": cols / span if span > 0 else None,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),

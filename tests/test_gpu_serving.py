@@ -127,3 +127,33 @@ def _entry(a):
     from acgpu.serving import _GraphEntry
     acgpu.seed(1)
     return _GraphEntry("x", a, acgpu.approx_chol(a))
+
+
+def test_disconnected_graph_is_served_per_component(gpu_ok):
+    """A disconnected graph: each component of at least 50 vertices is served
+    by its own loop, smaller ones on the host, singletons get zero; the
+    assembled x matches the exact solve of every component."""
+    import scipy.sparse as sp
+    parts = [G.grid2(12, weights="loguniform", seed=1), G.star_graph(9), G.path_plus_matchings(400, seed=2)]
+    a = sp.block_diag(parts + [sp.csc_matrix((1, 1))] * 2, format="csc")
+    a.sort_indices()
+    n = a.shape[0]
+    B = np.random.default_rng(3).standard_normal((n, 2))
+    co = acgpu.components(a)
+    for c in np.unique(co):
+        m = co == c
+        B[m] -= B[m].mean(axis=0)
+    server = SolveServer(hbm_budget=8 << 30, slots=8, precision="fp64")
+    server.register("u", a, seed=4)
+    with server:
+        X, infos = server.submit("u", B, tol=1e-10).result(timeout=300)
+    assert server.latency_stats()["requests"] == 1
+    for col in range(2):
+        start = 0
+        for p in parts:
+            k = p.shape[0]
+            xe = O.exact_solve(p, B[start:start + k, col])
+            xs = X[start:start + k, col]
+            assert np.linalg.norm((xs - xs.mean()) - xe) <= 1e-7 * np.linalg.norm(xe)
+            start += k
+        assert np.all(X[start:, col] == 0)
