@@ -788,8 +788,9 @@ def matchings_2m_record(n=2_000_000):
 
 def run_extras(args, rank, world):
     """The rest of the metric, beside the headline (N = 1 only; each takes
-    seconds): serving p50/p99 on a short Poisson stream, and the 2M
-    path+matchings graph's level count and LDLinv GB/s."""
+    seconds): serving p50/p99 on a short Poisson stream, the 2M
+    path+matchings graph's level count and LDLinv GB/s, and the solve with the
+    opt-in parallel elimination's factor."""
     if world > 1 or rank != 0:
         return {}
     out = {}
@@ -802,7 +803,56 @@ def run_extras(args, rank, world):
                       "graphs": [(gid, int(a.shape[0])) for gid, a in pool], "factor_s_total": factor_s,
                       "wall_s": time.perf_counter() - t, **res}
     out["path_matchings_2m"] = matchings_2m_record()
+    out["parallel_factor"] = parallel_factor_record()
     return out
+
+
+def parallel_factor_record(k=64, steps=3):
+    """The opt-in parallel elimination (acgpu.approx_chol_parallel; not the
+    reference's, a different random sample) on the same 1M grid: host time on
+    all cores, rounds, the DAG depth the GPU sweeps walk, and the 64-column
+    mixed solve rate with that factor (device-resident right-hand sides)."""
+    import torch
+    import acgpu
+    from acgpu import generators as G
+    from acgpu._lib import AcgSolveInfo, check, lib
+    a = G.grid3(GRID_SIDE, weights="loguniform", seed=WEIGHT_SEED)
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    t = time.perf_counter()
+    ldli, rounds = acgpu.approx_chol_parallel(a, seed=FACTOR_SEED, threads=threads)
+    factor_s = time.perf_counter() - t
+    n = a.shape[0]
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    st = dev.stats()
+    B = torch.empty((steps + 1, k, n), dtype=torch.float64, device="cuda")
+    for i in range(steps + 1):
+        for c in range(k):
+            B[i, c] = torch.from_numpy(rhs(n, 7_000_000 + 1000 * i + c))
+    X = torch.empty((k, n), dtype=torch.float64, device="cuda")
+    infos = (AcgSolveInfo * k)()
+    res = []
+    for i in range(steps + 1):
+        if i == 1:
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        check(lib().acg_solve_batch_device(dev._h, ctypes.c_void_p(B[i].data_ptr()), ctypes.c_void_p(X.data_ptr()),
+                                           k, n, TOL, MAXITS, float("inf"), 5, 1, infos))
+        if i >= 1:
+            res += [(infos[c].iterations, infos[c].true_relres, infos[c].status) for c in range(k)]
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    kt = dev.time_kernels_batch(k, "mixed", reps=3)
+    dev.close()
+    return {"workload": f"grid3({GRID_SIDE}) log-uniform weights, factor by the opt-in parallel elimination, "
+                        f"{k} RHS per batched mixed solve, tol 1e-8",
+            "factor_s": factor_s, "threads": threads, "rounds": rounds, "factor_nnz": ldli.nnz,
+            "levels": st["levels"], "dense_levels": st["dense_levels"],
+            "solves_per_s": steps * k / (ms * 1e-3), "pcg_iterations_mean": float(np.mean([r[0] for r in res])),
+            "true_relres_max": float(max(r[1] for r in res)), "all_converged": all(r[2] == 0 for r in res),
+            "forward_sweep_ms": kt["forward_sweep_ms"], "backward_sweep_ms": kt["backward_sweep_ms"]}
 
 
 def run_reference(args):

@@ -80,6 +80,22 @@ int acg_approxchol_ordered(int64_t n, const int64_t* colptr, const int64_t* rowv
  * 138-183) with compressAvgCol! (src/approxChol.jl:541-600). */
 int acg_approxchol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval, int64_t split,
                          int64_t merge, uint64_t rng_state[4], acg_factor** out);
+/* Opt-in, not the reference's elimination: a parallel approximate Cholesky
+ * elimination in rounds.  Each round takes an independent set of live
+ * vertices whose degree is a local minimum and at most max(2, the median live
+ * degree) (ties by pseudo-random priorities), and eliminates the set at once
+ * on `threads` host threads with
+ * the reference's per-vertex step (src/approxChol.jl:888-966: merge parallel
+ * edges, order by weight, sample and join neighbours).  Its random numbers are
+ * keyed by (seed, vertex, entry) rather than drawn from Julia's rand() stream,
+ * so the factor is a different sample than approxChol's (not bit-identical to
+ * the reference); it does not depend on `threads`.  The last vertices (at
+ * most 4,096, more when rounds find few vertices) are eliminated one at a
+ * time in order of degree; before them the factor's dependency DAG is at most
+ * `*rounds` levels deep.  Same LDLinv layout and the same requirements on `a`
+ * as acg_approxchol (a connected graph). */
+int acg_approxchol_parallel(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                            uint64_t seed, int threads, int64_t* rounds, acg_factor** out);
 /* n and F = length(ldli.fval). */
 int acg_factor_dims(const acg_factor* f, int64_t* n, int64_t* nnz);
 /* Copy out the LDLinv arrays in the reference layout (src/approxCholTypes.jl:73-79),

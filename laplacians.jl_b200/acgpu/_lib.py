@@ -76,6 +76,8 @@ SIGNATURES = [
                                                ctypes.POINTER(ctypes.c_void_p)]),
     ("acg_approxchol_split", ctypes.c_int, [ctypes.c_int64, i64p, i64p, f64p, ctypes.c_int64, ctypes.c_int64, u64p,
                                              ctypes.POINTER(ctypes.c_void_p)]),
+    ("acg_approxchol_parallel", ctypes.c_int, [ctypes.c_int64, i64p, i64p, f64p, ctypes.c_uint64, ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_void_p)]),
     ("acg_factor_dims", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     ("acg_factor_export", ctypes.c_int, [ctypes.c_void_p, i64p, i64p, i64p, f64p, f64p]),
     ("acg_factor_free", None, [ctypes.c_void_p]),

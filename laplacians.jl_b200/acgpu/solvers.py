@@ -33,7 +33,7 @@ from ._lib import AcgOptions, AcgSolveInfo, AcgStats, check, lib
 __all__ = [
     "ApproxCholParams", "LDLinv", "approxchol_lap", "approxchol_lap1", "lap", "seed", "rng_state",
     "set_rng_state", "approx_chol", "components", "vec_to_comps", "DeviceLapSolver", "GroupSolver", "null_solver",
-    "ServeLoop", "Ticket",
+    "ServeLoop", "Ticket", "approx_chol_parallel",
 ]
 
 _PRECISIONS = {"fp64": 0, "mixed": 1}
@@ -165,6 +165,25 @@ def approx_chol(a, params: ApproxCholParams | None = None) -> LDLinv:
         pp = None if p is None else p.ctypes.data_as(ctypes.c_void_p)
         check(L.acg_approxchol_ordered(n, cp, rv, np.ascontiguousarray(a.data), pp, _RNG, ctypes.byref(h)))
     return _take_factor(h)
+
+
+def approx_chol_parallel(a, seed: int = 1, threads: int | None = None) -> tuple[LDLinv, int]:
+    """Opt-in parallel elimination (acg_approxchol_parallel; not in the
+    reference): rounds of independent low-degree vertices eliminated at once on
+    `threads` host threads (default: all), each with the reference's
+    per-vertex step but its own keyed random numbers, so the factor is a
+    different sample than approx_chol's.  Returns (factor, rounds); the
+    factor's DAG is at most `rounds` levels deep."""
+    a = _csc(a)
+    n = a.shape[0]
+    if threads is None:
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    h = ctypes.c_void_p()
+    rounds = ctypes.c_int64()
+    check(lib().acg_approxchol_parallel(n, a.indptr.astype(np.int64) + 1, a.indices.astype(np.int64) + 1,
+                                        np.ascontiguousarray(a.data), int(seed) & ((1 << 64) - 1), int(threads),
+                                        ctypes.byref(rounds), ctypes.byref(h)))
+    return _take_factor(h), int(rounds.value)
 
 
 def _take_factor(h) -> LDLinv:
@@ -586,7 +605,11 @@ class _BlockSolver:
         x = np.zeros(b.shape)
         its = 0
         for ind, s in zip(self.comps, self.solvers):
-            x[ind] = s(b[ind])
+            if b.ndim == 1:
+                x[ind] = s(b[ind])
+            else:
+                for c in range(b.shape[1]):
+                    x[ind, c] = s(b[ind, c])
         if self.group is not None:
             cols = b.reshape(b.shape[0], -1)
             xcols = x.reshape(b.shape[0], -1)

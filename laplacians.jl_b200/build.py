@@ -25,7 +25,7 @@ HOST_OUT = PKG / "acgpu" / "libacghost.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CU_SOURCES = ["acg_solver.cu"]
-CPP_SOURCES = ["acg_rng.cpp", "acg_factor.cpp", "acg_host_api.cpp"]
+CPP_SOURCES = ["acg_rng.cpp", "acg_factor.cpp", "acg_factor_par.cpp", "acg_host_api.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

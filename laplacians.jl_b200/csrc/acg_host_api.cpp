@@ -130,6 +130,33 @@ int acg_approxchol_ordered(int64_t n, const int64_t* colptr, const int64_t* rowv
   return approxchol_entry("acg_approxchol_ordered", n, colptr, rowval, nzval, perm, 1, 1, 1, rng_state, out);
 }
 
+int acg_approxchol_parallel(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                            uint64_t seed, int threads, int64_t* rounds, acg_factor** out) {
+  if (!out || !colptr || !rowval || !nzval || n < 2) {
+    acg::set_last_error("acg_approxchol_parallel: bad arguments (need n >= 2 and non-null arrays)");
+    return ACG_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (colptr[0] != 0 && colptr[0] != 1) {
+    acg::set_last_error("acg_approxchol_parallel: colptr[0] must be 0 or 1");
+    return ACG_ERR_INVALID;
+  }
+  auto* fac = new acg_factor();
+  try {
+    acg::approx_chol_parallel(n, colptr, rowval, nzval, seed, threads, fac->f, rounds);
+  } catch (const std::bad_alloc&) {
+    delete fac;
+    acg::set_last_error("acg_approxchol_parallel: host out of memory");
+    return ACG_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    delete fac;
+    acg::set_last_error(std::string("acg_approxchol_parallel: ") + e.what());
+    return ACG_ERR_INVALID;
+  }
+  *out = fac;
+  return ACG_OK;
+}
+
 int acg_approxchol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval, int64_t split,
                          int64_t merge, uint64_t rng_state[4], acg_factor** out) {
   if (split < 1 || merge < 1 || split > 64) {

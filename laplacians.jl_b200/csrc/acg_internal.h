@@ -26,6 +26,11 @@ void approx_chol_ord(int64_t n, const int64_t* colptr, const int64_t* rowval, co
 void approx_chol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
                        int64_t split, int64_t merge, JuliaRng* rng, HostFactor& out);
 
+// Opt-in elimination in rounds of independent low-degree vertices on `threads`
+// host threads, with its own keyed random numbers; see acg_factor_par.cpp.
+void approx_chol_parallel(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
+                          uint64_t seed, int threads, HostFactor& out, int64_t* rounds);
+
 // Thread-local error text returned by acg_last_error().
 void set_last_error(const std::string& msg);
 

@@ -54,3 +54,28 @@ def test_approxchol_lap2(gpu_ok):
     f = acgpu.approxchol_lap2(a, tol=1e-8, precision="mixed")
     x = f(b)
     assert O.relres(a, x, b - b.mean()) <= 1e-8 * 1.01
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_parallel_factor_on_the_gpu(gpu_ok, precision):
+    """The opt-in parallel elimination's factor (acg_approxchol_parallel) is an
+    LDLinv like any other: the GPU solve with it agrees with the oracle's on
+    the same factor, and its DAG is shallower than the :deg factor's."""
+    a = G.grid3(24, weights="loguniform", seed=6)
+    f, rounds = acgpu.approx_chol_parallel(a, seed=3, threads=4)
+    acgpu.seed(3)
+    fdeg = acgpu.approx_chol(a)
+    dev = acgpu.DeviceLapSolver(a, f)
+    ddeg = acgpu.DeviceLapSolver(a, fdeg)
+    assert dev.stats()["levels"] < ddeg.stats()["levels"]
+    ddeg.close()
+    b = np.random.default_rng(4).standard_normal(a.shape[0])
+    its = [0]
+    x = dev(b, tol=1e-8, maxits=1000, pcgIts=its, precision=precision)
+    xo, ito, _, _ = O.OracleSolver(a, f)(b, tol=1e-8, maxits=1000)
+    if precision == "fp64":
+        assert abs(its[0] - ito) <= 1
+        assert np.linalg.norm(O.center(x) - O.center(xo)) <= 1e-7 * np.linalg.norm(O.center(xo))
+    else:
+        assert O.relres(a, x, b - b.mean()) <= 1e-8 * 1.01
+    dev.close()
