@@ -586,6 +586,33 @@ def run_grid3_64rhs(args):
     dev.close()
 
 
+def run_sweep_levels(args):
+    """The 64-column FP32 sweeps of the headline workload cut after a range of
+    levels (acg_time_sweep_levels): how the sweep time splits over the
+    dependency DAG's levels.  Not a bench line: one JSON object with the points
+    and the per-level cost between them."""
+    import acgpu
+    a, ldli, _ = build_workload()
+    dev = acgpu.DeviceLapSolver(a, ldli)
+    st = dev.stats()
+    swept = int(st["levels"] - st["dense_levels"])
+    pts = sorted({0, 1, 2, 5, 10, 20, 50, 100, 150, 200, 250, 300, 350, 400} | {max(swept - 1, 0)})
+    pts = [p for p in pts if p < swept]
+    rows = dev.time_sweep_levels(pts, nrhs=args.rhs, precision=args.precision, reps=5)
+    for i, r in enumerate(rows):
+        if i + 1 < len(rows):
+            nxt = rows[i + 1]
+            span = nxt["level"] - r["level"]
+            # forward: levels (L, L'] cost f(L') - f(L); backward: levels [L, L')
+            r["forward_us_per_level_next"] = 1e3 * (nxt["forward_ms"] - r["forward_ms"]) / span
+            r["backward_us_per_level_next"] = 1e3 * (r["backward_ms"] - nxt["backward_ms"]) / span
+    out = {"workload": f"grid3({GRID_SIDE}) log-uniform weights, {args.rhs} columns, {args.precision}",
+           "levels": int(st["levels"]), "swept_levels": swept, "dense_levels": int(st["dense_levels"]),
+           "points": rows}
+    print(json.dumps(out), flush=True)
+    dev.close()
+
+
 def run_many_graphs(args):
     """256 graphs in one launch: half 2D grids with side uniform in [32, 256],
     half random geometric graphs (n uniform in [1e3, 1e5], mean degree 8,
@@ -922,7 +949,8 @@ def main():
     ap.add_argument("--side", type=int, default=GRID_SIDE, help="grid side (100 = the benchmark workload)")
     ap.add_argument("--rhs", type=int, default=64, help="independent right-hand sides per step (batched)")
     ap.add_argument("--workload", default="grid3",
-                    choices=["grid3", "grid2_200", "matchings_2m", "grid3_64rhs", "many_graphs", "serving", "orderings"],
+                    choices=["grid3", "grid2_200", "matchings_2m", "grid3_64rhs", "many_graphs", "serving", "orderings",
+                             "sweep_levels"],
                     help="grid3 = the headline line; the others report the remaining workloads")
     ap.add_argument("--serving-graphs", type=int, default=16)
     ap.add_argument("--group-graphs", type=int, default=256)
@@ -941,7 +969,7 @@ def main():
         import torch
         torch.cuda.init()
         {"orderings": run_orderings, "grid2_200": run_grid2_200, "matchings_2m": run_matchings_2m, "grid3_64rhs": run_grid3_64rhs, "many_graphs": run_many_graphs,
-         "serving": run_serving}[args.workload](args)
+         "serving": run_serving, "sweep_levels": run_sweep_levels}[args.workload](args)
 
 
 if __name__ == "__main__":

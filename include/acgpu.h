@@ -301,6 +301,17 @@ int acg_time_kernels(acg_solver* h, int precision, int reps, acg_kernel_times* o
  * (iteration_ms is not measured there). */
 int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg_kernel_times* out);
 
+/* The batched sweeps cut at given levels of the factor's dependency DAG.  For
+ * each levels[i] = L: fwd_ms[i] is the forward sweep over the tasks of levels
+ * 0..L and bwd_ms[i] the backward sweep over the tasks of levels >= L (the
+ * swept head; the dense tail's levels are never swept), each per launch with
+ * nrhs right-hand sides; fwd_tasks[i] / bwd_tasks[i] are those tasks.  Levels
+ * are clamped to [0, levels - 1].  The differences between points show what
+ * each range of levels costs.  Diagnostic only: it uses the batch buffers, so a
+ * solver that serves answers ACG_ERR_BUSY; a group solver ACG_ERR_INVALID. */
+int acg_time_sweep_levels(acg_solver* h, int precision, int nrhs, int reps, int npts, const int* levels,
+                          double* fwd_ms, double* bwd_ms, int* fwd_tasks, int* bwd_tasks);
+
 /* ---- serving loop: continuous batching on the device -------------------- */
 /* The reference has no server: its closure solves one vector per call
  * (src/approxChol.jl:1624).  A serving loop turns a one-graph solver's batched

@@ -43,7 +43,7 @@ class AdmissionError(RuntimeError):
     """A graph whose solver alone exceeds the server's HBM budget."""
 
 
-@dataclass
+@dataclass(eq=False)  # compared by identity: the fields hold numpy arrays
 class Request:
     gid: object
     B: np.ndarray          # n x k right-hand sides (k >= 1)
@@ -297,8 +297,11 @@ class SolveServer:
     def __exit__(self, *exc):
         self.close()
 
+    def _nothing_queued(self):
+        return not any(e.queue or e.loading for e in self._graphs.values())
+
     def _idle(self):
-        return not any(e.queue or e.loading for e in self._graphs.values()) and not self._pending
+        return self._nothing_queued() and not self._pending
 
     def _dispatch(self):
         """Hand queued requests to their graphs' loops, uploading graphs as needed."""
@@ -306,7 +309,8 @@ class SolveServer:
             load = None
             with self._cv:
                 while True:
-                    if self._stop and self._idle():
+                    # in-flight solves are the completer's: it alone waits for them
+                    if self._stop and self._nothing_queued():
                         return
                     ready = [e for e in self._graphs.values() if e.queue and e.loop is not None]
                     waiting = [e for e in self._graphs.values() if e.queue and e.solver is None and not e.loading]
@@ -350,7 +354,13 @@ class SolveServer:
                         return
                     self._cv.wait(timeout=0.05)
                 pending = list(self._pending)
-            finished = [r for r in pending if r.ticket.done()]
+            finished = []
+            for r in pending:
+                try:
+                    if r.ticket.done():
+                        finished.append(r)
+                except Exception:  # noqa: BLE001 - a failed loop: wait() below raises it to the caller
+                    finished.append(r)
             if not finished:
                 time.sleep(5e-5)
                 continue

@@ -348,6 +348,22 @@ class DeviceLapSolver:
         check(lib().acg_time_kernels_batch(self._h, _PRECISIONS[precision], int(nrhs), int(reps), ctypes.byref(t)))
         return {k: getattr(t, k) for k, _ in _lib.AcgKernelTimes._fields_}
 
+    def time_sweep_levels(self, levels, nrhs=64, precision="mixed", reps=5) -> list:
+        """The batched sweeps cut at each level L of `levels`: the forward sweep
+        over levels 0..L and the backward sweep over levels >= L, per launch
+        (ms), with the tasks each covers.  Diagnostic (acg_time_sweep_levels)."""
+        lv = np.ascontiguousarray(levels, dtype=np.int32)
+        m = lv.size
+        f = np.zeros(m)
+        b = np.zeros(m)
+        tf = np.zeros(m, np.int32)
+        tb = np.zeros(m, np.int32)
+        ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        check(lib().acg_time_sweep_levels(self._h, _PRECISIONS[precision], int(nrhs), int(reps), m, ptr(lv), ptr(f),
+                                          ptr(b), ptr(tf), ptr(tb)))
+        return [{"level": int(lv[i]), "forward_tasks": int(tf[i]), "forward_ms": float(f[i]),
+                 "backward_tasks": int(tb[i]), "backward_ms": float(b[i])} for i in range(m)]
+
     def lap_mul(self, x, precision="fp64"):
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty_like(x)

@@ -33,6 +33,7 @@ struct BatchShared {
   int k;            // right-hand sides in this launch (the rest of kp is padding)
   int l1_due;       // kb_yzr deferred the third L1 test of some column to kb_pupdate_z
   unsigned int counter[16];
+  unsigned int gcounter[16][kRedGroups];  // per-group tickets of the two-level reductions
 };
 
 // ---- vector relaxed loads/stores of CPL consecutive values -----------------
@@ -494,6 +495,142 @@ __device__ __forceinline__ bool batch_reduce(double (&v)[NV], int kp, double* pa
   return true;
 }
 
+// Thread (c, part) of a block sums column c of NV tables over rows [r0, r1)
+// (src[q * qstride + row * kp + c]), each table's rows in ascending order, with
+// up to 8 loads in flight across the tables.
+template <int NV>
+__device__ __forceinline__ void sum_rows(const double* src, size_t qstride, int kp, int c, int r0, int r1,
+                                         double (&s)[NV]) {
+#pragma unroll
+  for (int q = 0; q < NV; ++q) s[q] = 0.0;
+  const int nr = r1 - r0, m = NV * nr;
+  for (int j0 = 0; j0 < m; j0 += 8) {
+    double l[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int j = j0 + u;
+      l[u] = j < m ? __ldcg(src + (size_t)(j / nr) * qstride + (size_t)(r0 + j % nr) * kp + c) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int j = j0 + u;
+#pragma unroll
+      for (int q = 0; q < NV; ++q)
+        if (j < m && j / nr == q) s[q] += l[u];
+    }
+  }
+}
+
+// Sums, per column, the rows [0, rows) of NV tables of kp columns into `out`
+// of the threads below kp: the block's threads split the rows into
+// blockDim / kp contiguous parts, and the parts are added in order.
+template <int NV>
+__device__ __forceinline__ void block_sum_rows(const double* src, size_t qstride, int kp, int rows,
+                                               double (&sm)[NV][kVecThreads * 4], double (&out)[NV]) {
+  const int per = (int)blockDim.x / kp;
+  const int c = threadIdx.x % kp, part = threadIdx.x / kp;
+  double s[NV];
+  sum_rows<NV>(src, qstride, kp, c, (int)((long long)rows * part / per), (int)((long long)rows * (part + 1) / per), s);
+#pragma unroll
+  for (int q = 0; q < NV; ++q) sm[q][threadIdx.x] = s[q];
+  __syncthreads();
+  if ((int)threadIdx.x < kp) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double t = 0.0;
+      for (int j = 0; j < per; ++j) t += sm[q][threadIdx.x + j * kp];
+      out[q] = t;
+    }
+  }
+}
+
+// The same reduction when each thread holds VPT consecutive columns
+// (v[q][j] for column (VPT * threadIdx.x + j) mod kp; blockDim * VPT and the
+// grid stride are multiples of kp), in two levels: the block's values are laid
+// out as VPT * blockDim virtual threads in shared memory and summed per column
+// into one row of partials per block; the last block to finish in each of up
+// to kRedGroups contiguous groups of blocks sums its group's rows into a group
+// row, and the last group to finish sums the group rows.  One block alone
+// would read every block's row (592 x NV x kp values) with a few loads in
+// flight per thread, tens of dependent L2 round trips; two levels take a
+// handful.  The order of every sum is fixed by the grid, so results repeat
+// bit for bit.  Threads below kp of the returning block get the totals of
+// column threadIdx.x in out.  partials holds NV * (gridDim + kRedGroups) * kp
+// values.
+template <int NV, int VPT>
+__device__ __forceinline__ bool batch_reduce_v(double (&v)[NV][VPT], int kp, double* partials, BatchShared* bs,
+                                               int ci, double (&out)[NV]) {
+  static_assert(VPT <= 4, "shared tile holds 4 values per thread");
+  __shared__ double sm[NV][kVecThreads * 4];
+  __shared__ bool am_last;
+#pragma unroll
+  for (int q = 0; q < NV; ++q)
+#pragma unroll
+    for (int j = 0; j < VPT; ++j) sm[q][threadIdx.x * VPT + j] = v[q][j];
+  __syncthreads();
+  const int G = gridDim.x;
+  const int gs = (G + kRedGroups - 1) / kRedGroups;  // blocks per group
+  const int NG = (G + gs - 1) / gs;                   // groups
+  const int g = blockIdx.x / gs, gb0 = g * gs, gb1 = min(G, gb0 + gs);
+  double* grows = partials + (size_t)NV * G * kp;     // group rows: [q][NG][kp]
+  const int per_v = (int)blockDim.x * VPT / kp;
+  if ((int)threadIdx.x < kp) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double s = 0.0;
+      for (int j = 0; j < per_v; ++j) s += sm[q][threadIdx.x + j * kp];
+      partials[((size_t)q * G + blockIdx.x) * kp + threadIdx.x] = s;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    am_last = atomicAdd(&bs->gcounter[ci][g], 1u) == (unsigned)(gb1 - gb0 - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  // the group's last block: its rows into the group row
+  {
+    double t[NV];
+    block_sum_rows<NV>(partials + (size_t)gb0 * kp, (size_t)G * kp, kp, gb1 - gb0, sm, t);
+    if ((int)threadIdx.x < kp) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q) grows[((size_t)q * NG + g) * kp + threadIdx.x] = t[q];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bs->gcounter[ci][g] = 0u;
+    __threadfence();
+    am_last = atomicAdd(&bs->counter[ci], 1u) == (unsigned)(NG - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  block_sum_rows<NV>(grows, (size_t)NG * kp, kp, NG, sm, out);
+  if (threadIdx.x == 0) bs->counter[ci] = 0u;
+  return true;
+}
+
+// 16-byte vectors of the loop-body kernels: 4 FP32 or 2 FP64 columns.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  static constexpr int W = 4;
+  using V = float4;
+  __device__ static void split(const V& x, float (&o)[4]) { o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = x.w; }
+  __device__ static V join(const float (&o)[4]) { return make_float4(o[0], o[1], o[2], o[3]); }
+};
+template <>
+struct Vec16<double> {
+  static constexpr int W = 2;
+  using V = double2;
+  __device__ static void split(const V& x, double (&o)[2]) { o[0] = x.x; o[1] = x.y; }
+  __device__ static V join(const double (&o)[2]) { return make_double2(o[0], o[1]); }
+};
+
 // After the per-column scalar steps: end the launch's loop when all columns stopped.
 __device__ __forceinline__ void batch_check_all(PcgState* st, BatchShared* bs, int kp, const LoopCtl& ctl) {
   __syncthreads();
@@ -513,93 +650,157 @@ __device__ __forceinline__ void batch_check_all(PcgState* st, BatchShared* bs, i
 // still run in element order.
 constexpr int kBU = 4;
 
+// The loop-body kernels (kb_pq, kb_update, kb_yzr, kb_pupdate_z) move 16
+// bytes per access: thread t owns the W = 16 / sizeof(T) consecutive columns
+// starting at (W * t) mod kp, walks the block in W-wide vectors with a grid
+// stride that is a multiple of kp, and keeps kBU vectors of every operand in
+// flight.  With 4-byte accesses the same kernels moved 2.7-5.3 TB/s on the 1M
+// grid at 64 columns.
+
 // pq, |p|_1, |q|_1 per column -> alpha, stagnation tests 1 and 2
 template <typename T>
-__global__ void __launch_bounds__(kBVecThreads) kb_pq(int n, int kp, const T* __restrict__ p, const T* __restrict__ q,
-                                                      PcgState* st, BatchShared* bs, double* partials, double eps,
-                                                      LoopCtl ctl) {
+__global__ void __launch_bounds__(kVecThreads) kb_pq(int n, int kp, const T* __restrict__ p, const T* __restrict__ q,
+                                                     PcgState* st, BatchShared* bs, double* partials, double eps,
+                                                     LoopCtl ctl) {
   if (bs->all_done) return;
-  const size_t N = (size_t)n * kp;
+  using VT = Vec16<T>;
+  constexpr int W = VT::W;
+  using V = typename VT::V;
+  const size_t NW = (size_t)n * kp / W;
   const size_t S = (size_t)gridDim.x * blockDim.x;
   size_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  double acc[3] = {0.0, 0.0, 0.0};
-  for (; i + (kBU - 1) * S < N; i += kBU * S) {
-    T pv[kBU], qv[kBU];
+  const V* pv4 = reinterpret_cast<const V*>(p);
+  const V* qv4 = reinterpret_cast<const V*>(q);
+  double acc[3][W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) acc[0][j] = acc[1][j] = acc[2][j] = 0.0;
+  for (; i + (kBU - 1) * S < NW; i += kBU * S) {
+    V pv[kBU], qv[kBU];
 #pragma unroll
     for (int u = 0; u < kBU; ++u) {
-      pv[u] = p[i + u * S];
-      qv[u] = q[i + u * S];
+      pv[u] = pv4[i + u * S];
+      qv[u] = qv4[i + u * S];
     }
 #pragma unroll
     for (int u = 0; u < kBU; ++u) {
-      acc[0] += (double)pv[u] * (double)qv[u];
-      acc[1] += fabs((double)pv[u]);
-      acc[2] += fabs((double)qv[u]);
+      T a[W], b[W];
+      VT::split(pv[u], a);
+      VT::split(qv[u], b);
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        acc[0][j] += (double)a[j] * (double)b[j];
+        acc[1][j] += fabs((double)a[j]);
+        acc[2][j] += fabs((double)b[j]);
+      }
     }
   }
-  for (; i < N; i += S) {
-    const double pv = (double)p[i], qv = (double)q[i];
-    acc[0] += pv * qv;
-    acc[1] += fabs(pv);
-    acc[2] += fabs(qv);
+  for (; i < NW; i += S) {
+    T a[W], b[W];
+    VT::split(pv4[i], a);
+    VT::split(qv4[i], b);
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+      acc[0][j] += (double)a[j] * (double)b[j];
+      acc[1][j] += fabs((double)a[j]);
+      acc[2][j] += fabs((double)b[j]);
+    }
   }
   double tot[3];
-  if (batch_reduce<3>(acc, kp, partials, &bs->counter[0], tot)) {
+  if (batch_reduce_v<3, W>(acc, kp, partials, bs, 0, tot)) {
     const int c = threadIdx.x;
     if (c < kp && !st[c].done) pcg_scalar_pq(&st[c], tot[0], tot[1], tot[2], eps);
     batch_check_all(st, bs, kp, ctl);
   }
 }
 
+// The update holds three vectors and a column of x per step: two steps in
+// flight keep it within the registers of three blocks per SM.
+constexpr int kBUx = 2;
+
 // x' = x + alpha p, r -= alpha q (active columns); |r|^2, |x'|_1, |r|_1.  The
-// sweeps' vectors s and y are marked pending by the sweeps themselves.
+// sweeps' vectors s and y are marked pending by the sweeps themselves.  Each
+// column keeps its x in its own one of three buffers, so x moves one value at
+// a time; a vector whose columns have all stopped is skipped.
 template <typename T>
-__global__ void __launch_bounds__(kBVecThreads) kb_update(int n, int kp, T* x3, const T* __restrict__ p,
-                                                          const T* __restrict__ q, T* __restrict__ r, PcgState* st,
-                                                          BatchShared* bs, double* partials, LoopCtl ctl) {
+__global__ void __launch_bounds__(kVecThreads) kb_update(int n, int kp, T* x3, const T* __restrict__ p,
+                                                         const T* __restrict__ q, T* __restrict__ r, PcgState* st,
+                                                         BatchShared* bs, double* partials, LoopCtl ctl) {
   if (bs->all_done) return;
+  using VT = Vec16<T>;
+  constexpr int W = VT::W;
+  using V = typename VT::V;
   const size_t N = (size_t)n * kp;
+  const size_t NW = N / W;
   const size_t S = (size_t)gridDim.x * blockDim.x;
   const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = (int)(i0 % kp);
-  const bool act = !st[c].done;
-  const double al = st[c].alpha;
-  const T* xc = x3 + (size_t)st[c].xcur * N;
-  T* xn = x3 + (size_t)st[c].xnext * N;
-  double acc[3] = {0.0, 0.0, 0.0};
-  size_t i = i0;
-  if (!act) i = N;  // a stopped column keeps its vectors
-  for (; i + (kBU - 1) * S < N; i += kBU * S) {
-    T xv[kBU], pv[kBU], qv[kBU], rv[kBU];
+  const int c0 = (int)((i0 * W) % kp);
+  double al[W];
+  const T* xc[W];
+  T* xn[W];
+  bool any = false;
 #pragma unroll
-    for (int u = 0; u < kBU; ++u) {
-      xv[u] = xc[i + u * S];
-      pv[u] = p[i + u * S];
-      qv[u] = q[i + u * S];
-      rv[u] = r[i + u * S];
+  for (int j = 0; j < W; ++j) {
+    const PcgState* sc = &st[c0 + j];
+    const bool act = !sc->done;
+    any |= act;
+    al[j] = act ? sc->alpha : 0.0;  // a stopped column keeps its vectors
+    xc[j] = x3 + (size_t)sc->xcur * N;
+    xn[j] = x3 + (size_t)sc->xnext * N;
+  }
+  const V* pv4 = reinterpret_cast<const V*>(p);
+  const V* qv4 = reinterpret_cast<const V*>(q);
+  V* rv4 = reinterpret_cast<V*>(r);
+  double acc[3][W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) acc[0][j] = acc[1][j] = acc[2][j] = 0.0;
+  size_t i = any ? i0 : NW;
+  for (; i + (kBUx - 1) * S < NW; i += kBUx * S) {
+    V pv[kBUx], qv[kBUx], rv[kBUx];
+    T xv[kBUx][W];
+#pragma unroll
+    for (int u = 0; u < kBUx; ++u) {
+      pv[u] = pv4[i + u * S];
+      qv[u] = qv4[i + u * S];
+      rv[u] = rv4[i + u * S];
+#pragma unroll
+      for (int j = 0; j < W; ++j) xv[u][j] = xc[j][(i + u * S) * W + j];
     }
 #pragma unroll
-    for (int u = 0; u < kBU; ++u) {
-      const T xw = (T)((double)xv[u] + al * (double)pv[u]);
-      const T rw = (T)((double)rv[u] + (-al) * (double)qv[u]);
-      xn[i + u * S] = xw;
-      r[i + u * S] = rw;
-      acc[0] += (double)rw * (double)rw;
-      acc[1] += fabs((double)xw);
-      acc[2] += fabs((double)rw);
+    for (int u = 0; u < kBUx; ++u) {
+      T a[W], b[W], rr[W], rw[W];
+      VT::split(pv[u], a);
+      VT::split(qv[u], b);
+      VT::split(rv[u], rr);
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        const T xw = (T)((double)xv[u][j] + al[j] * (double)a[j]);
+        rw[j] = (T)((double)rr[j] + (-al[j]) * (double)b[j]);
+        xn[j][(i + u * S) * W + j] = xw;
+        acc[0][j] += (double)rw[j] * (double)rw[j];
+        acc[1][j] += fabs((double)xw);
+        acc[2][j] += fabs((double)rw[j]);
+      }
+      rv4[i + u * S] = VT::join(rw);
     }
   }
-  for (; i < N; i += S) {
-    const T xv = (T)((double)xc[i] + al * (double)p[i]);
-    const T rv = (T)((double)r[i] + (-al) * (double)q[i]);
-    xn[i] = xv;
-    r[i] = rv;
-    acc[0] += (double)rv * (double)rv;
-    acc[1] += fabs((double)xv);
-    acc[2] += fabs((double)rv);
+  for (; i < NW; i += S) {
+    T a[W], b[W], rr[W], rw[W];
+    VT::split(pv4[i], a);
+    VT::split(qv4[i], b);
+    VT::split(rv4[i], rr);
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+      const T xw = (T)((double)xc[j][i * W + j] + al[j] * (double)a[j]);
+      rw[j] = (T)((double)rr[j] + (-al[j]) * (double)b[j]);
+      xn[j][i * W + j] = xw;
+      acc[0][j] += (double)rw[j] * (double)rw[j];
+      acc[1][j] += fabs((double)xw);
+      acc[2][j] += fabs((double)rw[j]);
+    }
+    rv4[i] = VT::join(rw);
   }
   double tot[3];
-  if (batch_reduce<3>(acc, kp, partials, &bs->counter[1], tot)) {
+  if (batch_reduce_v<3, W>(acc, kp, partials, bs, 1, tot)) {
     const int cc = threadIdx.x;
     if (cc < kp && !st[cc].done) pcg_scalar_update(&st[cc], tot[0], tot[1], tot[2]);
     batch_check_all(st, bs, kp, ctl);
@@ -614,12 +815,12 @@ __global__ void __launch_bounds__(kBVecThreads) kb_ysum(int n, int kp, const T* 
   const size_t S = (size_t)gridDim.x * blockDim.x;
   size_t i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0.0};
-  for (; i + (kBU - 1) * S < N; i += kBU * S) {
-    T yv[kBU];
+  for (; i + (kBUx - 1) * S < N; i += kBUx * S) {
+    T yv[kBUx];
 #pragma unroll
-    for (int u = 0; u < kBU; ++u) yv[u] = y[i + u * S];
+    for (int u = 0; u < kBUx; ++u) yv[u] = y[i + u * S];
 #pragma unroll
-    for (int u = 0; u < kBU; ++u) acc[0] += (double)yv[u];
+    for (int u = 0; u < kBUx; ++u) acc[0] += (double)yv[u];
   }
   for (; i < N; i += S) acc[0] += (double)y[i];
   double tot[1];
@@ -647,15 +848,15 @@ __global__ void __launch_bounds__(kBVecThreads) kb_zdot(int n, int kp, T* __rest
   const double mu = st[c].mean;
   double acc[2] = {0.0, 0.0};
   size_t i = i0;
-  for (; i + (kBU - 1) * S < N; i += kBU * S) {
-    T yv[kBU], rv[kBU];
+  for (; i + (kBUx - 1) * S < N; i += kBUx * S) {
+    T yv[kBUx], rv[kBUx];
 #pragma unroll
-    for (int u = 0; u < kBU; ++u) {
+    for (int u = 0; u < kBUx; ++u) {
       yv[u] = yz[i + u * S];
       rv[u] = r[i + u * S];
     }
 #pragma unroll
-    for (int u = 0; u < kBU; ++u) {
+    for (int u = 0; u < kBUx; ++u) {
       const T z = (T)((double)yv[u] - mu);
       yz[i + u * S] = z;
       if (init) p[i + u * S] = z;
@@ -688,35 +889,54 @@ __global__ void __launch_bounds__(kBVecThreads) kb_zdot(int n, int kp, T* __rest
 // sums |z|_1 on the way.  p of a column stopped by those tests is updated
 // once more, which nothing reads: x comes from bestx.
 template <typename T>
-__global__ void __launch_bounds__(kBVecThreads) kb_yzr(int n, int kp, const T* __restrict__ y, const T* __restrict__ r,
-                                                       PcgState* st, BatchShared* bs, double* partials, double eps,
-                                                       LoopCtl ctl) {
+__global__ void __launch_bounds__(kVecThreads) kb_yzr(int n, int kp, const T* __restrict__ y, const T* __restrict__ r,
+                                                      PcgState* st, BatchShared* bs, double* partials, double eps,
+                                                      LoopCtl ctl) {
   if (bs->all_done) return;
-  const size_t N = (size_t)n * kp;
+  using VT = Vec16<T>;
+  constexpr int W = VT::W;
+  using V = typename VT::V;
+  const size_t NW = (size_t)n * kp / W;
   const size_t S = (size_t)gridDim.x * blockDim.x;
   size_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  double acc[3] = {0.0, 0.0, 0.0};
-  for (; i + (kBU - 1) * S < N; i += kBU * S) {
-    T yv[kBU], rv[kBU];
+  const V* yv4 = reinterpret_cast<const V*>(y);
+  const V* rv4 = reinterpret_cast<const V*>(r);
+  double acc[3][W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) acc[0][j] = acc[1][j] = acc[2][j] = 0.0;
+  for (; i + (kBU - 1) * S < NW; i += kBU * S) {
+    V yv[kBU], rv[kBU];
 #pragma unroll
     for (int u = 0; u < kBU; ++u) {
-      yv[u] = y[i + u * S];
-      rv[u] = r[i + u * S];
+      yv[u] = yv4[i + u * S];
+      rv[u] = rv4[i + u * S];
     }
 #pragma unroll
     for (int u = 0; u < kBU; ++u) {
-      acc[0] += (double)yv[u];
-      acc[1] += (double)yv[u] * (double)rv[u];
-      acc[2] += (double)rv[u];
+      T a[W], b[W];
+      VT::split(yv[u], a);
+      VT::split(rv[u], b);
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        acc[0][j] += (double)a[j];
+        acc[1][j] += (double)a[j] * (double)b[j];
+        acc[2][j] += (double)b[j];
+      }
     }
   }
-  for (; i < N; i += S) {
-    acc[0] += (double)y[i];
-    acc[1] += (double)y[i] * (double)r[i];
-    acc[2] += (double)r[i];
+  for (; i < NW; i += S) {
+    T a[W], b[W];
+    VT::split(yv4[i], a);
+    VT::split(rv4[i], b);
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+      acc[0][j] += (double)a[j];
+      acc[1][j] += (double)a[j] * (double)b[j];
+      acc[2][j] += (double)b[j];
+    }
   }
   double tot[3];
-  if (batch_reduce<3>(acc, kp, partials, &bs->counter[8], tot)) {
+  if (batch_reduce_v<3, W>(acc, kp, partials, bs, 8, tot)) {
     const int c = threadIdx.x;
     bool deferred = false;
     if (c < kp) {
@@ -739,43 +959,71 @@ __global__ void __launch_bounds__(kBVecThreads) kb_yzr(int n, int kp, const T* _
 }
 
 // z = y - mean, p = z + beta p (columns still running); on the iterations
-// kb_yzr deferred, also |z|_1 and the deferred tests.
+// kb_yzr deferred, also |z|_1 and the deferred tests.  A vector whose columns
+// have all stopped is skipped.
 template <typename T>
-__global__ void __launch_bounds__(kBVecThreads) kb_pupdate_z(int n, int kp, const T* __restrict__ y, T* __restrict__ p,
-                                                             PcgState* st, BatchShared* bs, double* partials,
-                                                             double eps, LoopCtl ctl) {
+__global__ void __launch_bounds__(kVecThreads) kb_pupdate_z(int n, int kp, const T* __restrict__ y, T* __restrict__ p,
+                                                            PcgState* st, BatchShared* bs, double* partials,
+                                                            double eps, LoopCtl ctl) {
   if (bs->all_done) return;
   const bool l1 = bs->l1_due != 0;  // the same for every thread of the launch
-  const size_t N = (size_t)n * kp;
+  using VT = Vec16<T>;
+  constexpr int W = VT::W;
+  using V = typename VT::V;
+  const size_t NW = (size_t)n * kp / W;
   const size_t S = (size_t)gridDim.x * blockDim.x;
   const size_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = (int)(i0 % kp);
-  const double mu = st[c].mean;
-  const double beta = st[c].beta;
-  double acc[1] = {0.0};
-  size_t i = st[c].done ? N : i0;
-  for (; i + (kBU - 1) * S < N; i += kBU * S) {
-    T yv[kBU], pv[kBU];
+  const int c0 = (int)((i0 * W) % kp);
+  double mu[W], beta[W];
+  bool any = false;
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    mu[j] = st[c0 + j].mean;
+    beta[j] = st[c0 + j].beta;
+    any |= !st[c0 + j].done;
+  }
+  const V* yv4 = reinterpret_cast<const V*>(y);
+  V* pv4 = reinterpret_cast<V*>(p);
+  double acc[1][W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) acc[0][j] = 0.0;
+  size_t i = any ? i0 : NW;
+  for (; i + (kBU - 1) * S < NW; i += kBU * S) {
+    V yv[kBU], pv[kBU];
 #pragma unroll
     for (int u = 0; u < kBU; ++u) {
-      yv[u] = y[i + u * S];
-      pv[u] = p[i + u * S];
+      yv[u] = yv4[i + u * S];
+      pv[u] = pv4[i + u * S];
     }
 #pragma unroll
     for (int u = 0; u < kBU; ++u) {
-      const T z = (T)((double)yv[u] - mu);
-      p[i + u * S] = (T)((double)z + beta * (double)pv[u]);
-      acc[0] += fabs((double)z);
+      T a[W], b[W], o[W];
+      VT::split(yv[u], a);
+      VT::split(pv[u], b);
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        const T z = (T)((double)a[j] - mu[j]);
+        o[j] = (T)((double)z + beta[j] * (double)b[j]);
+        acc[0][j] += fabs((double)z);
+      }
+      pv4[i + u * S] = VT::join(o);
     }
   }
-  for (; i < N; i += S) {
-    const T z = (T)((double)y[i] - mu);
-    p[i] = (T)((double)z + beta * (double)p[i]);
-    acc[0] += fabs((double)z);
+  for (; i < NW; i += S) {
+    T a[W], b[W], o[W];
+    VT::split(yv4[i], a);
+    VT::split(pv4[i], b);
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
+      const T z = (T)((double)a[j] - mu[j]);
+      o[j] = (T)((double)z + beta[j] * (double)b[j]);
+      acc[0][j] += fabs((double)z);
+    }
+    pv4[i] = VT::join(o);
   }
   if (!l1) return;
   double tot[1];
-  if (batch_reduce<1>(acc, kp, partials, &bs->counter[9], tot)) {
+  if (batch_reduce_v<1, W>(acc, kp, partials, bs, 9, tot)) {
     const int cc = threadIdx.x;
     if (cc < kp && !st[cc].done && st[cc].itcnt > 0 && st[cc].itcnt % 10 == 0) {
       st[cc].sum_abs_z = tot[0];

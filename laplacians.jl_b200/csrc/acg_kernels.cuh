@@ -27,6 +27,7 @@ namespace acg {
 
 constexpr int kMaxPartialBlocks = 2048;
 constexpr int kVecBlocks = 148 * 4;   // grid of the streaming vector kernels
+constexpr int kRedGroups = 24;        // block groups of the two-level batched reductions
 constexpr int kVecThreads = 256;
 constexpr double kEps64 = 2.220446049250313e-16;
 

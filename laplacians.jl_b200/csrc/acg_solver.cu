@@ -151,6 +151,7 @@ struct SolverImpl {
   BatchShared* bsh = nullptr;
   PcgState* h_bst = nullptr;
   int bsweep_blocks[2][4] = {};          // [precision][log2(kp/8)]
+  int bvec_blocks[2][4] = {};            // [precision][pq, update, yzr, pupdate]: one resident wave
   int bspmv_blocks[2][4] = {};           // batched mat-vec grid: every resident block
   int batch_bps = 0;                     // batched sweep blocks per SM (0 = occupancy limit)
   // dense tail: vertices [dt_v0, n) (levels >= dt_L0) handled by s_T = M w_T,
@@ -165,6 +166,9 @@ struct SolverImpl {
   size_t dt_part_cols = 0;               // columns dt_part holds
   int ntasks_bb = 0, ntasks_fb = 0;      // task tables of the batched sweeps
   DevBuf<SweepTask> tasks_bb, tasks_fb;
+  // per level l: the forward table's tasks of levels <= l, and the backward
+  // table's tasks of levels >= l (the backward table walks levels downwards)
+  std::vector<int> tfb_upto, tbb_from;
   cudaGraphExec_t bexec[2][2][4] = {};  // [slot][precision][log2(kp/8)]
 
   // asynchronous batched solves (acg_solve_async): two slots, each with its
@@ -1042,10 +1046,16 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
       const int bheavy = (opts && opts->batch_bwd_heavy > 0) ? opts->batch_bwd_heavy : 8;
       const int fheavy = (opts && opts->batch_fwd_heavy > 0) ? opts->batch_fwd_heavy : 8;
       std::vector<SweepTask> tbb, tfb;
-      for (int l = blev - 1; l >= 0; --l)
+      S.tbb_from.assign(nlev, 0);
+      S.tfb_upto.assign(nlev, 0);
+      for (int l = blev - 1; l >= 0; --l) {
         for (const auto& r : runs[l]) emit_level(tbb, r.first, r.second, outdeg, bptr, bheavy);
-      for (int l = 0; l < nlev; ++l)
+        S.tbb_from[l] = (int)tbb.size();
+      }
+      for (int l = 0; l < nlev; ++l) {
         for (const auto& r : runs[l]) emit_level(tfb, r.first, r.second, fdeg, fptr, fheavy);
+        S.tfb_upto[l] = (int)tfb.size();
+      }
       // Testing only: blank one forward task record (it stores nothing), so
       // the values of its vertices are never produced and the waits on them
       // run out after spin_limit polls; the solve then reports
@@ -1435,7 +1445,7 @@ void with_cpl(int kp, F&& f) {
 }
 
 template <typename T, int CPL, bool kForward>
-void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, T* sfwd, T* out, T* mark) {
+void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, T* sfwd, T* out, T* mark, int ntasks = -1) {
   const TypedArrays<T> A = arrays_of<T>(S);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(S.bsweep_blocks[plan_index<T>()][kp_index(CPL * kBatchLanes)]);
@@ -1446,7 +1456,8 @@ void enqueue_bsweep(cudaStream_t s, const SolverImpl& S, const T* aux, T* sfwd, 
   at[0].val.cooperative = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  ACG_CUDA(cudaLaunchKernelEx(&cfg, kb_sweep<T, CPL, kForward>, kForward ? S.ntasks_fb : S.ntasks_bb,
+  if (ntasks < 0) ntasks = kForward ? S.ntasks_fb : S.ntasks_bb;
+  ACG_CUDA(cudaLaunchKernelEx(&cfg, kb_sweep<T, CPL, kForward>, ntasks,
                               (const SweepTask*)(kForward ? S.tasks_fb.p : S.tasks_bb.p), kForward ? A.fi : A.bi,
                               kForward ? A.fc : A.bc, aux, (const T*)sfwd, out, mark, S.bsh, S.spin_limit));
 }
@@ -1478,11 +1489,12 @@ void enqueue_biteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* y, 
   const TypedArrays<T> A = arrays_of<T>(S);
   const int n = S.n;
   kb_spmv<T, CPL><<<S.bspmv_blocks[plan_index<T>()][kp_index(kp)], kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, p, q, S.bsh);
-  kb_pq<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, ctl);
-  kb_update<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, ctl);
+  const int* vg = S.bvec_blocks[plan_index<T>()];
+  kb_pq<T><<<vg[0], kVecThreads, 0, s>>>(n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, ctl);
+  kb_update<T><<<vg[1], kVecThreads, 0, s>>>(n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, ctl);
   enqueue_bsweeps<T, CPL>(s, S, r, sv, y);
-  kb_yzr<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, y, r, S.bst, S.bsh, S.bpartials.p, eps, ctl);
-  kb_pupdate_z<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(n, kp, y, p, S.bst, S.bsh, S.bpartials.p, eps, ctl);
+  kb_yzr<T><<<vg[2], kVecThreads, 0, s>>>(n, kp, y, r, S.bst, S.bsh, S.bpartials.p, eps, ctl);
+  kb_pupdate_z<T><<<vg[3], kVecThreads, 0, s>>>(n, kp, y, p, S.bst, S.bsh, S.bpartials.p, eps, ctl);
 }
 
 template <int CPL>
@@ -1595,13 +1607,32 @@ int spmv_occupancy(int sms) {
   return sms * std::max(1, a);
 }
 
+// Grid of a loop-body vector kernel: every block resident at once, so its
+// grid-stride walk ends in one wave (a fixed 592-block grid of a kernel with 3
+// resident blocks per SM left a second wave of 148 blocks), and at most
+// kVecBlocks, the blocks whose partials the reductions hold.
+template <class K>
+int vec_occupancy(K kernel, int sms) {
+  int a = 0;
+  ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kernel, kVecThreads, 0));
+  return std::min(kVecBlocks, sms * std::max(1, a));
+}
+
+template <typename T>
+void vec_grids(int sms, int (&out)[4]) {
+  out[0] = vec_occupancy(kb_pq<T>, sms);
+  out[1] = vec_occupancy(kb_update<T>, sms);
+  out[2] = vec_occupancy(kb_yzr<T>, sms);
+  out[3] = vec_occupancy(kb_pupdate_z<T>, sms);
+}
+
 void ensure_batch(SolverImpl& S, int kp) {
   if (!S.bst) {
     ACG_CUDA(cudaMalloc(&S.bst, sizeof(PcgState) * kMaxBatch));
     ACG_CUDA(cudaMalloc(&S.bsh, sizeof(BatchShared)));
     ACG_CUDA(cudaMemset(S.bsh, 0, sizeof(BatchShared)));
     ACG_CUDA(cudaMallocHost(&S.h_bst, sizeof(PcgState) * kMaxBatch));
-    S.bpartials.alloc((size_t)4 * kVecBlocks * kMaxBatch);
+    S.bpartials.alloc((size_t)4 * (kVecBlocks + kRedGroups) * kMaxBatch);
     int sms = 0;
     ACG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S.device));
     S.bsweep_blocks[0][0] = batch_occupancy<double, 1>(sms, S.batch_bps);
@@ -1612,6 +1643,8 @@ void ensure_batch(SolverImpl& S, int kp) {
     S.bsweep_blocks[1][1] = batch_occupancy<float, 2>(sms, S.batch_bps);
     S.bsweep_blocks[1][2] = batch_occupancy<float, 4>(sms, S.batch_bps);
     S.bsweep_blocks[1][3] = batch_occupancy<float, 8>(sms, S.batch_bps);
+    vec_grids<double>(sms, S.bvec_blocks[0]);
+    vec_grids<float>(sms, S.bvec_blocks[1]);
     S.bspmv_blocks[0][0] = spmv_occupancy<double, 1>(sms);
     S.bspmv_blocks[0][1] = spmv_occupancy<double, 2>(sms);
     S.bspmv_blocks[0][2] = spmv_occupancy<double, 4>(sms);
@@ -1952,6 +1985,33 @@ int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, 
 }
 
 // Device time per call of the batched kernels for kp columns (see time_kernels_t).
+// Captures `reps` calls of body() in one graph, launches it once to warm up
+// and once timed; returns the milliseconds per call.
+template <typename F>
+double graph_ms(cudaStream_t s, int reps, F&& body) {
+  cudaGraph_t g;
+  ACG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < reps; ++i) body();
+  ACG_CUDA(cudaStreamEndCapture(s, &g));
+  cudaGraphExec_t ge;
+  ACG_CUDA(cudaGraphInstantiate(&ge, g, 0));
+  ACG_CUDA(cudaGraphLaunch(ge, s));
+  cudaEvent_t e0, e1;
+  ACG_CUDA(cudaEventCreate(&e0));
+  ACG_CUDA(cudaEventCreate(&e1));
+  ACG_CUDA(cudaEventRecord(e0, s));
+  ACG_CUDA(cudaGraphLaunch(ge, s));
+  ACG_CUDA(cudaEventRecord(e1, s));
+  ACG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  ACG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGraphExecDestroy(ge);
+  cudaGraphDestroy(g);
+  return (double)ms / reps;
+}
+
 template <typename T, int CPL>
 void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T* y, T* p, T* q, T* x3) {
   constexpr int kp = CPL * kBatchLanes;
@@ -1962,29 +2022,7 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
   ACG_CUDA(cudaStreamSynchronize(s));
   const TypedArrays<T> A = arrays_of<T>(S);
   const size_t N = (size_t)S.n * kp;
-  auto time_graph = [&](auto&& body) -> double {
-    cudaGraph_t g;
-    ACG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < reps; ++i) body();
-    ACG_CUDA(cudaStreamEndCapture(s, &g));
-    cudaGraphExec_t ge;
-    ACG_CUDA(cudaGraphInstantiate(&ge, g, 0));
-    ACG_CUDA(cudaGraphLaunch(ge, s));
-    cudaEvent_t e0, e1;
-    ACG_CUDA(cudaEventCreate(&e0));
-    ACG_CUDA(cudaEventCreate(&e1));
-    ACG_CUDA(cudaEventRecord(e0, s));
-    ACG_CUDA(cudaGraphLaunch(ge, s));
-    ACG_CUDA(cudaEventRecord(e1, s));
-    ACG_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    ACG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaGraphExecDestroy(ge);
-    cudaGraphDestroy(g);
-    return (double)ms / reps;
-  };
+  auto time_graph = [&](auto&& body) -> double { return graph_ms(s, reps, body); };
   auto fill_s = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)N, sv, (T*)nullptr); };
   auto fill_y = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)N, y, (T*)nullptr); };
   const double t_fill = time_graph(fill_s);
@@ -2043,19 +2081,19 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
     const double t_reset = time_graph(reset);
     out->pq_ms = time_graph([&]() {
       reset();
-      kb_pq<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(S.n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, none);
+      kb_pq<T><<<S.bvec_blocks[plan_index<T>()][0], kVecThreads, 0, s>>>(S.n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, none);
     }) - t_reset;
     out->update_ms = time_graph([&]() {
       reset();
-      kb_update<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(S.n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, none);
+      kb_update<T><<<S.bvec_blocks[plan_index<T>()][1], kVecThreads, 0, s>>>(S.n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, none);
     }) - t_reset;
     out->yzr_ms = time_graph([&]() {
       reset();
-      kb_yzr<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(S.n, kp, y, r, S.bst, S.bsh, S.bpartials.p, eps, none);
+      kb_yzr<T><<<S.bvec_blocks[plan_index<T>()][2], kVecThreads, 0, s>>>(S.n, kp, y, r, S.bst, S.bsh, S.bpartials.p, eps, none);
     }) - t_reset;
     out->pupdate_ms = time_graph([&]() {
       reset();
-      kb_pupdate_z<T><<<kBVecBlocks, kBVecThreads, 0, s>>>(S.n, kp, y, p, S.bst, S.bsh, S.bpartials.p, eps, none);
+      kb_pupdate_z<T><<<S.bvec_blocks[plan_index<T>()][3], kVecThreads, 0, s>>>(S.n, kp, y, p, S.bst, S.bsh, S.bpartials.p, eps, none);
     }) - t_reset;
     const double vec = (double)S.n * kp * sizeof(T);
     out->pq_bytes = 2.0 * vec;       // p, q read
@@ -2079,6 +2117,76 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
   BatchShared hb;
   ACG_CUDA(cudaMemcpy(&hb, S.bsh, sizeof(BatchShared), cudaMemcpyDeviceToHost));
   if (hb.sweep_error) throw CudaError("a batched sweep wait gave up while timing");
+}
+
+// The batched sweeps cut at given levels: for each levels[i] = L, the forward
+// sweep over the tasks of levels 0..L and the backward sweep over the tasks of
+// levels >= L (swept head levels only), each timed alone from the same inputs
+// as in time_batch_t.  The fills and the restore copy that prepare each run
+// are timed apart and subtracted.  How the time grows with L shows where the
+// DAG's levels cost most: the wide first levels, the long middle, the narrow
+// deep end near the critical path.
+template <typename T, int CPL>
+void time_levels_t(SolverImpl& S, int reps, int npts, const int* levels, double* fwd_ms, double* bwd_ms,
+                   int* fwd_tasks, int* bwd_tasks, T* r, T* sv, T* y, T* saved) {
+  constexpr int kp = CPL * kBatchLanes;
+  cudaStream_t s = S.stream;
+  const size_t N = (size_t)S.n * kp;
+  ACG_CUDA(cudaMemsetAsync(S.bsh, 0, sizeof(BatchShared), s));
+  ACG_CUDA(cudaMemsetAsync(r, 0, sizeof(T) * N, s));
+  auto fill_s = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)N, sv, (T*)nullptr); };
+  auto fill_yh = [&]() {
+    k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)((size_t)(S.dt_K ? S.dt_v0 : S.n) * kp), y, (T*)nullptr);
+  };
+  auto restore_s = [&]() { ACG_CUDA(cudaMemcpyAsync(sv, saved, sizeof(T) * N, cudaMemcpyDeviceToDevice, s)); };
+  // one whole forward pass (sweep and dense product) gives the backward runs
+  // their input s; the dense backward product writes the tail rows of y once
+  fill_s();
+  enqueue_bforward<T, CPL>(s, S, r, sv, y);
+  ACG_CUDA(cudaMemcpyAsync(saved, sv, sizeof(T) * N, cudaMemcpyDeviceToDevice, s));
+  if (S.dt_K)
+    enqueue_dense<T, CPL>(s, S, false, sv, y, reinterpret_cast<T*>(S.dt_part.p), &S.bsh->all_done);
+  ACG_CUDA(cudaStreamSynchronize(s));
+  const double t_fill = graph_ms(s, reps, fill_s);
+  const double t_back = graph_ms(s, reps, [&]() {
+    restore_s();
+    fill_yh();
+  });
+  const int nl = (int)S.tfb_upto.size();
+  if (nl == 0 || (int)S.tbb_from.size() != nl) throw InputError("the solver has no batched sweep tables");
+  for (int i = 0; i < npts; ++i) {
+    const int L = std::min(std::max(levels[i], 0), nl - 1);
+    const int tf = S.tfb_upto[L], tb = S.tbb_from[L];
+    fwd_tasks[i] = tf;
+    bwd_tasks[i] = tb;
+    fwd_ms[i] = graph_ms(s, reps, [&]() {
+                  fill_s();
+                  if (tf > 0) enqueue_bsweep<T, CPL, true>(s, S, r, (T*)nullptr, sv, y, tf);
+                }) - t_fill;
+    bwd_ms[i] = graph_ms(s, reps, [&]() {
+                  restore_s();
+                  fill_yh();
+                  if (tb > 0) enqueue_bsweep<T, CPL, false>(s, S, arrays_of<T>(S).g, sv, y, sv, tb);
+                }) - t_back;
+  }
+  BatchShared hb;
+  ACG_CUDA(cudaMemcpy(&hb, S.bsh, sizeof(BatchShared), cudaMemcpyDeviceToHost));
+  if (hb.sweep_error) throw CudaError("a batched sweep wait gave up while timing");
+}
+
+void time_levels(SolverImpl& S, int precision, int kp, int reps, int npts, const int* levels, double* fwd_ms,
+                 double* bwd_ms, int* fwd_tasks, int* bwd_tasks) {
+  drain_async(S);
+  ensure_batch(S, std::max(kp, S.batch_kp));
+  with_cpl(kp, [&](auto cpl) {
+    constexpr int C = decltype(cpl)::value;
+    if (precision == 0)
+      time_levels_t<double, C>(S, reps, npts, levels, fwd_ms, bwd_ms, fwd_tasks, bwd_tasks, S.br64.p, S.bs64.p,
+                               S.by64.p, S.bq64.p);
+    else
+      time_levels_t<float, C>(S, reps, npts, levels, fwd_ms, bwd_ms, fwd_tasks, bwd_tasks, S.br32.p, S.bs32.p,
+                              S.by32.p, S.bq32.p);
+  });
 }
 
 void time_batch(SolverImpl& S, int precision, int kp, int reps, acg_kernel_times* out) {
@@ -2823,6 +2931,30 @@ int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg
     }
     std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
     acg::time_batch(h->impl, precision, acg::round_kp(nrhs), reps, out);
+    return ACG_OK;
+  });
+}
+
+int acg_time_sweep_levels(acg_solver* h, int precision, int nrhs, int reps, int npts, const int* levels,
+                          double* fwd_ms, double* bwd_ms, int* fwd_tasks, int* bwd_tasks) {
+  if (!h || reps < 1 || nrhs < 1 || nrhs > acg::kMaxBatch || (precision != 0 && precision != 1) || npts < 0 ||
+      (npts > 0 && (!levels || !fwd_ms || !bwd_ms || !fwd_tasks || !bwd_tasks))) {
+    acg::set_last_error("acg_time_sweep_levels: bad arguments");
+    return ACG_ERR_INVALID;
+  }
+  return guarded("acg_time_sweep_levels", [&]() {
+    std::lock_guard<std::mutex> lk(h->impl.mu);
+    if (h->impl.serving) {
+      acg::set_last_error("acg_time_sweep_levels: the solver's batch buffers belong to its serving loop");
+      return ACG_ERR_BUSY;
+    }
+    if (h->impl.nseg > 1) {
+      acg::set_last_error("acg_time_sweep_levels: a group solver has no batched sweeps");
+      return ACG_ERR_INVALID;
+    }
+    std::lock_guard<std::recursive_mutex> glk(acg::g_device_mu);
+    acg::time_levels(h->impl, precision, acg::round_kp(nrhs), reps, npts, levels, fwd_ms, bwd_ms, fwd_tasks,
+                     bwd_tasks);
     return ACG_OK;
   });
 }

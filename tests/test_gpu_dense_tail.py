@@ -109,3 +109,30 @@ def test_kernel_timing_with_dense_tail(graph):
     kp = plain.time_kernels("fp64", reps=2)
     assert kp["dense_ms"] == 0 and kp["launches_per_iteration"] == 8
     dev.close()
+
+
+def test_sweep_levels_timing(graph):
+    """acg_time_sweep_levels: the forward prefixes grow and the backward
+    suffixes shrink with the level; the deepest swept level leaves the backward
+    sweep its own tasks only, and levels past the end are clamped."""
+    a, ldli, plain = graph
+    for solver in (acgpu.DeviceLapSolver(a, ldli), plain):
+        st = solver.stats()
+        swept = st["levels"] - st["dense_levels"]
+        pts = [0, 1, swept // 2, swept - 1, st["levels"] + 10]
+        for prec in ("fp64", "mixed"):
+            rows = solver.time_sweep_levels(pts, nrhs=16, precision=prec, reps=2)
+            ft = [r["forward_tasks"] for r in rows]
+            bt = [r["backward_tasks"] for r in rows]
+            assert all(0 < x <= y for x, y in zip(ft, ft[1:]))
+            assert all(x >= y for x, y in zip(bt, bt[1:]))
+            assert bt[0] > bt[3] > 0
+            # the last level is swept only without a dense tail
+            assert bt[-1] == (bt[3] if st["dense_levels"] == 0 else 0)
+            assert all(r["forward_ms"] > 0 for r in rows)
+        # still solves correctly afterwards
+        b = np.random.default_rng(9).standard_normal(a.shape[0])
+        x = solver(b, tol=1e-8, maxits=2000, precision="mixed")
+        assert O.relres(a, x, b - b.mean()) <= 1e-8 * 1.01
+        if solver is not plain:
+            solver.close()

@@ -86,13 +86,21 @@ def test_relres_on_a_disjoint_union_of_five(gpu_ok, precision):
     a = disjoint_union([mixed_graph(1234, i) for i in range(1, 6)])
     b = np.random.default_rng(5).standard_normal(a.shape[0])
     b -= b.mean()
+    # b is centred over the whole graph only, as in the reference's test: its
+    # per-component means are outside the range of the Laplacian, so the
+    # residual against b keeps them (about 2e-2 here); against b with those
+    # means removed each component's solve must meet its tolerance.
+    co = acgpu.components(a)
+    bc = b.copy()
+    for c in np.unique(co):
+        bc[co == c] -= bc[co == c].mean()
     for order in ("deg", "wdeg", "given"):
         acgpu.seed(3)
         f = acgpu.approxchol_lap(a, tol=1e-6, maxtime=5, params=acgpu.ApproxCholParams(order=order),
                                  precision=precision)
         x = f(b)
         assert O.relres(a, x, b) <= 1e-1, order
-        assert O.relres(a, x, b) <= 1e-5, (order, O.relres(a, x, b))
+        assert O.relres(a, x, bc) <= 1e-5, (order, O.relres(a, x, bc))
 
 
 def test_documented_grid3_50_solves(gpu_ok):
