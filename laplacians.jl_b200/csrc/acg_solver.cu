@@ -3031,6 +3031,25 @@ int acg_serve_open(acg_solver* h, int precision, int slots, int queue, acg_serve
     for (auto& x : st0) x.done = 1;
     ACG_CUDA(cudaMemcpy(S.bst, st0.data(), sizeof(acg::PcgState) * acg::kMaxBatch, cudaMemcpyHostToDevice));
     ACG_CUDA(cudaMemset(S.bsh, 0, sizeof(acg::BatchShared)));
+    {
+      // The loop's sweeps find s marked pending by the previous tick's
+      // backward sweep, and y by the forward sweep; before the first tick
+      // nothing has marked them, so mark both here.  Without this the first
+      // forward sweep took whatever the buffer held (zeros, or a freed
+      // solver's values) for ready inputs, and the columns admitted in the
+      // first tick began their PCG from a wrong z.  The columns' other vectors
+      // start at zero, so free slots carry finite values through the sweeps.
+      const size_t N = (size_t)S.n * srv->kp;
+      for (acg::DevBuf<double>* b : {&S.bbm, &S.br64, &S.bxf, &S.bp64, &S.bq64})
+        ACG_CUDA(cudaMemsetAsync(b->p, 0, sizeof(double) * N, S.stream));
+      ACG_CUDA(cudaMemsetAsync(S.bx3_64.p, 0, sizeof(double) * 3 * N, S.stream));
+      for (acg::DevBuf<float>* b : {&S.br32, &S.bp32, &S.bq32})
+        ACG_CUDA(cudaMemsetAsync(b->p, 0, sizeof(float) * N, S.stream));
+      ACG_CUDA(cudaMemsetAsync(S.bx3_32.p, 0, sizeof(float) * 3 * N, S.stream));
+      acg::k_fill_pending<double><<<acg::kVecBlocks, acg::kVecThreads, 0, S.stream>>>((int)N, S.bs64.p, S.by64.p);
+      acg::k_fill_pending<float><<<acg::kVecBlocks, acg::kVecThreads, 0, S.stream>>>((int)N, S.bs32.p, S.by32.p);
+      ACG_CUDA(cudaGetLastError());
+    }
     acg::with_cpl(srv->kp, [&](auto cpl) {
       constexpr int C = decltype(cpl)::value;
       srv->exec = acg::build_serve_graph<C>(S, precision, srv->ring_d, srv->reqs_d, srv->slots);
