@@ -155,6 +155,8 @@ typedef struct {
                                 the forward sweep tables, so its vertices' values are never
                                 produced and the waits on them run out; a test of the
                                 bounded waits that neither faults nor hangs the GPU     */
+  double min_inner_tol;      /* mixed precision: the smallest relative residual an inner
+                                FP32 solve is asked for (0 = 1e-5)                      */
 } acg_options;
 
 /* Shape of an uploaded solver. */
@@ -261,11 +263,16 @@ int acg_solve_async(acg_solver* h, const double* b, double* x, int64_t nrhs, int
                     int64_t maxits, double maxtime, int stag_test, int precision, acg_request** out);
 int acg_poll(acg_request* r);
 int acg_wait(acg_request* r, acg_solve_info* info);
-/* As acg_solve for one right-hand side already in device memory. */
+/* As acg_solve for one right-hand side already in device memory (on the
+ * solver's device).  The solve is ordered after the work already queued on the
+ * legacy default stream; a caller that wrote b_dev on a stream of its own
+ * synchronizes that stream first.  Other streams are not waited for, so
+ * serving loops and copies elsewhere on the GPU keep running.  Returns when x_dev
+ * holds the result. */
 int acg_solve_device(acg_solver* h, const double* b_dev, double* x_dev, double tol, int64_t maxits, double maxtime,
                      int stag_test, int precision, acg_solve_info* info);
 /* Block of nrhs right-hand sides already in device memory (column-major,
- * leading dimension ld >= n): solved 64 at a time in one batched launch, each
+ * leading dimension ld >= n; ordered as acg_solve_device): solved 64 at a time in one batched launch, each
  * column its own PCG system with the same stop rules as acg_solve; info[nrhs]
  * optional.  The reference solves one vector per call (src/pcg.jl:256). */
 int acg_solve_batch_device(acg_solver* h, const double* b_dev, double* x_dev, int64_t nrhs, int64_t ld, double tol,

@@ -34,7 +34,7 @@ class AcgOptions(ctypes.Structure):
                 ("batch_blocks_per_sm", ctypes.c_int), ("sweep_heavy", ctypes.c_int),
                 ("dense_tail", ctypes.c_int), ("sweep_stride", ctypes.c_int),
                 ("level_order", ctypes.c_int), ("spin_limit", ctypes.c_int),
-                ("test_unproduced_task", ctypes.c_int)]
+                ("test_unproduced_task", ctypes.c_int), ("min_inner_tol", ctypes.c_double)]
 
 
 class AcgStats(ctypes.Structure):

@@ -238,11 +238,11 @@ def _maxits_int(maxits) -> int:
 def _options(options: dict | None) -> AcgOptions:
     """acg_options from a dict of knob names; a misspelled knob raises."""
     opts = AcgOptions()
-    known = {f[0] for f in AcgOptions._fields_}
+    known = dict(AcgOptions._fields_)
     for k, v in (options or {}).items():
         if k not in known:
             raise ValueError(f"unknown solver option {k!r}; known: {sorted(known)}")
-        setattr(opts, k, int(v))
+        setattr(opts, k, float(v) if known[k] is ctypes.c_double else int(v))
     return opts
 
 

@@ -111,6 +111,8 @@ struct SolverImpl {
   int sweep_blocks[2] = {0, 0};    // co-resident grid of k_sweep per value type
   int poll_mode = 0;
   unsigned spin_limit = kSpinLimit;  // polls before a sweep wait gives up
+  double min_inner_tol = 1e-5;       // mixed precision: floor of an inner solve's tolerance
+  cudaEvent_t order_ev = nullptr;    // device entry points: after the legacy stream's work
   DevBuf<SweepTask> tasks_f, tasks_b;
 
   DevBuf<int> perm, lvl_off_d;
@@ -205,6 +207,7 @@ struct SolverImpl {
     }
     if (h2d_stream) cudaStreamDestroy(h2d_stream);
     if (d2h_stream) cudaStreamDestroy(d2h_stream);
+    if (order_ev) cudaEventDestroy(order_ev);
     if (bst) cudaFree(bst);
     if (bsh) cudaFree(bsh);
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -1105,6 +1108,7 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
     S.sweep_mode = (opts && opts->sweep_lanes == 1 && nseg == 1) ? 1 : 0;
     if (opts && opts->poll_mode > 0) S.poll_mode = opts->poll_mode - 1;
     if (opts && opts->spin_limit > 0) S.spin_limit = (unsigned)opts->spin_limit;
+    if (opts && opts->min_inner_tol > 0) S.min_inner_tol = std::min(0.25, opts->min_inner_tol);
     S.batch_bps = (opts && opts->batch_blocks_per_sm > 0) ? opts->batch_blocks_per_sm : 0;
   }
   ACG_CUDA(cudaFuncSetAttribute(k_thin<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
@@ -1626,6 +1630,18 @@ void vec_grids(int sms, int (&out)[4]) {
   out[3] = vec_occupancy(kb_pupdate_z<T>, sms);
 }
 
+// The device-pointer entry points read b where the caller wrote it: order the
+// solver's stream after the work already queued on the legacy default stream
+// (where a caller without streams of its own writes), without holding up the
+// host or any other stream (a device-wide synchronization would stall every
+// serving loop and copy on the GPU).  A caller writing b on a stream of its
+// own synchronizes that stream first.
+void order_after_legacy_stream(SolverImpl& S) {
+  if (!S.order_ev) ACG_CUDA(cudaEventCreateWithFlags(&S.order_ev, cudaEventDisableTiming));
+  ACG_CUDA(cudaEventRecord(S.order_ev, cudaStreamLegacy));
+  ACG_CUDA(cudaStreamWaitEvent(S.stream, S.order_ev, 0));
+}
+
 void ensure_batch(SolverImpl& S, int kp) {
   if (!S.bst) {
     ACG_CUDA(cudaMalloc(&S.bst, sizeof(PcgState) * kMaxBatch));
@@ -1676,7 +1692,8 @@ void ensure_batch(SolverImpl& S, int kp) {
   S.batch_kp = kp;
 }
 
-void init_batch_states(PcgState* h, int kp, double tol, int64_t maxits, double maxtime, int stag_test) {
+void init_batch_states(PcgState* h, int kp, double tol, int64_t maxits, double maxtime, int stag_test,
+                       double min_inner_tol) {
   std::memset(h, 0, sizeof(PcgState) * kMaxBatch);
   for (int c = 0; c < kp; ++c) {
     h[c].tol = tol;
@@ -1685,7 +1702,7 @@ void init_batch_states(PcgState* h, int kp, double tol, int64_t maxits, double m
     h[c].stag_test = stag_test;
     h[c].tol_user = tol;
     h[c].maxits_user = maxits;
-    h[c].min_inner_tol = 1e-5;
+    h[c].min_inner_tol = min_inner_tol;
     h[c].max_outer = 40;
     h[c].inner_tol = std::min(0.25, std::max(h[c].min_inner_tol, 0.5 * tol));
   }
@@ -1738,7 +1755,7 @@ int solve_batch(SolverImpl& S, const double* B, int64_t ldb, double* X, int64_t 
   cudaGraphExec_t ge = batch_graph(S, 0, precision, kp);
   glk.unlock();
   PcgState* h = S.h_bst;
-  init_batch_states(h, kp, tol, maxits, maxtime, stag_test);
+  init_batch_states(h, kp, tol, maxits, maxtime, stag_test, S.min_inner_tol);
   BatchShared hb = {};
   hb.k = k;
   ACG_CUDA(cudaMemcpyAsync(S.bst, h, sizeof(PcgState) * kp, cudaMemcpyHostToDevice, s));
@@ -1899,7 +1916,7 @@ int solve_group(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, c
     h[g].nvert = S.seg_off[g + 1] - S.seg_off[g];
     h[g].tol_user = tol;
     h[g].maxits_user = maxits;
-    h[g].min_inner_tol = 1e-5;
+    h[g].min_inner_tol = S.min_inner_tol;
     h[g].max_outer = 40;
     h[g].inner_tol = std::min(0.25, std::max(h[g].min_inner_tol, 0.5 * tol));
   }
@@ -1952,7 +1969,7 @@ int solve_column(SolverImpl& S, const double* b, double* x, cudaMemcpyKind kin, 
   h.stag_test = stag_test;
   h.tol_user = tol;
   h.maxits_user = maxits;
-  h.min_inner_tol = 1e-5;
+  h.min_inner_tol = S.min_inner_tol;
   h.max_outer = 40;
   double it0 = 0.5 * tol;
   h.inner_tol = std::min(0.25, std::max(h.min_inner_tol, it0));
@@ -2078,22 +2095,25 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
     const double eps = sizeof(T) == 4 ? 1.1920928955078125e-07 : kEps64;
     const LoopCtl none{0, 0};
     auto reset = [&]() { kb_timing_state<<<1, 64, 0, s>>>(S.bst, S.bsh, kp); };
+    // the copies without the loop-condition call (the same passes; a profiler
+    // measures these, not the loop's own kernels)
+    const int* vg = S.bvec_blocks[plan_index<T>()];
     const double t_reset = time_graph(reset);
     out->pq_ms = time_graph([&]() {
       reset();
-      kb_pq<T><<<S.bvec_blocks[plan_index<T>()][0], kVecThreads, 0, s>>>(S.n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, none);
+      kb_pq<T, false><<<vg[0], kVecThreads, 0, s>>>(S.n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, none);
     }) - t_reset;
     out->update_ms = time_graph([&]() {
       reset();
-      kb_update<T><<<S.bvec_blocks[plan_index<T>()][1], kVecThreads, 0, s>>>(S.n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, none);
+      kb_update<T, false><<<vg[1], kVecThreads, 0, s>>>(S.n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, none);
     }) - t_reset;
     out->yzr_ms = time_graph([&]() {
       reset();
-      kb_yzr<T><<<S.bvec_blocks[plan_index<T>()][2], kVecThreads, 0, s>>>(S.n, kp, y, r, S.bst, S.bsh, S.bpartials.p, eps, none);
+      kb_yzr<T, false><<<vg[2], kVecThreads, 0, s>>>(S.n, kp, y, r, S.bst, S.bsh, S.bpartials.p, eps, none);
     }) - t_reset;
     out->pupdate_ms = time_graph([&]() {
       reset();
-      kb_pupdate_z<T><<<S.bvec_blocks[plan_index<T>()][3], kVecThreads, 0, s>>>(S.n, kp, y, p, S.bst, S.bsh, S.bpartials.p, eps, none);
+      kb_pupdate_z<T, false><<<vg[3], kVecThreads, 0, s>>>(S.n, kp, y, p, S.bst, S.bsh, S.bpartials.p, eps, none);
     }) - t_reset;
     const double vec = (double)S.n * kp * sizeof(T);
     out->pq_bytes = 2.0 * vec;       // p, q read
@@ -2306,7 +2326,7 @@ int submit_async(acg_solver* h, const double* B, double* X, int k, int64_t ld, d
   cudaPointerAttributes pa;
   if (cudaPointerGetAttributes(&pa, X) == cudaSuccess) req->pinned_x = pa.type == cudaMemoryTypeHost;
   else cudaGetLastError();
-  init_batch_states(a.h_init, kp, tol, maxits, maxtime, stag_test);
+  init_batch_states(a.h_init, kp, tol, maxits, maxtime, stag_test, S.min_inner_tol);
   *a.h_bsh = BatchShared{};
   a.h_bsh->k = k;
   const size_t row = sizeof(double) * S.n;
@@ -2794,7 +2814,7 @@ int acg_solve_device(acg_solver* h, const double* b_dev, double* x_dev, double t
   }
   return guarded("acg_solve_device", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
-    ACG_CUDA(cudaDeviceSynchronize());
+    acg::order_after_legacy_stream(h->impl);
     return acg::solve_column(h->impl, b_dev, x_dev, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice, tol, maxits,
                              maxtime, stag_test, precision, info);
   });
@@ -2812,7 +2832,7 @@ int acg_solve_batch_device(acg_solver* h, const double* b_dev, double* x_dev, in
       acg::set_last_error("acg_solve_batch_device: the solver's batch buffers belong to its serving loop");
       return ACG_ERR_BUSY;
     }
-    ACG_CUDA(cudaDeviceSynchronize());
+    acg::order_after_legacy_stream(h->impl);
     int worst = ACG_OK;
     for (int64_t c0 = 0; c0 < nrhs; c0 += acg::kMaxBatch) {
       const int k = (int)std::min<int64_t>(acg::kMaxBatch, nrhs - c0);
