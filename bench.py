@@ -872,6 +872,12 @@ def parallel_factor_record(k=64, steps=3):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     kt = dev.time_kernels_batch(k, "mixed", reps=3)
+    # one right-hand side alone: the shallower DAG shortens every sweep
+    single = []
+    for i in range(3):
+        check(lib().acg_solve_device(dev._h, ctypes.c_void_p(B[0, i].data_ptr()), ctypes.c_void_p(X.data_ptr()), TOL,
+                                     MAXITS, float("inf"), 5, 1, infos))
+        single.append(infos[0].solve_ms)
     dev.close()
     return {"workload": f"grid3({GRID_SIDE}) log-uniform weights, factor by the opt-in parallel elimination, "
                         f"{k} RHS per batched mixed solve, tol 1e-8",
@@ -879,7 +885,8 @@ def parallel_factor_record(k=64, steps=3):
             "levels": st["levels"], "dense_levels": st["dense_levels"],
             "solves_per_s": steps * k / (ms * 1e-3), "pcg_iterations_mean": float(np.mean([r[0] for r in res])),
             "true_relres_max": float(max(r[1] for r in res)), "all_converged": all(r[2] == 0 for r in res),
-            "forward_sweep_ms": kt["forward_sweep_ms"], "backward_sweep_ms": kt["backward_sweep_ms"]}
+            "forward_sweep_ms": kt["forward_sweep_ms"], "backward_sweep_ms": kt["backward_sweep_ms"],
+            "single_rhs_latency_ms": float(np.median(single))}
 
 
 def run_reference(args):

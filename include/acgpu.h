@@ -77,7 +77,8 @@ int acg_approxchol_ordered(int64_t n, const int64_t* colptr, const int64_t* rowv
                            const int64_t* perm, uint64_t rng_state[4], acg_factor** out);
 /* The split/merge elimination of approxchol_lap2 (split = merge = 2 there):
  * approxChol(LLmatp(a, split), split, merge) (src/approxChol.jl:979-1157,
- * 138-183) with compressAvgCol! (src/approxChol.jl:541-600). */
+ * 138-183) with compressAvgCol! (src/approxChol.jl:541-600); merge < 1 is
+ * approxChol(LLmatp(a, split), split) (src/approxChol.jl:1162-1322, avgCol!). */
 int acg_approxchol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval, int64_t split,
                          int64_t merge, uint64_t rng_state[4], acg_factor** out);
 /* Opt-in, not the reference's elimination: a parallel approximate Cholesky

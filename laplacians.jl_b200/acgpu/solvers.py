@@ -142,7 +142,8 @@ def approx_chol(a, params: ApproxCholParams | None = None) -> LDLinv:
     """The reference's host elimination, drawing from the global stream:
     `approxChol(LLmatp(a))` for the default :deg order (src/approxChol.jl:864-977),
     `approxChol(LLmatp(a, split), split, merge)` for :deg with split, merge >= 1
-    (src/approxChol.jl:979-1157; approxchol_lap2 uses 2, 2), and
+    (src/approxChol.jl:979-1157; approxchol_lap2 uses 2, 2), `approxChol(LLmatp(a,
+    split), split)` for split >= 1, merge < 1 (src/approxChol.jl:1162-1322), and
     `approxChol(LLMatOrd(a[, p]))` for :wdeg, :random and any other order, which
     the reference treats as :given (src/approxChol.jl:758-862, 1791-1851)."""
     a = _csc(a)
@@ -154,8 +155,7 @@ def approx_chol(a, params: ApproxCholParams | None = None) -> LDLinv:
     cp = a.indptr.astype(np.int64) + 1
     rv = a.indices.astype(np.int64) + 1
     if order == "deg" and params.split >= 1:
-        if params.merge < 1:
-            raise NotImplementedError("approxChol(llmat, split) without merging is not built; use merge >= 1")
+        # merge < 1: approxChol(llmat, split) (src/approxChol.jl:1162-1322)
         check(L.acg_approxchol_split(n, cp, rv, np.ascontiguousarray(a.data), int(params.split), int(params.merge),
                                      _RNG, ctypes.byref(h)))
     elif order == "deg":

@@ -177,6 +177,16 @@ __device__ __forceinline__ void st_stream_row(double* p, const double (&v)[CPL],
   }
 }
 
+// Build-time tuning of the batched sweeps: resident blocks per SM the 32- and
+// 64-column FP32 sweeps are compiled for (their register budget), and the
+// input rows a lane loads per batch when a row is at most 32 bytes.
+#ifndef ACG_BSWEEP_F32_BLOCKS
+#define ACG_BSWEEP_F32_BLOCKS 2
+#endif
+#ifndef ACG_BSWEEP_ROWS
+#define ACG_BSWEEP_ROWS 8
+#endif
+
 // ---- batched sync-free sweep -----------------------------------------------
 //
 // Task records as in k_sweep.  Groups of 8 lanes; lane l of a group owns
@@ -198,7 +208,7 @@ __device__ __forceinline__ void st_stream_row(double* p, const double (&v)[CPL],
 // spills).  The narrower FP32 sweeps fit two blocks anyway.
 template <typename T, int CPL>
 __host__ __device__ constexpr int kb_sweep_min_blocks() {
-  return (sizeof(T) == 4 && CPL >= 4) ? 2 : 1;
+  return (sizeof(T) == 4 && CPL >= 4) ? ACG_BSWEEP_F32_BLOCKS : 1;
 }
 
 template <typename T, int CPL, bool kForward>
@@ -209,7 +219,7 @@ __global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>())
   if (bs->all_done) return;
   constexpr int kp = CPL * kBatchLanes;
   // rows loaded per batch: a whole slot of 8 entries where registers allow
-  constexpr int EB = (CPL * sizeof(T) <= 32) ? 8 : 4;
+  constexpr int EB = (CPL * sizeof(T) <= 32) ? ACG_BSWEEP_ROWS : 4;
   const int lane = threadIdx.x & 31;
   const int gl = lane & 7;
   const int W = (int)((gridDim.x * blockDim.x) >> 5);

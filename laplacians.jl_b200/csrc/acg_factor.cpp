@@ -533,10 +533,16 @@ void approx_chol_ord(int64_t n, const int64_t* colptr, const int64_t* rowval, co
 // Every edge becomes `split` parallel records of weight w/split; record k of
 // CSC entry p (0-based) is split*p + k, paired with record k of the entry's
 // transpose.
+// merge < 1 is approxChol(a, split) (src/approxChol.jl:1162-1322), which
+// differs from the merge form only in averaging parallel edges with avgCol!
+// (src/approxChol.jl:497-533) instead of compressAvgCol!: with no cap on the
+// parallel edges compressAvgCol! keeps every record, divides by their count
+// and sorts as avgCol! does, so merge < 1 runs as an unreachable cap.
 void approx_chol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval,
                        int64_t split, int64_t merge, JuliaRng* rng, HostFactor& out) {
   if (n < 2) throw std::runtime_error("approxChol needs at least 2 vertices");
-  if (split < 1 || merge < 1) throw std::runtime_error("split and merge must be at least 1");
+  if (split < 1) throw std::runtime_error("split must be at least 1");
+  if (merge < 1) merge = INT64_MAX;
   const int64_t base = colptr[0];
   const int64_t nnz = colptr[n] - base;
   LinkedCols a;

@@ -159,8 +159,8 @@ int acg_approxchol_parallel(int64_t n, const int64_t* colptr, const int64_t* row
 
 int acg_approxchol_split(int64_t n, const int64_t* colptr, const int64_t* rowval, const double* nzval, int64_t split,
                          int64_t merge, uint64_t rng_state[4], acg_factor** out) {
-  if (split < 1 || merge < 1 || split > 64) {
-    acg::set_last_error("acg_approxchol_split: need 1 <= split <= 64 and merge >= 1");
+  if (split < 1 || split > 64) {
+    acg::set_last_error("acg_approxchol_split: need 1 <= split <= 64");
     return ACG_ERR_INVALID;
   }
   return approxchol_entry("acg_approxchol_split", n, colptr, rowval, nzval, nullptr, 2, split, merge, rng_state, out);

@@ -418,7 +418,11 @@ def approx_chol_ord(colptr, rowval, nzval, rng: JuliaRng, perm=None):
 def approx_chol_split(colptr, rowval, nzval, rng: JuliaRng, split=2, merge=2):
     """approxChol(::LLmatp, split, merge) (src/approxChol.jl:979-1157) on
     LLmatp(a, split) (src/approxChol.jl:138-183) with compressAvgCol!
-    (src/approxChol.jl:541-600).  colptr/rowval 1-based."""
+    (src/approxChol.jl:541-600).  colptr/rowval 1-based.  merge < 1 is
+    approxChol(::LLmatp, split) (src/approxChol.jl:1162-1322), whose avgCol!
+    (src/approxChol.jl:497-533) is compressAvgCol! with no cap reached."""
+    if merge < 1:
+        merge = float("inf")
     n = len(colptr) - 1
     m = colptr[n] - 1
     # LLmatp(a, split): llelems[split*(ind-1)+k], k = 1..split

@@ -139,7 +139,7 @@ def _ref_split(a, seed, split, merge):
 
 
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("split,merge", [(2, 2), (3, 2), (2, 1)])
+@pytest.mark.parametrize("split,merge", [(2, 2), (3, 2), (2, 1), (2, 0), (3, 0)])
 def test_split_merge_factor_matches_restatement(name, make, split, merge):
     a = make()
     ref = _ref_split(a, 5, split, merge)
@@ -150,3 +150,17 @@ def test_split_merge_factor_matches_restatement(name, make, split, merge):
         assert np.array_equal(np.asarray(x), np.asarray(y)), what
     n = a.shape[0]
     assert len(set(f.col.tolist())) == n - 1 and f.colptr[-1] - 1 == f.fval.shape[0]
+
+
+@pytest.mark.parametrize("split", [2, 3])
+def test_split_without_merge_is_an_unreached_cap(split):
+    """approxChol(llmat, split) (merge < 1) averages parallel edges like
+    compressAvgCol! with a cap no vertex reaches: the factor equals the merge
+    form with merge >= the largest multiplicity, and differs from a low cap."""
+    a = G.grid2(12, weights="loguniform", seed=3)
+    fs = []
+    for merge in (0, 10 ** 9, 1):
+        acgpu.seed(9)
+        fs.append(acgpu.approx_chol(a, acgpu.ApproxCholParams("deg", 5, split, merge)))
+    assert np.array_equal(fs[0].fval, fs[1].fval) and np.array_equal(fs[0].rowval, fs[1].rowval)
+    assert not (fs[0].fval.shape == fs[2].fval.shape and np.array_equal(fs[0].fval, fs[2].fval))
