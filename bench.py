@@ -674,8 +674,23 @@ def run_many_graphs(args):
         infos = gs.last_info
         out[prec] = {"group_ms": 1e3 * min(times), "graphs_per_s": len(graphs) / min(times),
                      "its_max": max(i.iterations for i in infos),
+                     "its_mean": float(np.mean([i.iterations for i in infos])),
                      "true_relres_max": max(i.true_relres for i in infos),
                      "all_converged": all(i.status == 0 for i in infos)}
+        its_by_prec = out.setdefault("_its", {})
+        its_by_prec[prec] = [(int(i.iterations), int(i.refinements), int(i.status)) for i in infos]
+    # the group waits for its slowest member: the five with the most iterations
+    # in each precision, with the member's size and weight spread
+    slow = {}
+    for prec in ("fp64", "mixed"):
+        order = sorted(range(len(members)), key=lambda m: -out["_its"][prec][m][0])[:5]
+        slow[prec] = [{"member": m, "n": int(comp_graphs[m].shape[0]),
+                       "weight_max_over_min": float(comp_graphs[m].data.max() / comp_graphs[m].data.min()),
+                       "fp64_its": out["_its"]["fp64"][m][0],
+                       "mixed_its": out["_its"]["mixed"][m][0], "mixed_refinements": out["_its"]["mixed"][m][1]}
+                      for m in order]
+    out["slowest_members"] = slow
+    del out["_its"]
     out["levels_max"] = gs.stats()["levels"]
     seq = []
     for a, f, b in zip(comp_graphs, factors, comp_b):

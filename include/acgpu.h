@@ -294,7 +294,8 @@ int acg_create_group(int64_t ngraphs, const int64_t* offsets, int64_t n, const i
 /* One right-hand side per graph (b: n values of the union, host); info[ngraphs].
  * precision 0: FP64 PCG per graph; 1: each graph's FP32 PCG inside its own FP64
  * refinement on the true residual (as acg_solve's precision 1), all graphs in
- * the same launches. */
+ * the same launches.  A group of one graph (or any one-graph solver) is solved
+ * as acg_solve does. */
 int acg_solve_group(acg_solver* h, const double* b, double* x, double tol, int64_t maxits, double maxtime,
                     int stag_test, int precision, acg_solve_info* info);
 

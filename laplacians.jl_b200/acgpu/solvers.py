@@ -588,12 +588,21 @@ class _GroupPart:
     blockSolver, src/solverInterface.jl:152-188)."""
 
     def __init__(self, graphs, factors, params, precision, options):
-        self.group = GroupSolver(graphs, factors, stag_test=params.stag_test, options=options)
         self.precision = precision
+        if len(graphs) == 1:
+            # one large component: the one-graph solver (dense tail and all)
+            self.group = None
+            self.single = DeviceLapSolver(graphs[0], factors[0], params=params, options=options)
+        else:
+            self.group = GroupSolver(graphs, factors, stag_test=params.stag_test, options=options)
+            self.single = None
 
     def __call__(self, bs, tol, maxits, maxtime, precision=None):
-        xs = self.group(bs, tol=tol, maxits=maxits, maxtime=maxtime,
-                        precision=self.precision if precision is None else precision)
+        precision = self.precision if precision is None else precision
+        if self.single is not None:
+            x = self.single(bs[0], tol=tol, maxits=maxits, maxtime=maxtime, precision=precision)
+            return [x], int(self.single.last_info[0].iterations)
+        xs = self.group(bs, tol=tol, maxits=maxits, maxtime=maxtime, precision=precision)
         its = max(int(i.iterations) for i in self.group.last_info)
         return xs, its
 

@@ -179,12 +179,15 @@ __device__ __forceinline__ void st_stream_row(double* p, const double (&v)[CPL],
 
 // Build-time tuning of the batched sweeps: resident blocks per SM the 32- and
 // 64-column FP32 sweeps are compiled for (their register budget), and the
-// input rows a lane loads per batch when a row is at most 32 bytes.
+// input rows a lane loads per batch (rows of at most 32 bytes, wider rows).
 #ifndef ACG_BSWEEP_F32_BLOCKS
 #define ACG_BSWEEP_F32_BLOCKS 2
 #endif
 #ifndef ACG_BSWEEP_ROWS
 #define ACG_BSWEEP_ROWS 8
+#endif
+#ifndef ACG_BSWEEP_WIDE_ROWS  // the same for rows wider than 32 bytes
+#define ACG_BSWEEP_WIDE_ROWS 8
 #endif
 
 // ---- batched sync-free sweep -----------------------------------------------
@@ -205,7 +208,10 @@ __device__ __forceinline__ void st_stream_row(double* p, const double (&v)[CPL],
 // forward 1.05 -> 0.90 ms, backward 1.24 -> 1.04 ms, with 140-148 B of
 // spills; loading 4 rows per batch instead of 8 to avoid the spills was
 // slower, 1.08 / 1.10 ms; 32 columns: 0.90 / 0.95 -> 0.66 / 0.78 ms, no
-// spills).  The narrower FP32 sweeps fit two blocks anyway.
+// spills).  The narrower FP32 sweeps fit two blocks anyway.  Three blocks
+// (80 registers, 4-row batches) were slower again: 1.21 / 1.25 ms.  The
+// 64-column FP64 sweeps run one block per SM and load 8 of their 64-byte rows
+// per batch (242 registers, no spills; 4 rows: 1.87 / 1.78 -> 1.42 / 1.39 ms).
 template <typename T, int CPL>
 __host__ __device__ constexpr int kb_sweep_min_blocks() {
   return (sizeof(T) == 4 && CPL >= 4) ? ACG_BSWEEP_F32_BLOCKS : 1;
@@ -219,7 +225,7 @@ __global__ void __launch_bounds__(kSweepThreads, kb_sweep_min_blocks<T, CPL>())
   if (bs->all_done) return;
   constexpr int kp = CPL * kBatchLanes;
   // rows loaded per batch: a whole slot of 8 entries where registers allow
-  constexpr int EB = (CPL * sizeof(T) <= 32) ? ACG_BSWEEP_ROWS : 4;
+  constexpr int EB = (CPL * sizeof(T) <= 32) ? ACG_BSWEEP_ROWS : ACG_BSWEEP_WIDE_ROWS;
   const int lane = threadIdx.x & 31;
   const int gl = lane & 7;
   const int W = (int)((gridDim.x * blockDim.x) >> 5);

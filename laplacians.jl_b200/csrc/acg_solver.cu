@@ -2795,12 +2795,16 @@ int acg_create_group(int64_t ngraphs, const int64_t* offsets, int64_t n, const i
 
 int acg_solve_group(acg_solver* h, const double* b, double* x, double tol, int64_t maxits, double maxtime,
                     int stag_test, int precision, acg_solve_info* info) {
-  if (!h || !b || !x || h->impl.nseg < 2 || (precision != 0 && precision != 1)) {
-    acg::set_last_error("acg_solve_group: bad arguments (needs a solver made by acg_create_group, precision 0 or 1)");
+  if (!h || !b || !x || (precision != 0 && precision != 1)) {
+    acg::set_last_error("acg_solve_group: bad arguments (precision 0 or 1)");
     return ACG_ERR_INVALID;
   }
   return guarded("acg_solve_group", [&]() {
     std::lock_guard<std::mutex> lk(h->impl.mu);
+    // a group of one graph is an ordinary solver: one column, info[0]
+    if (h->impl.nseg < 2)
+      return acg::solve_column(h->impl, b, x, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol, maxits, maxtime,
+                               stag_test, precision, info);
     return acg::solve_group(h->impl, b, x, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, tol, maxits, maxtime,
                             stag_test, precision, info);
   });

@@ -87,3 +87,31 @@ def test_negative_weight_error(gpu_ok):
     a[0, 1] = a[1, 0] = -2.0
     with pytest.raises(ValueError):
         acgpu.approxchol_lap(a.tocsc())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_one_large_component_with_isolated_vertices(gpu_ok, precision):
+    """The common disconnected case: one component of at least 50 vertices plus
+    a small one and isolated vertices.  The large one runs on the one-graph
+    solver; a one-graph group solves too (as acg_solve does)."""
+    big = G.grid2(30, weights="loguniform", seed=7)
+    a = _union([big, G.path_graph(6)], 4)
+    n = a.shape[0]
+    co = acgpu.components(a)
+    b = np.random.default_rng(2).standard_normal(n)
+    for c in np.unique(co):
+        b[co == c] -= b[co == c].mean()
+    acgpu.seed(4)
+    its = [0]
+    f = acgpu.approxchol_lap(a, tol=1e-9, pcgIts=its, precision=precision)
+    assert f.group is not None and f.group.group is None and f.group.single is not None
+    x = f(b)
+    assert O.relres(a, x, b) < 1e-8 and its[0] > 0
+    assert np.all(x[-4:] == 0)
+    acgpu.seed(4)
+    ldli = acgpu.approx_chol(big)
+    g1 = acgpu.GroupSolver([big], [ldli])
+    nb = big.shape[0]
+    xg = g1([b[:nb]], tol=1e-9, precision=precision)[0]
+    assert O.relres(big, xg, b[:nb]) < 1e-8 and g1.last_info[0].status == 0
+    g1.close()
