@@ -8,6 +8,8 @@
 // one-right-hand-side kernels, run by thread c for column c); a launch ends
 // early only when every column has stopped.
 #pragma once
+#include <type_traits>
+
 #include "acg_pcg.cuh"
 
 namespace acg {
@@ -32,6 +34,8 @@ struct BatchShared {
   int sweep_error;  // a bounded sweep wait gave up
   int k;            // right-hand sides in this launch (the rest of kp is padding)
   int l1_due;       // kb_yzr deferred the third L1 test of some column to kb_pupdate_z
+  int pq_full;      // kb_pq makes its pass: some column's next step runs the L1 tests
+  int pad;
   unsigned int counter[16];
   unsigned int gcounter[16][kRedGroups];  // per-group tickets of the two-level reductions
 };
@@ -392,20 +396,36 @@ __device__ __forceinline__ void ldg_row(T (&v)[CPL], const T* src) {
   }
 }
 
+template <int NV, int VPT>
+__device__ __forceinline__ bool batch_reduce_v(double (&v)[NV][VPT], int kp, double* partials, BatchShared* bs,
+                                               int ci, double (&out)[NV]);
+
 // One row per group of 8 lanes.  The group's lanes load up to 8 of the row's
 // entries at once, share them with shuffles inside the group, and issue every
 // gathered row before the first multiply-add; entries are summed in row order.
-template <typename T, int CPL>
+//
+// kDot (the PCG loop body): also p.q per column, each lane summing its rows'
+// p_v * q_v (p_v read again, from L1: the row's diagonal entry gathered it), in
+// FP32 for FP32 vectors and FP64 for FP64, then over the grid in FP64 in a
+// fixed order (st[c].pq_dot).  The last block also tells kb_pq whether some
+// column's next step is one of the every-10th steps that need |p|_1 and |q|_1
+// (BatchShared::pq_full); on the other steps kb_pq skips its pass over p and q.
+template <typename T, int CPL, bool kDot = false>
 __global__ void __launch_bounds__(kVecThreads) kb_spmv(int n, const int* __restrict__ ptr, const int* __restrict__ idx,
                                                        const T* __restrict__ val, const T* __restrict__ p,
-                                                       T* __restrict__ q, const BatchShared* bs) {
+                                                       T* __restrict__ q, BatchShared* bs, PcgState* st = nullptr,
+                                                       double* partials = nullptr) {
   if (bs && bs->all_done) return;
   constexpr int kp = CPL * kBatchLanes;
+  using Acc = typename std::conditional<sizeof(T) == 4, float, double>::type;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int gl = gt & 7;
   const unsigned gmask = 0xffu << (threadIdx.x & 24);  // this group's lanes
   const int groups = gridDim.x * blockDim.x / 8;
   const unsigned long long pol = l2_evict_first_policy();
+  Acc pq[CPL];
+#pragma unroll
+  for (int j = 0; j < CPL; ++j) pq[j] = Acc(0);
   int row = gt / 8;
   int n0 = row < n ? __ldg(&ptr[row]) : 0, n1 = row < n ? __ldg(&ptr[row + 1]) : 0;
   for (; row < n; row += groups) {
@@ -440,6 +460,28 @@ __global__ void __launch_bounds__(kVecThreads) kb_spmv(int n, const int* __restr
         }
     }
     st_stream_row<CPL>(q + (size_t)row * kp + gl * CPL, acc, pol);
+    if constexpr (kDot) {
+      T own[CPL];
+      ldg_row<T, CPL>(own, p + (size_t)row * kp + gl * CPL);
+#pragma unroll
+      for (int j = 0; j < CPL; ++j) pq[j] += (Acc)own[j] * (Acc)acc[j];
+    }
+  }
+  if constexpr (kDot) {
+    double v[1][CPL];
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) v[0][j] = (double)pq[j];
+    double tot[1];
+    if (batch_reduce_v<1, CPL>(v, kp, partials, bs, 13, tot)) {
+      const int c = threadIdx.x;
+      bool need = false;
+      if (c < kp) {
+        st[c].pq_dot = tot[0];
+        need = !st[c].done && !st[c].entering && (st[c].itcnt + 1) % 10 == 0;
+      }
+      const int any = __syncthreads_or(need);
+      if (threadIdx.x == 0) bs->pq_full = any;
+    }
   }
 }
 
@@ -540,9 +582,9 @@ __device__ __forceinline__ void sum_rows(const double* src, size_t qstride, int 
 // Sums, per column, the rows [0, rows) of NV tables of kp columns into `out`
 // of the threads below kp: the block's threads split the rows into
 // blockDim / kp contiguous parts, and the parts are added in order.
-template <int NV>
+template <int NV, int kTile>
 __device__ __forceinline__ void block_sum_rows(const double* src, size_t qstride, int kp, int rows,
-                                               double (&sm)[NV][kVecThreads * 4], double (&out)[NV]) {
+                                               double (&sm)[NV][kVecThreads * kTile], double (&out)[NV]) {
   const int per = (int)blockDim.x / kp;
   const int c = threadIdx.x % kp, part = threadIdx.x / kp;
   double s[NV];
@@ -576,8 +618,8 @@ __device__ __forceinline__ void block_sum_rows(const double* src, size_t qstride
 template <int NV, int VPT>
 __device__ __forceinline__ bool batch_reduce_v(double (&v)[NV][VPT], int kp, double* partials, BatchShared* bs,
                                                int ci, double (&out)[NV]) {
-  static_assert(VPT <= 4, "shared tile holds 4 values per thread");
-  __shared__ double sm[NV][kVecThreads * 4];
+  constexpr int kTile = VPT > 4 ? VPT : 4;
+  __shared__ double sm[NV][kVecThreads * kTile];
   __shared__ bool am_last;
 #pragma unroll
   for (int q = 0; q < NV; ++q)
@@ -609,7 +651,7 @@ __device__ __forceinline__ bool batch_reduce_v(double (&v)[NV][VPT], int kp, dou
   // the group's last block: its rows into the group row
   {
     double t[NV];
-    block_sum_rows<NV>(partials + (size_t)gb0 * kp, (size_t)G * kp, kp, gb1 - gb0, sm, t);
+    block_sum_rows<NV, kTile>(partials + (size_t)gb0 * kp, (size_t)G * kp, kp, gb1 - gb0, sm, t);
     if ((int)threadIdx.x < kp) {
 #pragma unroll
       for (int q = 0; q < NV; ++q) grows[((size_t)q * NG + g) * kp + threadIdx.x] = t[q];
@@ -624,7 +666,7 @@ __device__ __forceinline__ bool batch_reduce_v(double (&v)[NV][VPT], int kp, dou
   __syncthreads();
   if (!am_last) return false;
   __threadfence();
-  block_sum_rows<NV>(grows, (size_t)NG * kp, kp, NG, sm, out);
+  block_sum_rows<NV, kTile>(grows, (size_t)NG * kp, kp, NG, sm, out);
   if (threadIdx.x == 0) bs->counter[ci] = 0u;
   return true;
 }
@@ -683,6 +725,16 @@ __global__ void __launch_bounds__(kVecThreads) kb_pq(int n, int kp, const T* __r
                                                      PcgState* st, BatchShared* bs, double* partials, double eps,
                                                      LoopCtl ctl) {
   if (bs->all_done) return;
+  if (!bs->pq_full) {
+    // p.q came with the mat-vec and no column runs its L1 tests on this step
+    // (they alone read |p|_1 and |q|_1): only the scalar step, in block 0
+    if (blockIdx.x == 0) {
+      const int c = threadIdx.x;
+      if (c < kp && !st[c].done) pcg_scalar_pq(&st[c], st[c].pq_dot, 0.0, 0.0, eps);
+      batch_check_all<kLoop>(st, bs, kp, ctl);
+    }
+    return;
+  }
   using VT = Vec16<T>;
   constexpr int W = VT::W;
   using V = typename VT::V;
@@ -1077,6 +1129,7 @@ __global__ void kb_timing_state(PcgState* st, BatchShared* bs, int kp) {
   if (c == 0) {
     bs->all_done = 0;
     bs->l1_due = 0;
+    bs->pq_full = 1;  // kb_pq times its full pass (the every-10th steps)
   }
 }
 

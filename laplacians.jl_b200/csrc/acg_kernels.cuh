@@ -64,6 +64,7 @@ struct PcgState {
   long long nvert;             // vertices of this system (graphs of a group)
   int entering;                // joined a running serving loop: this pass is its pre-loop step
   int pad1;
+  double pq_dot;               // batched loop: p.q summed by the mat-vec
   unsigned int counter[16];    // last-block tickets of the reducing kernels
 };
 

@@ -1492,7 +1492,8 @@ void enqueue_biteration(cudaStream_t s, const SolverImpl& S, T* r, T* sv, T* y, 
   constexpr int kp = CPL * kBatchLanes;
   const TypedArrays<T> A = arrays_of<T>(S);
   const int n = S.n;
-  kb_spmv<T, CPL><<<S.bspmv_blocks[plan_index<T>()][kp_index(kp)], kVecThreads, 0, s>>>(n, A.lp, A.li, A.lv, p, q, S.bsh);
+  kb_spmv<T, CPL, true><<<S.bspmv_blocks[plan_index<T>()][kp_index(kp)], kVecThreads, 0, s>>>(
+      n, A.lp, A.li, A.lv, p, q, S.bsh, S.bst, S.bpartials.p);
   const int* vg = S.bvec_blocks[plan_index<T>()];
   kb_pq<T><<<vg[0], kVecThreads, 0, s>>>(n, kp, p, q, S.bst, S.bsh, S.bpartials.p, eps, ctl);
   kb_update<T><<<vg[1], kVecThreads, 0, s>>>(n, kp, x3, p, q, r, S.bst, S.bsh, S.bpartials.p, ctl);
@@ -1607,7 +1608,7 @@ int batch_occupancy(int sms, int cap) {
 template <typename T, int CPL>
 int spmv_occupancy(int sms) {
   int a = 0;
-  ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kb_spmv<T, CPL>, kVecThreads, 0));
+  ACG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, kb_spmv<T, CPL, true>, kVecThreads, 0));
   return sms * std::max(1, a);
 }
 
@@ -2044,8 +2045,8 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
   auto fill_y = [&]() { k_fill_pending<T><<<kVecBlocks, kVecThreads, 0, s>>>((int)N, y, (T*)nullptr); };
   const double t_fill = time_graph(fill_s);
   out->spmv_ms = time_graph([&]() {
-    kb_spmv<T, CPL><<<S.bspmv_blocks[plan_index<T>()][kp_index(kp)], kVecThreads, 0, s>>>(S.n, A.lp, A.li, A.lv, p, q,
-                                                                                       S.bsh);
+    kb_spmv<T, CPL, true><<<S.bspmv_blocks[plan_index<T>()][kp_index(kp)], kVecThreads, 0, s>>>(
+        S.n, A.lp, A.li, A.lv, p, q, S.bsh, S.bst, S.bpartials.p);
   });
   out->forward_ms = time_graph([&]() {
     fill_s();
