@@ -1135,19 +1135,41 @@ __global__ void kb_timing_state(PcgState* st, BatchShared* bs, int kp) {
 
 // ---- set-up and wrap-up ------------------------------------------------------
 
-// bint[v*kp + c] = B[c*ldb + perm[v]] for c < k, 0 for padding; per-column mean.
-__global__ void __launch_bounds__(kVecThreads) kb_gather_in(int n, int kp, const int* __restrict__ perm,
+// External right-hand-side blocks (column c of B contiguous in the caller's
+// vertex order) and the internal vertex-major rows (kp values per vertex, in
+// level order) are transposes of each other through the vertex permutation.
+// The gather and the scatter go through a shared-memory tile of kTrV external
+// vertices: each column's kTrV values move as one contiguous 256-byte run and
+// each vertex's kp values as one contiguous row, so both sides are coalesced
+// (element-wise, consecutive threads touched kp different columns: 1.45 and
+// 2.51 ms for 64 columns on the 1M grid).
+constexpr int kTrV = 32;
+
+// bint[iperm[e]*kp + c] = B[c*ldb + e] for c < k, 0 for padding; per-column mean.
+__global__ void __launch_bounds__(kVecThreads) kb_gather_in(int n, int kp, const int* __restrict__ iperm,
                                                             const double* __restrict__ B, long long ldb,
                                                             double* __restrict__ bint, PcgState* st, BatchShared* bs,
                                                             double* partials) {
-  const size_t N = (size_t)n * kp;
+  __shared__ double tile[kTrV][kMaxBatch + 1];
   const int k = bs->k;
+  const int t = threadIdx.x;
+  const int per = (int)blockDim.x / kp, part = t / kp, col = t % kp;
   double acc[1] = {0.0};
-  for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
-    const int v = (int)(i / kp), c = (int)(i % kp);
-    const double x = c < k ? B[(size_t)c * ldb + perm[v]] : 0.0;
-    bint[i] = x;
-    acc[0] += x;
+  const int ntiles = (n + kTrV - 1) / kTrV;
+  for (int tb = blockIdx.x; tb < ntiles; tb += gridDim.x) {
+    const int e0 = tb * kTrV;
+    for (int q = t; q < kTrV * kp; q += blockDim.x) {
+      const int c = q / kTrV, e = q % kTrV;
+      tile[e][c] = (c < k && e0 + e < n) ? B[(size_t)c * ldb + e0 + e] : 0.0;
+    }
+    __syncthreads();
+    // column sums in a fixed order: thread t sums column t % kp over its rows
+    for (int e = part; e < kTrV; e += per) acc[0] += tile[e][col];
+    for (int q = t; q < kTrV * kp; q += blockDim.x) {
+      const int e = q / kp, c = q % kp;
+      if (e0 + e < n) bint[(size_t)iperm[e0 + e] * kp + c] = tile[e][c];
+    }
+    __syncthreads();
   }
   double tot[1];
   if (batch_reduce<1>(acc, kp, partials, &bs->counter[4], tot)) {
@@ -1296,15 +1318,26 @@ __global__ void __launch_bounds__(kVecThreads) kb_true_residual(int n, const int
   if (threadIdx.x == 0) bs->counter[6] = 0u;
 }
 
-// X[c*ldx + perm[v]] = xf[v*kp + c], c < k
-__global__ void __launch_bounds__(kVecThreads) kb_scatter_out(int n, int kp, const int* __restrict__ perm,
+// X[c*ldx + e] = xf[iperm[e]*kp + c], c < k (the transpose of kb_gather_in).
+__global__ void __launch_bounds__(kVecThreads) kb_scatter_out(int n, int kp, const int* __restrict__ iperm,
                                                               const double* __restrict__ xf, double* __restrict__ X,
                                                               long long ldx, const BatchShared* bs) {
-  const size_t N = (size_t)n * kp;
+  __shared__ double tile[kTrV][kMaxBatch + 1];
   const int k = bs->k;
-  for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
-    const int v = (int)(i / kp), c = (int)(i % kp);
-    if (c < k) X[(size_t)c * ldx + perm[v]] = xf[i];
+  const int t = threadIdx.x;
+  const int ntiles = (n + kTrV - 1) / kTrV;
+  for (int tb = blockIdx.x; tb < ntiles; tb += gridDim.x) {
+    const int e0 = tb * kTrV;
+    for (int q = t; q < kTrV * kp; q += blockDim.x) {
+      const int e = q / kp, c = q % kp;
+      tile[e][c] = e0 + e < n ? xf[(size_t)iperm[e0 + e] * kp + c] : 0.0;
+    }
+    __syncthreads();
+    for (int q = t; q < kTrV * kp; q += blockDim.x) {
+      const int c = q / kTrV, e = q % kTrV;
+      if (c < k && e0 + e < n) X[(size_t)c * ldx + e0 + e] = tile[e][c];
+    }
+    __syncthreads();
   }
 }
 

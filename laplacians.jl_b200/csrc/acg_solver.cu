@@ -116,6 +116,7 @@ struct SolverImpl {
   DevBuf<SweepTask> tasks_f, tasks_b;
 
   DevBuf<int> perm, lvl_off_d;
+  DevBuf<int> iperm;               // external vertex -> internal (the batched gather and scatter)
   DevBuf<int> l_ptr, l_idx, f_ptr, f_idx, b_ptr, b_idx;
   DevBuf<double> l_v64, f_c64, b_c64, g64;
   DevBuf<float> l_v32, f_c32, b_c32, g32;
@@ -1118,6 +1119,11 @@ void build_solver(SolverImpl& S, int64_t n64, const int64_t* a_colptr, const int
   // ---- upload
   cudaStream_t s = S.stream;
   S.perm.upload(perm, s);
+  {
+    std::vector<int> iperm(perm.size());
+    for (size_t v = 0; v < perm.size(); ++v) iperm[perm[v]] = (int)v;
+    S.iperm.upload(iperm, s);
+  }
   S.lvl_off_d.upload(S.lvl_off, s);
   S.l_ptr.upload(lptr, s);
   S.l_idx.upload(lidx, s);
@@ -1515,7 +1521,7 @@ cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S, int slot) {
   LoopCtl ctl{h, 1};
   double* x3 = S.bx3_64.p;
   begin_into(s, top, {});
-  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bb_ext[slot].p, (long long)n, S.bbm.p, S.bst, S.bsh,
+  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.iperm.p, S.bb_ext[slot].p, (long long)n, S.bbm.p, S.bst, S.bsh,
                                                   S.bpartials.p);
   kb_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, x3, S.bs64.p, S.by64.p, S.bst,
                                                        S.bsh, S.bpartials.p, ctl);
@@ -1534,7 +1540,7 @@ cudaGraphExec_t build_batch_fp64_graph(SolverImpl& S, int slot) {
   kb_take_best<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, x3, S.bxf.p, S.bst);
   kb_true_residual<CPL><<<kVecBlocks, kVecThreads, 0, s>>>(n, S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.bxf.p, S.bbm.p,
                                                            nullptr, S.bst, S.bsh, S.bpartials.p);
-  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, S.bx_ext[slot].p, (long long)n, S.bsh);
+  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.iperm.p, S.bxf.p, S.bx_ext[slot].p, (long long)n, S.bsh);
   end_into(s);
   (void)N;
   cudaGraphExec_t exec;
@@ -1555,7 +1561,7 @@ cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S, int slot) {
   ACG_CUDA(cudaGraphConditionalHandleCreate(&ho, top, 1u, cudaGraphCondAssignDefault));
   LoopCtl octl{ho, 1};
   begin_into(s, top, {});
-  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bb_ext[slot].p, (long long)n, S.bbm.p, S.bst, S.bsh,
+  kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.iperm.p, S.bb_ext[slot].p, (long long)n, S.bbm.p, S.bst, S.bsh,
                                                   S.bpartials.p);
   kb_center<double><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, S.bxf.p, (double*)nullptr,
                                                        (double*)nullptr, S.bst, S.bsh, S.bpartials.p, octl);
@@ -1587,7 +1593,7 @@ cudaGraphExec_t build_batch_mixed_graph(SolverImpl& S, int slot) {
   kb_outer_decide<<<1, kMaxBatch, 0, s>>>(S.bst, S.bsh, kp, octl);
   end_into(s);
   begin_into(s, top, {onode});
-  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, S.bxf.p, S.bx_ext[slot].p, (long long)n, S.bsh);
+  kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.iperm.p, S.bxf.p, S.bx_ext[slot].p, (long long)n, S.bsh);
   end_into(s);
   cudaGraphExec_t exec;
   ACG_CUDA(cudaGraphInstantiate(&exec, top, 0));
