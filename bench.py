@@ -468,6 +468,10 @@ def run_acgpu(args):
                          # the sweep walks the DAG's head levels one after another: time per level
                          "swept_levels": swept_levels, "us_per_level": 1e3 * sweep_ms / max(1, swept_levels),
                          "spmv_ms": kt["spmv_ms"], "spmv_gbs": kt["spmv_bytes"] / (kt["spmv_ms"] * 1e-3) / 1e9},
+            # every kernel of a batched solve, each timed alone (CUDA events, ms per launch)
+            "kernel_ms": ({key: round(kt[key + "_ms"], 4) for key in
+                           ("spmv", "forward_sweep", "backward_sweep", "dense", "pq", "update", "yzr", "pupdate",
+                            "gather", "scatter", "true_residual")} if k > 1 else None),
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": int(round(launches)),

@@ -210,6 +210,10 @@ typedef struct {
      y, y.r and r; the p update; and their algorithmic bytes */
   double pq_ms, update_ms, yzr_ms, pupdate_ms;
   double pq_bytes, update_bytes, yzr_bytes, pupdate_bytes;
+  /* a batched solve's set-up and wrap-up (acg_time_kernels_batch only): the
+     gather of the right-hand-side block into vertex-major rows, the scatter
+     of x back, and one FP64 true residual b - L x of the block */
+  double gather_ms, scatter_ms, true_residual_ms;
 } acg_kernel_times;
 
 /* 0 if the current CUDA device is usable (sm_100), else an error code. */

@@ -62,7 +62,8 @@ class AcgKernelTimes(ctypes.Structure):
                 ("backward_sweep_bytes", ctypes.c_double), ("dense_bytes", ctypes.c_double),
                 ("pq_ms", ctypes.c_double), ("update_ms", ctypes.c_double), ("yzr_ms", ctypes.c_double),
                 ("pupdate_ms", ctypes.c_double), ("pq_bytes", ctypes.c_double), ("update_bytes", ctypes.c_double),
-                ("yzr_bytes", ctypes.c_double), ("pupdate_bytes", ctypes.c_double)]
+                ("yzr_bytes", ctypes.c_double), ("pupdate_bytes", ctypes.c_double),
+                ("gather_ms", ctypes.c_double), ("scatter_ms", ctypes.c_double), ("true_residual_ms", ctypes.c_double)]
 
 
 # (name, restype, argtypes) for every entry point of include/acgpu.h

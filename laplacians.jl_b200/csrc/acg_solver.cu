@@ -2122,6 +2122,24 @@ void time_batch_t(SolverImpl& S, int reps, acg_kernel_times* out, T* r, T* sv, T
       reset();
       kb_pupdate_z<T, false><<<vg[3], kVecThreads, 0, s>>>(S.n, kp, y, p, S.bst, S.bsh, S.bpartials.p, eps, none);
     }) - t_reset;
+    // set-up and wrap-up of a batched solve (FP64 blocks in both precisions)
+    {
+      const int kk = kp;
+      ACG_CUDA(cudaMemcpyAsync(&S.bsh->k, &kk, sizeof(int), cudaMemcpyHostToDevice, s));
+      ACG_CUDA(cudaStreamSynchronize(s));
+      out->gather_ms = time_graph([&]() {
+        kb_gather_in<<<kVecBlocks, kVecThreads, 0, s>>>(S.n, kp, S.iperm.p, S.bb_ext[0].p, (long long)S.n, S.bbm.p,
+                                                        S.bst, S.bsh, S.bpartials.p);
+      });
+      out->scatter_ms = time_graph([&]() {
+        kb_scatter_out<<<kVecBlocks, kVecThreads, 0, s>>>(S.n, kp, S.iperm.p, S.bxf.p, S.bx_ext[0].p,
+                                                          (long long)S.n, S.bsh);
+      });
+      out->true_residual_ms = time_graph([&]() {
+        kb_true_residual<CPL><<<kVecBlocks, kVecThreads, 0, s>>>(S.n, S.l_ptr.p, S.l_idx.p, S.l_v64.p, S.bxf.p,
+                                                                 S.bbm.p, S.br64.p, S.bst, S.bsh, S.bpartials.p);
+      });
+    }
     const double vec = (double)S.n * kp * sizeof(T);
     out->pq_bytes = 2.0 * vec;       // p, q read
     out->update_bytes = 6.0 * vec;   // x, p, q, r read; x', r written
