@@ -319,7 +319,8 @@ int acg_time_kernels_batch(acg_solver* h, int precision, int nrhs, int reps, acg
  * 0..L and bwd_ms[i] the backward sweep over the tasks of levels >= L (the
  * swept head; the dense tail's levels are never swept), each per launch with
  * nrhs right-hand sides; fwd_tasks[i] / bwd_tasks[i] are those tasks.  Levels
- * are clamped to [0, levels - 1].  The differences between points show what
+ * are clamped to [0, levels - 1]; times are differences of two timings, and a
+ * prefix shorter than the timing noise reads 0.  The differences between points show what
  * each range of levels costs.  Diagnostic only: it uses the batch buffers, so a
  * solver that serves answers ACG_ERR_BUSY; a group solver ACG_ERR_INVALID. */
 int acg_time_sweep_levels(acg_solver* h, int precision, int nrhs, int reps, int npts, const int* levels,

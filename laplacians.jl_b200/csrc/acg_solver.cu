@@ -2204,15 +2204,17 @@ void time_levels_t(SolverImpl& S, int reps, int npts, const int* levels, double*
     const int tf = S.tfb_upto[L], tb = S.tbb_from[L];
     fwd_tasks[i] = tf;
     bwd_tasks[i] = tb;
-    fwd_ms[i] = graph_ms(s, reps, [&]() {
-                  fill_s();
-                  if (tf > 0) enqueue_bsweep<T, CPL, true>(s, S, r, (T*)nullptr, sv, y, tf);
-                }) - t_fill;
-    bwd_ms[i] = graph_ms(s, reps, [&]() {
-                  restore_s();
-                  fill_yh();
-                  if (tb > 0) enqueue_bsweep<T, CPL, false>(s, S, arrays_of<T>(S).g, sv, y, sv, tb);
-                }) - t_back;
+    // differences of two timings: a prefix shorter than the timing noise may
+    // come out below zero, reported as 0
+    fwd_ms[i] = std::max(0.0, graph_ms(s, reps, [&]() {
+                                fill_s();
+                                if (tf > 0) enqueue_bsweep<T, CPL, true>(s, S, r, (T*)nullptr, sv, y, tf);
+                              }) - t_fill);
+    bwd_ms[i] = std::max(0.0, graph_ms(s, reps, [&]() {
+                                restore_s();
+                                fill_yh();
+                                if (tb > 0) enqueue_bsweep<T, CPL, false>(s, S, arrays_of<T>(S).g, sv, y, sv, tb);
+                              }) - t_back);
   }
   BatchShared hb;
   ACG_CUDA(cudaMemcpy(&hb, S.bsh, sizeof(BatchShared), cudaMemcpyDeviceToHost));

@@ -129,7 +129,9 @@ def test_sweep_levels_timing(graph):
             assert bt[0] > bt[3] > 0
             # the last level is swept only without a dense tail
             assert bt[-1] == (bt[3] if st["dense_levels"] == 0 else 0)
-            assert all(r["forward_ms"] > 0 for r in rows)
+            # differences of timings: tiny prefixes may be within the noise (reported as 0)
+            assert all(r["forward_ms"] >= 0 and r["backward_ms"] >= 0 for r in rows)
+            assert rows[-1]["forward_ms"] > 0 and rows[0]["backward_ms"] > 0
         # still solves correctly afterwards
         b = np.random.default_rng(9).standard_normal(a.shape[0])
         x = solver(b, tol=1e-8, maxits=2000, precision="mixed")
