@@ -1252,6 +1252,10 @@ __global__ void __launch_bounds__(kVecThreads) kb_take_best(int n, int kp, const
 }
 
 // t = bm - L x (FP64), optionally stored; per column |t| -> nr_true, scale.
+// Rows as kb_spmv walks them: 8 entries at a time shared inside the group of 8
+// lanes, every gathered row of x issued before the first multiply-add (one
+// entry at a time it took 1.10 ms for 64 columns on the 1M grid); the
+// per-column sums of t^2 in two levels (batch_reduce_v).
 template <int CPL>
 __global__ void __launch_bounds__(kVecThreads) kb_true_residual(int n, const int* __restrict__ ptr,
                                                                 const int* __restrict__ idx,
@@ -1264,58 +1268,61 @@ __global__ void __launch_bounds__(kVecThreads) kb_true_residual(int n, const int
   constexpr int kp = CPL * kBatchLanes;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int gl = gt & 7;
+  const unsigned gmask = 0xffu << (threadIdx.x & 24);  // this group's lanes
   const int groups = gridDim.x * blockDim.x / 8;
-  double acc[CPL];
+  double sq[1][CPL];
 #pragma unroll
-  for (int j = 0; j < CPL; ++j) acc[j] = 0.0;
-  for (int row = gt / 8; row < n; row += groups) {
-    const int k0 = __ldg(&ptr[row]), k1 = __ldg(&ptr[row + 1]);
-    double s[CPL];
+  for (int j = 0; j < CPL; ++j) sq[0][j] = 0.0;
+  int row = gt / 8;
+  int n0 = row < n ? __ldg(&ptr[row]) : 0, n1 = row < n ? __ldg(&ptr[row + 1]) : 0;
+  for (; row < n; row += groups) {
+    const int k0 = n0, k1 = n1;
+    const int nxt = row + groups;
+    n0 = nxt < n ? __ldg(&ptr[nxt]) : 0;
+    n1 = nxt < n ? __ldg(&ptr[nxt + 1]) : 0;
+    double acc[CPL];
 #pragma unroll
-    for (int j = 0; j < CPL; ++j) s[j] = 0.0;
-    for (int k = k0; k < k1; ++k) {
-      const int id = __ldg(&idx[k]);
-      const double c = __ldg(&val[k]);
-      const double* xr = x + (size_t)id * kp + gl * CPL;
+    for (int j = 0; j < CPL; ++j) acc[j] = 0.0;
+    for (int kb = k0; kb < k1; kb += 8) {
+      const int k = kb + gl;
+      const int myid = k < k1 ? __ldg(&idx[k]) : -1;
+      const double myc = k < k1 ? __ldg(&val[k]) : 0.0;
+      int ids[8];
+      double cs[8];
+      double v[8][CPL];
 #pragma unroll
-      for (int j = 0; j < CPL; ++j) s[j] += c * xr[j];
+      for (int u = 0; u < 8; ++u) {
+        ids[u] = __shfl_sync(gmask, myid, u, 8);
+        cs[u] = __shfl_sync(gmask, myc, u, 8);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (ids[u] >= 0) ldg_row<double, CPL>(v[u], x + (size_t)ids[u] * kp + gl * CPL);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (ids[u] >= 0) {
+#pragma unroll
+          for (int j = 0; j < CPL; ++j) acc[j] += cs[u] * v[u][j];
+        }
     }
+    double b[CPL];
+    ldg_row<double, CPL>(b, bm + (size_t)row * kp + gl * CPL);
 #pragma unroll
     for (int j = 0; j < CPL; ++j) {
-      const size_t e = (size_t)row * kp + gl * CPL + j;
-      const double t = bm[e] - s[j];
-      if (rout) rout[e] = t;
-      acc[j] += t * t;
+      const double t = b[j] - acc[j];
+      if (rout) rout[(size_t)row * kp + gl * CPL + j] = t;
+      sq[0][j] += t * t;
     }
   }
-  // per column reduction: thread holds columns gl*CPL + j
-  __shared__ double sm[kVecThreads][CPL];
-  __shared__ bool am_last;
-#pragma unroll
-  for (int j = 0; j < CPL; ++j) sm[threadIdx.x][j] = acc[j];
-  __syncthreads();
-  if ((int)threadIdx.x < kp) {
-    const int lane8 = threadIdx.x / CPL, j = threadIdx.x % CPL;
-    double s = 0.0;
-    for (int t = lane8; t < (int)blockDim.x; t += 8) s += sm[t][j];
-    partials[(size_t)blockIdx.x * kp + threadIdx.x] = s;
+  double tot[1];
+  if (batch_reduce_v<1, CPL>(sq, kp, partials, bs, 6, tot)) {
+    const int c = threadIdx.x;
+    if (c < kp) {
+      PcgState* p = &st[c];
+      p->scale = sqrt(tot[0]);
+      p->nr_true = p->nb64 > 0.0 ? p->scale / p->nb64 : 0.0;
+    }
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    am_last = atomicAdd(&bs->counter[6], 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!am_last) return;
-  __threadfence();
-  if ((int)threadIdx.x < kp) {
-    double s = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(&partials[(size_t)b * kp + threadIdx.x]);
-    PcgState* p = &st[threadIdx.x];
-    p->scale = sqrt(s);
-    p->nr_true = p->nb64 > 0.0 ? p->scale / p->nb64 : 0.0;
-  }
-  if (threadIdx.x == 0) bs->counter[6] = 0u;
 }
 
 // X[c*ldx + e] = xf[iperm[e]*kp + c], c < k (the transpose of kb_gather_in).

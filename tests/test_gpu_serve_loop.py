@@ -44,19 +44,19 @@ def test_requests_join_a_running_loop_and_match_alone(problem, precision):
     tol = 1e-8
     loop = acgpu.ServeLoop(dev, precision=precision, slots=8, queue=40)
     tickets = [None] * len(blocks)
-    # the first wave starts the loop; the rest arrive while it runs
+    # the first wave starts the loop; the rest arrive while it runs (a solve
+    # here takes a millisecond or two, so the late ones follow at once)
     for i in range(4):
         tickets[i] = loop.submit(blocks[i], tol=tol)
-    time.sleep(0.002)
     joined_while_running = 0
 
     def late():
         nonlocal joined_while_running
         for i in range(4, len(blocks)):
-            if not tickets[0].done():
+            if any(not tickets[j].done() for j in range(i)):
                 joined_while_running += 1
             tickets[i] = loop.submit(blocks[i], tol=tol)
-            time.sleep(0.001)
+            time.sleep(0.0002)
 
     th = threading.Thread(target=late)
     th.start()
