@@ -696,6 +696,27 @@ def run_many_graphs(args):
     out["slowest_members"] = slow
     del out["_its"]
     out["levels_max"] = gs.stats()["levels"]
+    if args.tune:
+        # config 4b's tuned tiles: one round of coordinate descent over the
+        # union sweeps' knobs, measured by the FP64 group solve itself
+        from acgpu.tuning import coordinate_descent
+
+        def group_ms(opts):
+            g = acgpu.GroupSolver(comp_graphs, factors, options={k: v for k, v in opts.items() if v != 0})
+            try:
+                ts = []
+                for _ in range(2):
+                    t0 = time.perf_counter()
+                    g(comp_b, tol=TOL, maxits=MAXITS, precision="fp64")
+                    ts.append(time.perf_counter() - t0)
+                return 1e3 * min(ts)
+            finally:
+                g.close()
+
+        space = {"sweep_heavy": [0, 8, 32], "sweep_blocks_per_sm": [0, 2, 3], "poll_mode": [0, 1, 2]}
+        tr = coordinate_descent(group_ms, space, rounds=1, min_gain=0.02)
+        out["tuned_fp64"] = {"options": tr.options, "group_ms": tr.ms, "default_ms": tr.baseline_ms,
+                             "trials": [(o, round(ms, 2)) for o, ms in tr.trials]}
     seq = []
     for a, f, b in zip(comp_graphs, factors, comp_b):
         dev = acgpu.DeviceLapSolver(a, f)
@@ -983,6 +1004,7 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=300)
     ap.add_argument("--serving-rate", type=float, default=40.0, help="requests per second")
     ap.add_argument("--serving-hbm-gb", type=float, default=120.0)
+    ap.add_argument("--tune", action="store_true", help="many_graphs: tune the group's sweep knobs first")
     args = ap.parse_args()
     globals()["GRID_SIDE"] = args.side
     if args.warmup < 3 and args.impl == "acgpu":
