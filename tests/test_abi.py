@@ -58,6 +58,10 @@ def test_bad_arguments_are_errors():
     assert L.acg_solve_async(None, None, None, 1, 1, 1e-8, 10, 1.0, 5, 0, ctypes.byref(req)) == -1
     assert L.acg_poll(None) == -1
     assert L.acg_wait(None, None) == -1
+    # diagnostics and group entries reject null handles before touching a device
+    assert L.acg_time_sweep_levels(None, 1, 64, 1, 0, None, None, None, None, None) == -1
+    assert L.acg_solve_group(None, f, f, 1e-8, 10, 1.0, 5, 0, None) == -1
+    assert L.acg_time_kernels_batch(None, 1, 64, 1, None) == -1
 
 
 def _header_struct_fields(tag):
