@@ -157,7 +157,7 @@ typedef struct {
                                 produced and the waits on them run out; a test of the
                                 bounded waits that neither faults nor hangs the GPU     */
   double min_inner_tol;      /* mixed precision: the smallest relative residual an inner
-                                FP32 solve is asked for (0 = 1e-5)                      */
+                                FP32 solve is asked for (0 = 2e-5)                      */
 } acg_options;
 
 /* Shape of an uploaded solver. */

@@ -69,7 +69,7 @@ struct ServeSlots {
 
 // 1. Admission (one block of kMaxBatch threads; thread 0 takes the ring).
 __global__ void ks_admit(ServeRing* ring, ServeRequest* reqs, ServeSlots* sl, PcgState* st, BatchShared* bs, int kp,
-                         LoopCtl ctl) {
+                         LoopCtl ctl, double min_inner_tol) {
   __shared__ int free_list[kMaxBatch];
   __shared__ int nfree, busy;
   const int c = threadIdx.x;
@@ -116,7 +116,7 @@ __global__ void ks_admit(ServeRing* ring, ServeRequest* reqs, ServeSlots* sl, Pc
       s->stag_test = r.stag_test;
       s->tol_user = r.tol;
       s->maxits_user = r.maxits;
-      s->min_inner_tol = 1e-5;
+      s->min_inner_tol = min_inner_tol;
       s->max_outer = 40;
       double it = 0.5 * r.tol;
       if (it < s->min_inner_tol) it = s->min_inner_tol;

@@ -111,7 +111,7 @@ struct SolverImpl {
   int sweep_blocks[2] = {0, 0};    // co-resident grid of k_sweep per value type
   int poll_mode = 0;
   unsigned spin_limit = kSpinLimit;  // polls before a sweep wait gives up
-  double min_inner_tol = 1e-5;       // mixed precision: floor of an inner solve's tolerance
+  double min_inner_tol = 2e-5;       // mixed precision: floor of an inner solve's tolerance
   cudaEvent_t order_ev = nullptr;    // device entry points: after the legacy stream's work
   DevBuf<SweepTask> tasks_f, tasks_b;
 
@@ -2403,7 +2403,7 @@ cudaGraphExec_t build_serve_graph(SolverImpl& S, int precision, ServeRing* ring,
   cudaGraph_t body;
   add_while(top, {}, h, &body);
   begin_into(s, body, {});
-  ks_admit<<<1, kMaxBatch, 0, s>>>(ring, reqs, sl, S.bst, S.bsh, kp, ctl);
+  ks_admit<<<1, kMaxBatch, 0, s>>>(ring, reqs, sl, S.bst, S.bsh, kp, ctl, S.min_inner_tol);
   ks_gather<<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.perm.p, ring, reqs, sl, S.bbm.p, S.bst, S.bsh, S.bpartials.p);
   if (mixed) {
     ks_center<float><<<kVecBlocks, kVecThreads, 0, s>>>(n, kp, S.bbm.p, S.br64.p, S.br32.p, S.bx3_32.p, S.bxf.p,
